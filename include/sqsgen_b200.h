@@ -1,0 +1,211 @@
+/*
+ * sqsgen_b200 — C ABI of the B200-native SQS optimisation hot path.
+ *
+ * The library replaces the optimisation loop of dgehringer/sqsgenerator 0.5.6 (a header-only C++
+ * library with no C ABI of its own). Each entry point below names the reference interface it
+ * replaces (paths relative to the reference repository root).
+ *
+ * Conventions
+ *  - Plain C types, caller-owned buffers, no exceptions across the ABI: every call returns an
+ *    sqsg_status; sqsg_last_error() gives the message of the calling thread's last failure.
+ *  - prec selects the floating type of every `void*` array: 0 = float (single), 1 = double.
+ *  - Cubes (prefactors, pair weights, targets, SRO) are row-major [shell][a][b] over dense species
+ *    indices (sorted atomic numbers), shells packed by ascending shell index.
+ *  - Species arrays passed to the optimiser are "packed": values 0..K-1 in the sorted site order
+ *    produced by the host precompute (sqsg_sort_by_sublattice).
+ *  - The optimiser runs on one CUDA device per call; calls on different host threads with different
+ *    jobs may run concurrently. There is no CPU fallback: without a usable CUDA device the
+ *    optimiser returns SQSG_ERR_CUDA.
+ */
+#ifndef SQSGEN_B200_H
+#define SQSGEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SQSG_ABI_VERSION 1
+
+typedef enum {
+  SQSG_OK = 0,
+  SQSG_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  SQSG_ERR_OUT_OF_RANGE = 2,     /* std::out_of_range in the reference */
+  SQSG_ERR_CAPACITY = 3,         /* caller buffer too small; the needed size is reported */
+  SQSG_ERR_CUDA = 4,             /* CUDA runtime failure or no device */
+  SQSG_ERR_UNSUPPORTED = 5,      /* a size this build does not handle (message says which) */
+  SQSG_ERR_TIMEOUT = 6,          /* a bounded device wait ran out */
+  SQSG_ERR_BUSY = 7              /* server queue full / admission refused */
+} sqsg_status;
+
+enum { SQSG_PREC_SINGLE = 0, SQSG_PREC_DOUBLE = 1 };
+enum { SQSG_ITERATION_RANDOM = 0, SQSG_ITERATION_SYSTEMATIC = 1 };
+enum { SQSG_SUBLATTICE_INTERACT = 0, SQSG_SUBLATTICE_SPLIT = 1 };
+enum { SQSG_TIMING_TOTAL = 0, SQSG_TIMING_CHUNK_SETUP = 1, SQSG_TIMING_LOOP = 2, SQSG_TIMING_COMM = 3 };
+
+/* ------------------------------------------------------------------------------------------------
+ * Library information
+ */
+const char* sqsg_version(void);
+/* Copies the calling thread's last error message (NUL-terminated, truncated to len). */
+size_t sqsg_last_error(char* buf, size_t len);
+/* Number of CUDA devices visible to the library (0 when none). */
+int sqsg_device_count(void);
+
+/* ------------------------------------------------------------------------------------------------
+ * Host precompute: geometry, shells, prefactors, pair list (run once per job, on the CPU).
+ */
+
+/* core::structure::supercell — include/sqsgen/core/structure.h:335-366.
+ * lattice: 3x3 row-major (rows are lattice vectors); frac: n x 3. Outputs hold a*b*c*n sites. */
+sqsg_status sqsg_supercell(int prec, const void* lattice, const void* frac, const uint8_t* species,
+                           uint32_t n, uint32_t a, uint32_t b, uint32_t c, void* lattice_out,
+                           void* frac_out, uint8_t* species_out);
+
+/* core::detail::distance_matrix — include/sqsgen/core/structure.h:35-69 (minimum over the 27
+ * images (-1,0,1)^3). out: n x n row-major. */
+sqsg_status sqsg_distance_matrix(int prec, const void* lattice, const void* frac, uint32_t n, void* out);
+
+/* core::detail::shell_matrix — include/sqsgen/core/structure.h:71-100. radii[0] must be 0. */
+sqsg_status sqsg_shell_matrix(int prec, const void* distances, uint32_t n, const void* radii,
+                              uint32_t n_radii, double atol, double rtol, uint32_t* out);
+
+/* core::distances_naive — include/sqsgen/core/structure.h:195-207.
+ * *n_out: in = capacity of out, out = number of radii (SQSG_ERR_CAPACITY if it did not fit). */
+sqsg_status sqsg_distances_naive(int prec, const void* distances, uint32_t n, double atol, double rtol,
+                                 void* out, uint32_t* n_out);
+
+/* core::distances_histogram — include/sqsgen/core/structure.h:209-258 (peak detection). */
+sqsg_status sqsg_distances_histogram(int prec, const void* distances, uint32_t n, double bin_width,
+                                     double peak_isolation, void* out, uint32_t* n_out);
+
+/* core::detail::compute_prefactors — include/sqsgen/core/structure.h:136-192.
+ * shells: n x n shell matrix; shell_ids: the weighted shells (ascending); species: atomic numbers.
+ * out: S x K x K row-major, K = distinct species. */
+sqsg_status sqsg_prefactors(int prec, const uint32_t* shells, uint32_t n, const uint32_t* shell_ids,
+                            uint32_t n_shells, const uint8_t* species, void* out);
+
+/* core::structure::pairs — include/sqsgen/core/structure.h:434-451 (i < j, packed shell index).
+ * *n_pairs: in = capacity (in pairs), out = count. pairs_out: 3 x count (i, j, shell). */
+sqsg_status sqsg_pairs(const uint32_t* shells, uint32_t n, const uint32_t* shell_ids, uint32_t n_shells,
+                       uint32_t* pairs_out, uint32_t* n_pairs);
+
+/* optimization::compute_shuffling_bounds — include/sqsgen/core/optimization.h:35-72.
+ * sublattice_of_site[i] = index of the sublattice containing site i, or n_sublattices when none.
+ * Writes sort_order (n; sorted position -> original site) and windows (2 x *n_windows). */
+sqsg_status sqsg_sort_by_sublattice(const uint32_t* sublattice_of_site, uint32_t n, uint32_t n_sublattices,
+                                    uint32_t* sort_order, uint32_t* windows, uint32_t* n_windows);
+
+/* ------------------------------------------------------------------------------------------------
+ * Multiset permutations (u64 ranks; the reference parser rejects counts above u64,
+ * include/sqsgen/io/config/combined.h:88-95).
+ */
+/* core::num_permutations — include/sqsgen/core/permutation.h:17-32. SQSG_ERR_OUT_OF_RANGE on overflow. */
+sqsg_status sqsg_num_permutations(const uint8_t* conf, uint32_t n, uint64_t* out);
+/* core::rank_permutation — include/sqsgen/core/permutation.h:34-50 (1-based, dense values). */
+sqsg_status sqsg_rank_permutation(const uint8_t* conf, uint32_t n, uint64_t* rank);
+/* core::unrank_permutation — include/sqsgen/core/permutation.h:52-78 (writes dense values). */
+sqsg_status sqsg_unrank_permutation(uint8_t* conf, uint32_t n, uint64_t rank);
+
+/* ------------------------------------------------------------------------------------------------
+ * The optimiser — replaces sqsgen::run_optimization (include/sqsgen/sqs.h:625-634) and its worker
+ * loop optimizer<T,IterationMode,SublatticeMode>::run (include/sqsgen/sqs.h:299-580).
+ */
+typedef struct {
+  uint32_t n_sites;           /* N: sites of this optimised structure, sorted order */
+  uint32_t n_species;         /* K */
+  uint32_t n_shells;          /* S */
+  uint32_t n_pairs;           /* P */
+  uint32_t n_windows;         /* shuffle windows (interact: one per sublattice) */
+  uint32_t reserved;
+  const uint32_t* pairs;      /* 3 x P: (i, j, shell), i < j */
+  const uint8_t* species;     /* N packed species (0..K-1) */
+  const uint32_t* windows;    /* 2 x n_windows: [lo, hi) */
+  const void* prefactors;     /* S x K x K */
+  const void* pair_weights;   /* S x K x K, already multiplied by the shell weights */
+  const void* target;         /* S x K x K */
+} sqsg_sublattice;
+
+typedef struct {
+  uint64_t finished;          /* configurations evaluated */
+  uint64_t working;           /* configurations in flight */
+  uint64_t best_rank;         /* systematic: rank of the best; random: (chain << 32) | iteration */
+  double best_objective;
+  uint64_t timings_ns[4];     /* SQSG_TIMING_* */
+} sqsg_statistics;
+
+/* Progress callback, invoked from the calling host thread (never from device code) while the
+ * device works. Return non-zero to stop early (like sqs_callback_context::stop, types.h:222-232);
+ * results found so far are kept. */
+typedef int (*sqsg_callback)(const sqsg_statistics* stats, void* user);
+
+typedef struct {
+  int32_t prec;
+  int32_t iteration_mode;
+  int32_t sublattice_mode;
+  uint32_t n_sublattices;     /* interact: 1 (windows carry the sublattices); split: one per sublattice */
+  const sqsg_sublattice* sublattices;
+  uint64_t iterations;        /* random: configurations to evaluate; systematic: 0 = all permutations */
+  uint64_t chunk_size;        /* progress-callback granularity in configurations (0: default) */
+  uint64_t keep;              /* the reference's `keep` (1..31 in this build) */
+  int64_t max_results_per_objective; /* < 0: unset */
+  uint64_t seed;              /* random mode: Philox key */
+  int32_t has_seed;           /* 0: a random seed is drawn */
+  int32_t device;             /* CUDA device ordinal */
+  const volatile int32_t* cancel; /* optional: set non-zero from any thread to stop early */
+  sqsg_callback callback;     /* optional */
+  void* user;
+  uint64_t max_results;       /* record capacity of the result set (0: library default, grown on demand
+                                 within a 4 GiB device budget) */
+} sqsg_job;
+
+typedef struct sqsg_run sqsg_run;
+
+/* Runs one job to completion on job->device and returns its result set in *run (free with
+ * sqsg_run_free). The result set is every distinct configuration whose objective is within the
+ * keep+1 best distinct objectives seen — the configurations the reference's result collection
+ * (include/sqsgen/core/results.h:42-99, sqs.h:421-438) always returns — capped at
+ * max_results_per_objective+1 per objective when that is set. */
+sqsg_status sqsg_optimize(const sqsg_job* job, sqsg_run** run);
+
+/* Result access. Records are sorted by total objective, then by id. */
+uint64_t sqsg_run_count(const sqsg_run* run);
+/* Copies records [first, first+n). Any output pointer may be NULL. Per record: objective (prec),
+ * sub_objectives (n_sublattices, prec), species (sum of N, packed, sorted order), sro
+ * (sum of S*K*K, prec, row-major), id (systematic: 1-based rank; random: (chain << 32) | iteration). */
+sqsg_status sqsg_run_copy(const sqsg_run* run, uint64_t first, uint64_t n, void* objective,
+                          void* sub_objectives, uint8_t* species, void* sro, uint64_t* id);
+sqsg_status sqsg_run_statistics(const sqsg_run* run, sqsg_statistics* stats);
+void sqsg_run_free(sqsg_run* run);
+
+/* The keep+1 best distinct objectives seen (ascending), each with the number of evaluations that
+ * produced it and an order-independent checksum of their ids (two 32-bit sums of splitmix64(id),
+ * low and high halves). These are exact even when the record set was cut at its capacity.
+ * *n: in = capacity, out = number of levels. No reference counterpart (the reference keeps every
+ * record); they make results of any size comparable. */
+sqsg_status sqsg_run_levels(const sqsg_run* run, uint32_t* n, double* values, uint64_t* counts,
+                            uint64_t* checksums);
+/* candidates: records the device appended; truncated: 1 when the record set hit its capacity;
+ * levels_exact: 0 when the level table overflowed (then only the records define the result). */
+sqsg_status sqsg_run_info(const sqsg_run* run, uint64_t* candidates, int32_t* truncated, int32_t* levels_exact);
+
+/* Debug/parity trace: like sqsg_optimize, but additionally records every evaluated configuration
+ * (at most `capacity`; SQSG_ERR_CAPACITY otherwise) with its packed species, ordered bond counts
+ * (S x K x K u32 per sublattice, like core/optimization.h:74-77) and objective. Sizes: species
+ * capacity x sum N; bonds capacity x sum S*K*K; objective capacity (prec); id capacity. */
+sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t capacity, uint64_t* count,
+                                uint8_t* species, uint32_t* bonds, void* objective, uint64_t* id);
+
+/* ------------------------------------------------------------------------------------------------
+ * Batched form: many independent jobs in one persistent launch fed by a device tile queue
+ * (no reference counterpart; the reference runs one configuration per call).
+ */
+sqsg_status sqsg_optimize_batch(const sqsg_job* jobs, uint32_t n_jobs, sqsg_run** runs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SQSGEN_B200_H */

@@ -1,0 +1,16 @@
+"""B200-native SQS optimisation hot path with the API of ``sqsgenerator``.
+
+``parse_config`` and ``optimize`` mirror ``sqsgenerator.parse_config`` / ``sqsgenerator.optimize``;
+the optimisation loop runs in hand-written sm_100a CUDA kernels behind the C ABI declared in
+``include/sqsgen_b200.h``. There is no CPU fallback for the loop.
+"""
+from .config import parse_config
+from .core import (IterationMode, LogLevel, ParseError, ParseErrorCode, Prec, ShellRadiiDetection, SqsConfiguration,
+                   SqsResult, SqsResultPack, SqsResultSplit, SqsStatistics, Structure, SublatticeMode)
+from .optimize import optimize, prepare
+
+__all__ = [
+    "parse_config", "optimize", "prepare", "IterationMode", "LogLevel", "ParseError", "ParseErrorCode", "Prec",
+    "ShellRadiiDetection", "SqsConfiguration", "SqsResult", "SqsResultPack", "SqsResultSplit", "SqsStatistics",
+    "Structure", "SublatticeMode",
+]

@@ -1,0 +1,280 @@
+"""ctypes binding of ``libsqsg_b200.so`` (declared in ``include/sqsgen_b200.h``).
+
+The library is built in-tree (``sqsgenerator_b200/build.py``). Importing this module never falls
+back to another implementation: when the shared library is missing, ``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libsqsg_b200.so")
+
+SQSG_OK = 0
+STATUS_NAMES = {
+    0: "SQSG_OK",
+    1: "SQSG_ERR_INVALID_ARGUMENT",
+    2: "SQSG_ERR_OUT_OF_RANGE",
+    3: "SQSG_ERR_CAPACITY",
+    4: "SQSG_ERR_CUDA",
+    5: "SQSG_ERR_UNSUPPORTED",
+    6: "SQSG_ERR_TIMEOUT",
+    7: "SQSG_ERR_BUSY",
+}
+
+#: Every entry point the header declares (checked by the CPU test-suite).
+EXPORTED = (
+    "sqsg_version", "sqsg_last_error", "sqsg_device_count",
+    "sqsg_supercell", "sqsg_distance_matrix", "sqsg_shell_matrix", "sqsg_distances_naive",
+    "sqsg_distances_histogram", "sqsg_prefactors", "sqsg_pairs", "sqsg_sort_by_sublattice",
+    "sqsg_num_permutations", "sqsg_rank_permutation", "sqsg_unrank_permutation",
+    "sqsg_optimize", "sqsg_run_count", "sqsg_run_copy", "sqsg_run_statistics", "sqsg_run_free",
+    "sqsg_optimize_trace", "sqsg_optimize_batch", "sqsg_run_levels", "sqsg_run_info",
+)
+
+
+class NativeError(RuntimeError):
+    """A non-OK sqsg_status, with the library's message."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.status_name = STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{self.status_name}: {message}")
+
+
+class SqsgSublattice(C.Structure):
+    _fields_ = [
+        ("n_sites", C.c_uint32),
+        ("n_species", C.c_uint32),
+        ("n_shells", C.c_uint32),
+        ("n_pairs", C.c_uint32),
+        ("n_windows", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("pairs", C.c_void_p),
+        ("species", C.c_void_p),
+        ("windows", C.c_void_p),
+        ("prefactors", C.c_void_p),
+        ("pair_weights", C.c_void_p),
+        ("target", C.c_void_p),
+    ]
+
+
+class SqsgStatistics(C.Structure):
+    _fields_ = [
+        ("finished", C.c_uint64),
+        ("working", C.c_uint64),
+        ("best_rank", C.c_uint64),
+        ("best_objective", C.c_double),
+        ("timings_ns", C.c_uint64 * 4),
+    ]
+
+
+CALLBACK = C.CFUNCTYPE(C.c_int, C.POINTER(SqsgStatistics), C.c_void_p)
+
+
+class SqsgJob(C.Structure):
+    _fields_ = [
+        ("prec", C.c_int32),
+        ("iteration_mode", C.c_int32),
+        ("sublattice_mode", C.c_int32),
+        ("n_sublattices", C.c_uint32),
+        ("sublattices", C.c_void_p),
+        ("iterations", C.c_uint64),
+        ("chunk_size", C.c_uint64),
+        ("keep", C.c_uint64),
+        ("max_results_per_objective", C.c_int64),
+        ("seed", C.c_uint64),
+        ("has_seed", C.c_int32),
+        ("device", C.c_int32),
+        ("cancel", C.c_void_p),
+        ("callback", CALLBACK),
+        ("user", C.c_void_p),
+        ("max_results", C.c_uint64),
+    ]
+
+
+_LIB = None
+_LOCK = threading.Lock()
+
+
+def lib():
+    """Load the native library (raises when it has not been built)."""
+    global _LIB
+    with _LOCK:
+        if _LIB is not None:
+            return _LIB
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python sqsgenerator_b200/build.py` "
+                "(there is no CPU fallback)"
+            )
+        L = C.CDLL(LIB_PATH)
+        L.sqsg_version.restype = C.c_char_p
+        L.sqsg_last_error.restype = C.c_size_t
+        L.sqsg_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        L.sqsg_device_count.restype = C.c_int
+        vp, u32, u64, dbl = C.c_void_p, C.c_uint32, C.c_uint64, C.c_double
+        L.sqsg_supercell.argtypes = [C.c_int, vp, vp, vp, u32, u32, u32, u32, vp, vp, vp]
+        L.sqsg_distance_matrix.argtypes = [C.c_int, vp, vp, u32, vp]
+        L.sqsg_shell_matrix.argtypes = [C.c_int, vp, u32, vp, u32, dbl, dbl, vp]
+        L.sqsg_distances_naive.argtypes = [C.c_int, vp, u32, dbl, dbl, vp, C.POINTER(u32)]
+        L.sqsg_distances_histogram.argtypes = [C.c_int, vp, u32, dbl, dbl, vp, C.POINTER(u32)]
+        L.sqsg_prefactors.argtypes = [C.c_int, vp, u32, vp, u32, vp, vp]
+        L.sqsg_pairs.argtypes = [vp, u32, vp, u32, vp, C.POINTER(u32)]
+        L.sqsg_sort_by_sublattice.argtypes = [vp, u32, u32, vp, vp, C.POINTER(u32)]
+        L.sqsg_num_permutations.argtypes = [vp, u32, C.POINTER(u64)]
+        L.sqsg_rank_permutation.argtypes = [vp, u32, C.POINTER(u64)]
+        L.sqsg_unrank_permutation.argtypes = [vp, u32, u64]
+        L.sqsg_optimize.argtypes = [C.POINTER(SqsgJob), C.POINTER(vp)]
+        L.sqsg_optimize_batch.argtypes = [C.POINTER(SqsgJob), u32, C.POINTER(vp)]
+        L.sqsg_optimize_trace.argtypes = [C.POINTER(SqsgJob), C.POINTER(vp), u64, C.POINTER(u64), vp, vp, vp, vp]
+        L.sqsg_run_count.restype = u64
+        L.sqsg_run_count.argtypes = [vp]
+        L.sqsg_run_copy.argtypes = [vp, u64, u64, vp, vp, vp, vp, vp]
+        L.sqsg_run_statistics.argtypes = [vp, C.POINTER(SqsgStatistics)]
+        L.sqsg_run_free.argtypes = [vp]
+        L.sqsg_run_levels.argtypes = [vp, C.POINTER(u32), vp, vp, vp]
+        L.sqsg_run_info.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        for name in EXPORTED:
+            if name not in ("sqsg_version", "sqsg_last_error", "sqsg_device_count", "sqsg_run_count",
+                            "sqsg_run_free"):
+                getattr(L, name).restype = C.c_int
+        _LIB = L
+        return _LIB
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().sqsg_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != SQSG_OK:
+        raise NativeError(status, last_error())
+
+
+def ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def prec_code(dtype) -> int:
+    return 1 if np.dtype(dtype) == np.float64 else 0
+
+
+def device_count() -> int:
+    return int(lib().sqsg_device_count())
+
+
+def version() -> str:
+    return lib().sqsg_version().decode()
+
+
+# ----------------------------------------------------------------------------- geometry wrappers
+def supercell(lattice, frac, species, a, b, c, dtype=np.float64):
+    lattice = np.ascontiguousarray(lattice, dtype=dtype)
+    frac = np.ascontiguousarray(frac, dtype=dtype)
+    species = np.ascontiguousarray(species, dtype=np.uint8)
+    n = len(species)
+    m = n * a * b * c
+    lo = np.zeros((3, 3), dtype=dtype)
+    fo = np.zeros((m, 3), dtype=dtype)
+    so = np.zeros(m, dtype=np.uint8)
+    check(lib().sqsg_supercell(prec_code(dtype), ptr(lattice), ptr(frac), ptr(species), n, a, b, c,
+                               ptr(lo), ptr(fo), ptr(so)))
+    return lo, fo, so
+
+
+def distance_matrix(lattice, frac, dtype=np.float64):
+    lattice = np.ascontiguousarray(lattice, dtype=dtype)
+    frac = np.ascontiguousarray(frac, dtype=dtype)
+    n = frac.shape[0]
+    out = np.zeros((n, n), dtype=dtype)
+    check(lib().sqsg_distance_matrix(prec_code(dtype), ptr(lattice), ptr(frac), n, ptr(out)))
+    return out
+
+
+def shell_matrix(dist, radii, atol, rtol):
+    dist = np.ascontiguousarray(dist)
+    radii = np.ascontiguousarray(radii, dtype=dist.dtype)
+    n = dist.shape[0]
+    out = np.zeros((n, n), dtype=np.uint32)
+    check(lib().sqsg_shell_matrix(prec_code(dist.dtype), ptr(dist), n, ptr(radii), len(radii), float(atol),
+                                  float(rtol), ptr(out)))
+    return out
+
+
+def _radii(fn, dist, a, b):
+    dist = np.ascontiguousarray(dist)
+    n = dist.shape[0]
+    cap = C.c_uint32(max(16, n * n + 1))
+    out = np.zeros(cap.value, dtype=dist.dtype)
+    check(fn(prec_code(dist.dtype), ptr(dist), n, float(a), float(b), ptr(out), C.byref(cap)))
+    return out[: cap.value].copy()
+
+
+def distances_naive(dist, atol, rtol):
+    return _radii(lib().sqsg_distances_naive, dist, atol, rtol)
+
+
+def distances_histogram(dist, bin_width, peak_isolation):
+    return _radii(lib().sqsg_distances_histogram, dist, bin_width, peak_isolation)
+
+
+def prefactors(shells, shell_ids, species, dtype=np.float64):
+    shells = np.ascontiguousarray(shells, dtype=np.uint32)
+    ids = np.ascontiguousarray(sorted(shell_ids), dtype=np.uint32)
+    species = np.ascontiguousarray(species, dtype=np.uint8)
+    K = len(set(species.tolist()))
+    out = np.zeros((len(ids), K, K), dtype=dtype)
+    check(lib().sqsg_prefactors(prec_code(dtype), ptr(shells), shells.shape[0], ptr(ids), len(ids),
+                                ptr(species), ptr(out)))
+    return out
+
+
+def pairs(shells, shell_ids):
+    shells = np.ascontiguousarray(shells, dtype=np.uint32)
+    ids = np.ascontiguousarray(sorted(shell_ids), dtype=np.uint32)
+    n = shells.shape[0]
+    cnt = C.c_uint32(0)
+    check_cap = lib().sqsg_pairs(ptr(shells), n, ptr(ids), len(ids), None, C.byref(cnt))
+    if check_cap not in (SQSG_OK, 3):
+        check(check_cap)
+    out = np.zeros((max(cnt.value, 1), 3), dtype=np.uint32)
+    cap = C.c_uint32(cnt.value)
+    check(lib().sqsg_pairs(ptr(shells), n, ptr(ids), len(ids), ptr(out), C.byref(cap)))
+    return out[: cap.value]
+
+
+def sort_by_sublattice(sublattice_of_site, n_sublattices):
+    s = np.ascontiguousarray(sublattice_of_site, dtype=np.uint32)
+    n = len(s)
+    order = np.zeros(n, dtype=np.uint32)
+    windows = np.zeros((max(n_sublattices, 1) + 1, 2), dtype=np.uint32)
+    nw = C.c_uint32(windows.shape[0])
+    check(lib().sqsg_sort_by_sublattice(ptr(s), n, n_sublattices, ptr(order), ptr(windows), C.byref(nw)))
+    return order, windows[: nw.value].copy()
+
+
+def num_permutations(conf):
+    c = np.ascontiguousarray(conf, dtype=np.uint8)
+    out = C.c_uint64(0)
+    check(lib().sqsg_num_permutations(ptr(c), len(c), C.byref(out)))
+    return int(out.value)
+
+
+def rank_permutation(conf):
+    c = np.ascontiguousarray(conf, dtype=np.uint8)
+    out = C.c_uint64(0)
+    check(lib().sqsg_rank_permutation(ptr(c), len(c), C.byref(out)))
+    return int(out.value)
+
+
+def unrank_permutation(conf, rank):
+    c = np.ascontiguousarray(conf, dtype=np.uint8).copy()
+    check(lib().sqsg_unrank_permutation(ptr(c), len(c), int(rank)))
+    return c

@@ -1,0 +1,936 @@
+// Host driver and C ABI of the SQS engine: validates a job, lays out its device blob, cuts it into
+// tiles, launches the persistent kernel, watches progress/cancellation, and turns the candidate
+// records into the reference's result set.
+//
+// Replaces sqsgen::run_optimization / optimizer<T,IMode,SMode>::run (include/sqsgen/sqs.h:299-634
+// of dgehringer/sqsgenerator 0.5.6). The result set follows include/sqsgen/core/results.h:42-99:
+// distinct configurations keyed by exact objective; see select_results() for the precise rule.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <string>
+#include <thread>
+#include <unordered_set>
+#include <vector>
+
+#include "engine_device.cuh"
+#include "sqsg_internal.h"
+
+namespace sqsg {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+#define CUDA_CHECK(expr)                                                                              \
+  do {                                                                                                \
+    cudaError_t err__ = (expr);                                                                       \
+    if (err__ != cudaSuccess)                                                                         \
+      throw cuda_error(std::string(#expr) + ": " + cudaGetErrorString(err__));                       \
+  } while (0)
+
+static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+static inline uint32_t host_site_off(uint32_t x) { return (x >> 2) * (kBlock * 4) + (x & 3); }
+
+// ------------------------------------------------------------------------------------------------
+// Job preparation (host)
+struct PartMeta {
+  uint32_t N, K, S;
+};
+
+struct PreparedJob {
+  JobDesc desc{};               // device pointers filled at upload
+  std::vector<uint8_t> blob;    // staged sections of all parts
+  std::vector<PartMeta> parts;
+  int prec = 1;
+  bool systematic = false;
+  uint64_t total = 0;           // configurations
+  uint64_t keep = 1;
+  int64_t max_rpo = -1;
+  size_t record_bytes = 0;
+  size_t tsz = 8;               // sizeof(T)
+  uint32_t configs_per_thread = 1;
+  uint64_t max_results = 0;     // caller's record capacity (0 = default)
+};
+
+template <class T> static void copy_cube(std::vector<uint8_t>& blob, size_t off, const void* src, size_t n) {
+  std::memcpy(blob.data() + off, src, n * sizeof(T));
+}
+
+// Pair stream of a part: for each shell s and site i (ascending) a header word (s | cnt << 8), the
+// byte offset of i in a species column, and cnt byte offsets of its neighbours j > i in shell s.
+static std::vector<uint32_t> build_stream(const sqsg_sublattice& sl) {
+  const uint32_t N = sl.n_sites, S = sl.n_shells, P = sl.n_pairs;
+  std::vector<std::vector<uint32_t>> by(static_cast<size_t>(S) * N);
+  std::vector<uint64_t> per_shell(S, 0);
+  for (uint32_t p = 0; p < P; ++p) {
+    uint32_t i = sl.pairs[3 * p], j = sl.pairs[3 * p + 1], s = sl.pairs[3 * p + 2];
+    if (i >= N || j >= N) throw std::out_of_range("pair index out of range");
+    if (s >= S) throw std::out_of_range("pair shell index out of range");
+    if (i == j) throw std::invalid_argument("pair with i == j");
+    if (i > j) std::swap(i, j);  // ordered counts are defined for i < j (structure.h:445-447)
+    by[static_cast<size_t>(s) * N + i].push_back(j);
+    per_shell[s]++;
+  }
+  for (uint32_t s = 0; s < S; ++s)
+    if (per_shell[s] > 0xffffu)
+      throw unsupported_error("a shell holds more than 65535 pairs; the 16-bit bond counters cannot hold it");
+  std::vector<uint32_t> st;
+  st.reserve(P + 2 * static_cast<size_t>(S) * N);
+  for (uint32_t s = 0; s < S; ++s)
+    for (uint32_t i = 0; i < N; ++i) {
+      auto& js = by[static_cast<size_t>(s) * N + i];
+      std::sort(js.begin(), js.end());
+      for (size_t b = 0; b < js.size(); b += kMaxGroup) {
+        uint32_t cnt = static_cast<uint32_t>(std::min<size_t>(kMaxGroup, js.size() - b));
+        st.push_back(s | (cnt << 8));
+        st.push_back(host_site_off(i));
+        for (uint32_t e = 0; e < cnt; ++e) st.push_back(host_site_off(js[b + e]));
+      }
+    }
+  return st;
+}
+
+static uint64_t window_permutations(const sqsg_sublattice& sl, PartDesc& pd) {
+  const uint32_t lo = sl.windows[0], hi = sl.windows[1];
+  uint32_t counts[256] = {0};
+  for (uint32_t x = lo; x < hi; ++x) counts[sl.species[x]]++;
+  uint32_t k = 0;
+  uint32_t dense[kMaxSpecies];
+  for (uint32_t v = 0; v < 256; ++v)
+    if (counts[v]) {
+      if (k >= kMaxSpecies) throw unsupported_error("more than 8 species in the systematic window");
+      pd.unrank_rev[k] = static_cast<uint8_t>(v);
+      pd.unrank_hist[k] = counts[v];
+      dense[k] = counts[v];
+      ++k;
+    }
+  pd.unrank_k = k;
+  uint64_t total = 0;
+  if (!num_permutations_counts(dense, static_cast<int>(k), &total))
+    throw std::out_of_range("The number of permutations to test does not fit in 64 bits");
+  return total;
+}
+
+static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
+  PreparedJob pj;
+  if (job.prec != SQSG_PREC_SINGLE && job.prec != SQSG_PREC_DOUBLE) throw std::invalid_argument("invalid prec");
+  if (job.iteration_mode != SQSG_ITERATION_RANDOM && job.iteration_mode != SQSG_ITERATION_SYSTEMATIC)
+    throw std::invalid_argument("invalid iteration mode");
+  if (job.sublattice_mode != SQSG_SUBLATTICE_INTERACT && job.sublattice_mode != SQSG_SUBLATTICE_SPLIT)
+    throw std::invalid_argument("invalid sublattice mode");
+  if (!job.sublattices || job.n_sublattices == 0) throw std::invalid_argument("no sublattices");
+  if (job.sublattice_mode == SQSG_SUBLATTICE_INTERACT && job.n_sublattices != 1)
+    throw std::invalid_argument("interact mode takes one optimised structure (windows carry the sublattices)");
+  if (job.n_sublattices > static_cast<uint32_t>(kMaxParts))
+    throw unsupported_error("more than 8 sublattices in split mode");
+  if (job.iteration_mode == SQSG_ITERATION_SYSTEMATIC && job.sublattice_mode == SQSG_SUBLATTICE_SPLIT)
+    throw std::invalid_argument(
+        "It is not possible to do an exhaustive search on multiple sublattices in mode \"split\"");
+  if (job.keep == 0) throw std::invalid_argument("The number of best kept structures must be greater than 0");
+  if (job.keep > 31) throw unsupported_error("keep > 31 is not supported by the warp-level best list");
+  pj.prec = job.prec;
+  pj.tsz = job.prec == SQSG_PREC_DOUBLE ? 8 : 4;
+  pj.systematic = job.iteration_mode == SQSG_ITERATION_SYSTEMATIC;
+  pj.keep = job.keep;
+  pj.max_rpo = job.max_results_per_objective;
+  pj.max_results = job.max_results;
+  JobDesc& d = pj.desc;
+  d.prec = static_cast<uint32_t>(job.prec);
+  d.mode = pj.systematic ? 1 : 0;
+  d.n_parts = job.n_sublattices;
+  d.keep = static_cast<uint32_t>(job.keep);
+  d.kw = 1;
+
+  size_t blob_size = 0, smem = 0;
+  size_t rec = 16, tsp = 0, tbd = 0;
+  std::vector<std::vector<uint32_t>> streams(job.n_sublattices);
+  for (uint32_t p = 0; p < job.n_sublattices; ++p) {
+    const sqsg_sublattice& sl = job.sublattices[p];
+    PartDesc& P = d.parts[p];
+    if (sl.n_sites == 0) throw std::invalid_argument("empty structure");
+    if (sl.n_species == 0 || sl.n_shells == 0) throw std::out_of_range("no coordination shells selected");
+    if (sl.n_species > static_cast<uint32_t>(kMaxSpecies))
+      throw unsupported_error("more than 8 species in one optimised structure");
+    if (sl.n_shells > 255) throw unsupported_error("more than 255 shells");
+    if (!sl.species || !sl.prefactors || !sl.pair_weights || !sl.target || (sl.n_pairs && !sl.pairs))
+      throw std::invalid_argument("null array in sublattice");
+    if (sl.n_windows == 0 || !sl.windows) throw std::invalid_argument("no shuffle window");
+    if (sl.n_windows > static_cast<uint32_t>(kMaxWindows)) throw unsupported_error("more than 16 shuffle windows");
+    for (uint32_t x = 0; x < sl.n_sites; ++x)
+      if (sl.species[x] >= sl.n_species) throw std::out_of_range("packed species index >= n_species");
+    for (uint32_t w = 0; w < sl.n_windows; ++w) {
+      if (sl.windows[2 * w] >= sl.windows[2 * w + 1] || sl.windows[2 * w + 1] > sl.n_sites)
+        throw std::out_of_range("invalid shuffle window");
+      if (w > 0 && sl.windows[2 * w] < sl.windows[2 * w - 1]) throw std::invalid_argument("overlapping windows");
+    }
+    if (pj.systematic && sl.n_windows != 1)
+      throw std::invalid_argument("In \"systematic\" iteration mode only one sublattice is allowed");
+    P.n_sites = sl.n_sites;
+    P.n_species = sl.n_species;
+    P.n_shells = sl.n_shells;
+    P.n_windows = sl.n_windows;
+    P.hw = (sl.n_species + 1) / 2;
+    if (sl.n_species > 4) d.kw = 2;
+    streams[p] = build_stream(sl);
+    P.stream_words = static_cast<uint32_t>(streams[p].size());
+    const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
+    // staged section layout: cubes | windows | stream | species codes
+    size_t off = 0;
+    P.cube_off = 0;
+    off = align_up(3 * skk * pj.tsz, 16);
+    P.win_off = static_cast<uint32_t>(off);
+    off = align_up(off + 8ull * sl.n_windows, 16);
+    P.stream_off = static_cast<uint32_t>(off);
+    off = align_up(off + 4ull * streams[p].size(), 16);
+    P.species_off = static_cast<uint32_t>(off);
+    off = align_up(off + sl.n_sites, 16);
+    P.static_bytes = static_cast<uint32_t>(off);
+    P.blob_off = static_cast<uint32_t>(blob_size);
+    blob_size += off;
+    // shared memory: staged section, species columns, histogram
+    P.smem_off = static_cast<uint32_t>(smem);
+    P.col_off = static_cast<uint32_t>(off);
+    off += static_cast<size_t>((sl.n_sites + 3) / 4) * kBlock * 4;
+    P.hist_off = static_cast<uint32_t>(off);
+    off += static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw * kBlock * 4;
+    smem += align_up(off, 16);
+    // candidate record layout
+    P.rec_species_off = static_cast<uint32_t>(rec);
+    rec = align_up(rec + sl.n_sites, 8);
+    P.rec_obj_off = static_cast<uint32_t>(rec);
+    rec += 8;
+    P.rec_sro_off = static_cast<uint32_t>(rec);
+    rec = align_up(rec + skk * pj.tsz, 8);
+    P.trace_species_off = static_cast<uint32_t>(tsp);
+    tsp += sl.n_sites;
+    P.trace_bonds_off = static_cast<uint32_t>(tbd);
+    tbd += skk;
+    pj.parts.push_back(PartMeta{sl.n_sites, sl.n_species, sl.n_shells});
+    if (pj.systematic) pj.total = window_permutations(sl, P);
+  }
+  if (!pj.systematic) pj.total = job.iterations;
+  d.total = pj.total;
+  d.record_bytes = static_cast<uint32_t>(align_up(rec, 16));
+  pj.record_bytes = d.record_bytes;
+  d.smem_bytes = static_cast<uint32_t>(smem);
+  d.trace = trace_capacity > 0 ? 1 : 0;
+  d.trace_capacity = trace_capacity;
+  d.trace_species_stride = static_cast<uint32_t>(tsp);
+  d.trace_bonds_stride = static_cast<uint32_t>(tbd);
+  if (job.has_seed) {
+    d.seed = job.seed;
+  } else {
+    std::random_device rd;  // core/shuffle.h:16-21 draws an unseeded run's seed the same way
+    d.seed = (static_cast<uint64_t>(rd()) << 32) ^ rd();
+  }
+  pj.blob.assign(blob_size, 0);
+  for (uint32_t p = 0; p < job.n_sublattices; ++p) {
+    const sqsg_sublattice& sl = job.sublattices[p];
+    const PartDesc& P = d.parts[p];
+    const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
+    uint8_t* base = pj.blob.data() + P.blob_off;
+    std::memcpy(base + P.cube_off, sl.prefactors, skk * pj.tsz);
+    std::memcpy(base + P.cube_off + skk * pj.tsz, sl.pair_weights, skk * pj.tsz);
+    std::memcpy(base + P.cube_off + 2 * skk * pj.tsz, sl.target, skk * pj.tsz);
+    std::memcpy(base + P.win_off, sl.windows, 8ull * sl.n_windows);
+    std::memcpy(base + P.stream_off, streams[p].data(), 4ull * streams[p].size());
+    for (uint32_t x = 0; x < sl.n_sites; ++x) base[P.species_off + x] = static_cast<uint8_t>(sl.species[x] << 3);
+  }
+  return pj;
+}
+
+// Tiles depend only on the job, never on the device, so a seeded run evaluates the same
+// configurations on every GPU: about 16384 tiles of kBlock threads, each thread running
+// configs_per_thread configurations.
+static void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles) {
+  const uint64_t total = pj.total;
+  if (total == 0) return;
+  const uint64_t per_tile_target = (total + 16383) / 16384;
+  uint64_t cpt = std::max<uint64_t>(1, (per_tile_target + kBlock - 1) / kBlock);
+  cpt = std::min<uint64_t>(cpt, 1u << 16);
+  pj.configs_per_thread = static_cast<uint32_t>(cpt);
+  const uint64_t tile_configs = cpt * kBlock;
+  uint64_t start = 0, chain = 0;
+  while (start < total) {
+    Tile t{};
+    t.job = job_index;
+    t.count = std::min(tile_configs, total - start);
+    t.start = pj.systematic ? start + 1 : start;
+    t.chain_base = chain;
+    tiles.push_back(t);
+    start += t.count;
+    chain += kBlock;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Device workspaces: grow-only buffers and streams, pooled per device.
+struct DevBuf {
+  void* p = nullptr;
+  size_t size = 0;
+  void ensure(size_t n) {
+    if (n <= size) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    size = 0;
+    CUDA_CHECK(cudaMalloc(&p, n));
+    size = n;
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+struct Workspace {
+  int device = 0;
+  cudaStream_t stream = nullptr, monitor = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  DevBuf blob, records, counters, levels, tiles, jobs, queue, status, trace_sp, trace_bd, trace_obj, trace_id;
+  int32_t* ctrl_host = nullptr;  // mapped pinned: [0] = cancel
+  int32_t* ctrl_dev = nullptr;
+  unsigned long long* mirror = nullptr;  // pinned copy of counters for progress
+  explicit Workspace(int dev) : device(dev) {
+    CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CUDA_CHECK(cudaStreamCreateWithFlags(&monitor, cudaStreamNonBlocking));
+    CUDA_CHECK(cudaEventCreate(&ev_start));
+    CUDA_CHECK(cudaEventCreate(&ev_stop));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&ctrl_host), 64, cudaHostAllocMapped));
+    CUDA_CHECK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctrl_dev), ctrl_host, 0));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&mirror), 64 * kNumCounters * sizeof(unsigned long long), 0));
+    std::memset(ctrl_host, 0, 64);
+  }
+  ~Workspace() {
+    if (stream) cudaStreamDestroy(stream);
+    if (monitor) cudaStreamDestroy(monitor);
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_stop) cudaEventDestroy(ev_stop);
+    if (ctrl_host) cudaFreeHost(ctrl_host);
+    if (mirror) cudaFreeHost(mirror);
+  }
+};
+
+class WorkspacePool {
+ public:
+  std::unique_ptr<Workspace> acquire(int device) {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      auto& v = free_[device];
+      if (!v.empty()) {
+        auto w = std::move(v.back());
+        v.pop_back();
+        return w;
+      }
+    }
+    return std::make_unique<Workspace>(device);
+  }
+  void release(std::unique_ptr<Workspace> w) {
+    std::lock_guard<std::mutex> l(m_);
+    free_[w->device].push_back(std::move(w));
+  }
+
+ private:
+  std::mutex m_;
+  std::map<int, std::vector<std::unique_ptr<Workspace>>> free_;
+};
+
+static WorkspacePool& pool() {
+  static auto* p = new WorkspacePool();  // never destroyed: avoids CUDA calls during exit
+  return *p;
+}
+
+struct WorkspaceLease {
+  std::unique_ptr<Workspace> w;
+  explicit WorkspaceLease(int device) : w(pool().acquire(device)) {}
+  ~WorkspaceLease() {
+    if (w) pool().release(std::move(w));
+  }
+  Workspace* operator->() { return w.get(); }
+};
+
+static int device_sm_count(int dev) {
+  int n = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  return n;
+}
+
+static void configure_kernel(size_t smem) {
+  static std::mutex m;
+  static size_t configured = 0;
+  std::lock_guard<std::mutex> l(m);
+  if (smem > configured) {
+    CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    configured = smem;
+  }
+}
+
+static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles) {
+  configure_kernel(smem);
+  int per_sm = 0;
+  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sqsg_engine, kBlock, smem));
+  if (per_sm <= 0) throw unsupported_error("the job needs more shared memory than one SM offers");
+  size_t grid = static_cast<size_t>(per_sm) * device_sm_count(dev);
+  return static_cast<uint32_t>(std::max<size_t>(1, std::min(grid, n_tiles)));
+}
+
+static size_t max_dynamic_smem(int dev) {
+  int v = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes attr{};
+  CUDA_CHECK(cudaFuncGetAttributes(&attr, sqsg_engine));
+  return static_cast<size_t>(v) - attr.sharedSizeBytes;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Results
+template <class T> static T read_t(const uint8_t* p) {
+  T v;
+  std::memcpy(&v, p, sizeof(T));
+  return v;
+}
+
+struct Run {
+  int prec = 1;
+  uint32_t n_parts = 1;
+  std::vector<PartMeta> parts;
+  size_t tsz = 8;
+  uint64_t count = 0;
+  std::vector<uint8_t> objective, sub_objective, sro;  // raw T bytes
+  std::vector<uint8_t> species;
+  std::vector<uint64_t> id;
+  sqsg_statistics stats{};
+  // keep+1 best distinct objectives with evaluation counts and id checksums (exact unless
+  // levels_exact is false), and whether the record set was cut at the capacity.
+  std::vector<double> level_value;
+  std::vector<uint64_t> level_count, level_checksum;
+  bool truncated = false, levels_exact = true;
+  uint64_t candidates = 0;
+};
+
+// The reference accepts a configuration when its objective is <= the search threshold, which only
+// ever falls to nth_best(keep) — the (keep+1)-th best distinct objective in the collection
+// (sqs.h:421-438, results.h:78-82) — and never evicts. Every configuration at or below the final
+// (keep+1)-th best distinct objective T* is therefore in the reference's result set on every run;
+// entries above T* depend on thread timing. The result set here is exactly the deterministic part:
+// all distinct configurations with objective <= T* (T* = +inf with fewer distinct objectives),
+// sorted by objective then id, at most max_results_per_objective+1 per objective (sqs.h:423-426
+// admits one more than the cap).
+template <class T>
+static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& recs, uint64_t n, Run& run,
+                           bool have_tstar, double tstar_levels) {
+  const size_t rb = pj.record_bytes;
+  std::vector<uint64_t> order(n);
+  for (uint64_t i = 0; i < n; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) {
+    const T oa = read_t<T>(&recs[a * rb]), ob = read_t<T>(&recs[b * rb]);
+    if (oa != ob) return oa < ob;
+    return read_t<uint64_t>(&recs[a * rb + 8]) < read_t<uint64_t>(&recs[b * rb + 8]);
+  });
+  T tstar = std::numeric_limits<T>::infinity();
+  if (have_tstar) {
+    tstar = static_cast<T>(tstar_levels);
+  } else {
+    uint64_t distinct = 0;
+    bool have = false;
+    T last = T(0);
+    for (uint64_t k = 0; k < n; ++k) {
+      const T o = read_t<T>(&recs[order[k] * rb]);
+      if (!have || o != last) {
+        if (distinct == pj.keep) {
+          tstar = o;
+          break;
+        }
+        ++distinct;
+        last = o;
+        have = true;
+      }
+    }
+  }
+  const JobDesc& d = pj.desc;
+  size_t sp_total = 0, sro_total = 0;
+  for (auto& p : pj.parts) {
+    sp_total += p.N;
+    sro_total += static_cast<size_t>(p.S) * p.K * p.K;
+  }
+  std::unordered_set<std::string> seen;
+  T cur_obj = T(0);
+  bool have_cur = false;
+  uint64_t cur_count = 0;
+  std::string key;
+  for (uint64_t k = 0; k < n; ++k) {
+    const uint8_t* r = &recs[order[k] * rb];
+    const T o = read_t<T>(r);
+    if (!(o <= tstar)) break;
+    key.clear();
+    for (uint32_t p = 0; p < d.n_parts; ++p)
+      key.append(reinterpret_cast<const char*>(r + d.parts[p].rec_species_off), d.parts[p].n_sites);
+    if (!seen.insert(key).second) continue;
+    if (!have_cur || o != cur_obj) {
+      cur_obj = o;
+      have_cur = true;
+      cur_count = 0;
+    }
+    if (pj.max_rpo >= 0 && cur_count > static_cast<uint64_t>(pj.max_rpo)) continue;
+    ++cur_count;
+    run.objective.insert(run.objective.end(), r, r + sizeof(T));
+    for (uint32_t p = 0; p < d.n_parts; ++p) {
+      const PartDesc& P = d.parts[p];
+      run.sub_objective.insert(run.sub_objective.end(), r + P.rec_obj_off, r + P.rec_obj_off + sizeof(T));
+      run.species.insert(run.species.end(), r + P.rec_species_off, r + P.rec_species_off + P.n_sites);
+      const size_t skk = static_cast<size_t>(P.n_shells) * P.n_species * P.n_species;
+      run.sro.insert(run.sro.end(), r + P.rec_sro_off, r + P.rec_sro_off + skk * sizeof(T));
+    }
+    run.id.push_back(read_t<uint64_t>(r + 8));
+    run.count++;
+  }
+  (void)sp_total;
+  (void)sro_total;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Executing prepared jobs on one device.
+struct TraceOut {
+  uint64_t capacity = 0;
+  uint64_t* count = nullptr;
+  uint8_t* species = nullptr;
+  uint32_t* bonds = nullptr;
+  void* objective = nullptr;
+  uint64_t* id = nullptr;
+};
+
+static uint64_t now_ns() {
+  return static_cast<uint64_t>(
+      std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+          .count());
+}
+
+// Runs a set of prepared jobs in one persistent launch (one job = the plain path). Returns once
+// every job finished, was cancelled, or a device error was raised.
+static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_job*>& srcs, int device,
+                    std::vector<Run>& runs, const TraceOut* trace) {
+  const uint64_t t0 = now_ns();
+  CUDA_CHECK(cudaSetDevice(device));
+  WorkspaceLease ws(device);
+  const size_t nj = pjs.size();
+  const size_t smem_limit = max_dynamic_smem(device);
+  size_t smem = 0, blob_total = 0;
+  std::vector<size_t> blob_off(nj), rec_off(nj);
+  std::vector<uint64_t> capacity(nj);
+  size_t rec_total = 0;
+  for (size_t j = 0; j < nj; ++j) {
+    if (pjs[j].desc.smem_bytes > smem_limit)
+      throw unsupported_error("the job needs " + std::to_string(pjs[j].desc.smem_bytes) +
+                              " bytes of shared memory per CTA; this device offers " + std::to_string(smem_limit));
+    smem = std::max<size_t>(smem, pjs[j].desc.smem_bytes);
+    blob_off[j] = blob_total;
+    blob_total = align_up(blob_total + pjs[j].blob.size(), 256);
+    const uint64_t budget = (512ull << 20) / pjs[j].record_bytes;
+    capacity[j] = pjs[j].max_results ? pjs[j].max_results : std::max<uint64_t>(1024, std::min<uint64_t>(1u << 20, budget));
+  }
+  std::vector<Tile> tiles;
+  for (size_t j = 0; j < nj; ++j) make_tiles(pjs[j], static_cast<uint32_t>(j), tiles);
+
+  const uint64_t t_setup = now_ns();
+  float loop_ms_total = 0.f;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    rec_total = 0;
+    for (size_t j = 0; j < nj; ++j) {
+      rec_off[j] = rec_total;
+      rec_total = align_up(rec_total + capacity[j] * pjs[j].record_bytes, 256);
+    }
+    ws->blob.ensure(std::max<size_t>(blob_total, 256));
+    ws->records.ensure(std::max<size_t>(rec_total, 256));
+    ws->counters.ensure(nj * kNumCounters * sizeof(unsigned long long));
+    ws->levels.ensure(nj * kLevelSlots * sizeof(LevelSlot));
+    ws->tiles.ensure(std::max<size_t>(tiles.size(), 1) * sizeof(Tile));
+    ws->jobs.ensure(nj * sizeof(JobDesc));
+    ws->queue.ensure(sizeof(QueueCtl));
+    ws->status.ensure(sizeof(unsigned long long));
+    auto* counters = static_cast<unsigned long long*>(ws->counters.p);
+    std::vector<unsigned long long> init(nj * kNumCounters, 0);
+    std::vector<JobDesc> descs(nj);
+    for (size_t j = 0; j < nj; ++j) {
+      JobDesc d = pjs[j].desc;
+      d.blob = static_cast<const uint8_t*>(ws->blob.p) + blob_off[j];
+      d.records = static_cast<uint8_t*>(ws->records.p) + rec_off[j];
+      d.capacity = capacity[j];
+      d.counters = counters + j * kNumCounters;
+      d.levels = static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots;
+      const double maxv = pjs[j].prec == 1 ? std::numeric_limits<double>::max()
+                                           : static_cast<double>(std::numeric_limits<float>::max());
+      init[j * kNumCounters + kThreshold] = ord_bits(maxv);
+      init[j * kNumCounters + kBest] = ord_bits(std::numeric_limits<double>::infinity());
+      if (trace && trace->capacity) {
+        const size_t sp = d.trace_species_stride, bd = d.trace_bonds_stride;
+        ws->trace_sp.ensure(std::max<size_t>(trace->capacity * sp, 16));
+        ws->trace_bd.ensure(std::max<size_t>(trace->capacity * bd * 4, 16));
+        ws->trace_obj.ensure(std::max<size_t>(trace->capacity * pjs[j].tsz, 16));
+        ws->trace_id.ensure(std::max<size_t>(trace->capacity * 8, 16));
+        d.trace_species = static_cast<uint8_t*>(ws->trace_sp.p);
+        d.trace_bonds = static_cast<uint32_t*>(ws->trace_bd.p);
+        d.trace_obj = ws->trace_obj.p;
+        d.trace_id = static_cast<uint64_t*>(ws->trace_id.p);
+      }
+      descs[j] = d;
+      CUDA_CHECK(cudaMemcpyAsync(static_cast<uint8_t*>(ws->blob.p) + blob_off[j], pjs[j].blob.data(),
+                                 pjs[j].blob.size(), cudaMemcpyHostToDevice, ws->stream));
+    }
+    CUDA_CHECK(cudaMemcpyAsync(counters, init.data(), init.size() * sizeof(unsigned long long),
+                               cudaMemcpyHostToDevice, ws->stream));
+    CUDA_CHECK(cudaMemcpyAsync(ws->jobs.p, descs.data(), nj * sizeof(JobDesc), cudaMemcpyHostToDevice, ws->stream));
+    if (!tiles.empty())
+      CUDA_CHECK(cudaMemcpyAsync(ws->tiles.p, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                                 ws->stream));
+    CUDA_CHECK(cudaMemsetAsync(ws->levels.p, 0, nj * kLevelSlots * sizeof(LevelSlot), ws->stream));
+    CUDA_CHECK(cudaMemsetAsync(ws->queue.p, 0, sizeof(QueueCtl), ws->stream));
+    CUDA_CHECK(cudaMemsetAsync(ws->status.p, 0, sizeof(unsigned long long), ws->stream));
+    ws->ctrl_host[0] = 0;
+
+    const uint32_t grid = launch_grid(device, smem, tiles.size());
+    CUDA_CHECK(cudaEventRecord(ws->ev_start, ws->stream));
+    if (!tiles.empty()) {
+      sqsg_engine<<<grid, kBlock, smem, ws->stream>>>(
+          static_cast<const JobDesc*>(ws->jobs.p), static_cast<const Tile*>(ws->tiles.p),
+          static_cast<uint32_t>(tiles.size()), static_cast<QueueCtl*>(ws->queue.p), ws->ctrl_dev,
+          static_cast<unsigned long long*>(ws->status.p));
+      CUDA_CHECK(cudaGetLastError());
+    }
+    CUDA_CHECK(cudaEventRecord(ws->ev_stop, ws->stream));
+
+    // Watch progress: cancellation flags and progress callbacks are served from this thread.
+    std::vector<uint64_t> next_cb(nj, 0);
+    for (size_t j = 0; j < nj; ++j) {
+      const uint64_t chunk = srcs[j]->chunk_size ? srcs[j]->chunk_size : 100000;
+      next_cb[j] = chunk;
+    }
+    bool any_watch = false;
+    for (size_t j = 0; j < nj; ++j) any_watch |= srcs[j]->cancel != nullptr || srcs[j]->callback != nullptr;
+    while (true) {
+      cudaError_t q = cudaEventQuery(ws->ev_stop);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) CUDA_CHECK(q);
+      if (!any_watch) {
+        CUDA_CHECK(cudaEventSynchronize(ws->ev_stop));
+        break;
+      }
+      std::this_thread::sleep_for(std::chrono::microseconds(500));
+      bool stop = false;
+      for (size_t j = 0; j < nj; ++j)
+        if (srcs[j]->cancel && *srcs[j]->cancel) stop = true;
+      bool need_cb = false;
+      for (size_t j = 0; j < nj; ++j) need_cb |= srcs[j]->callback != nullptr;
+      if (need_cb) {
+        CUDA_CHECK(cudaMemcpyAsync(ws->mirror, counters, nj * kNumCounters * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, ws->monitor));
+        CUDA_CHECK(cudaStreamSynchronize(ws->monitor));
+        for (size_t j = 0; j < nj; ++j) {
+          if (!srcs[j]->callback) continue;
+          const uint64_t fin = ws->mirror[j * kNumCounters + kFinished];
+          if (fin < next_cb[j]) continue;
+          const uint64_t chunk = srcs[j]->chunk_size ? srcs[j]->chunk_size : 100000;
+          while (next_cb[j] <= fin) next_cb[j] += chunk;
+          sqsg_statistics st{};
+          st.finished = fin;
+          st.working = pjs[j].total > fin ? pjs[j].total - fin : 0;
+          st.best_objective = from_ord(ws->mirror[j * kNumCounters + kBest]);
+          st.timings_ns[SQSG_TIMING_TOTAL] = now_ns() - t0;
+          if (srcs[j]->callback(&st, srcs[j]->user) != 0) stop = true;
+        }
+      }
+      if (stop) ws->ctrl_host[0] = 1;
+    }
+    CUDA_CHECK(cudaGetLastError());
+    float ms = 0.f;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
+    loop_ms_total += ms;
+    std::vector<unsigned long long> cnt(nj * kNumCounters);
+    CUDA_CHECK(cudaMemcpy(cnt.data(), counters, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    unsigned long long status = 0;
+    CUDA_CHECK(cudaMemcpy(&status, ws->status.p, sizeof(status), cudaMemcpyDeviceToHost));
+    if (status == kErrStageTimeout) throw timeout_error("shared-memory staging wait timed out on the device");
+    if (status != 0) throw cuda_error("device error code " + std::to_string(status));
+    // A candidate overflow re-runs the job with a larger buffer when the caller left the capacity
+    // to the library and the records fit the memory budget (tiles and Philox counters make the
+    // re-run evaluate the same configurations); otherwise the record set is cut and flagged.
+    bool rerun = false;
+    for (size_t j = 0; j < nj; ++j) {
+      const uint64_t need = cnt[j * kNumCounters + kCandidates];
+      if (need <= capacity[j] || pjs[j].max_results) continue;
+      const uint64_t budget = (4ull << 30) / pjs[j].record_bytes;
+      if (need + need / 4 <= budget && attempt < 2) {
+        capacity[j] = need + need / 4;
+        rerun = true;
+      }
+    }
+    if (rerun) continue;
+
+    const uint64_t t_loop = now_ns();
+    runs.assign(nj, Run{});
+    for (size_t j = 0; j < nj; ++j) {
+      const uint64_t n = std::min<uint64_t>(cnt[j * kNumCounters + kCandidates], capacity[j]);
+      std::vector<uint8_t> recs(n * pjs[j].record_bytes);
+      if (n)
+        CUDA_CHECK(cudaMemcpy(recs.data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], recs.size(),
+                              cudaMemcpyDeviceToHost));
+      Run& r = runs[j];
+      r.prec = pjs[j].prec;
+      r.n_parts = pjs[j].desc.n_parts;
+      r.parts = pjs[j].parts;
+      r.tsz = pjs[j].tsz;
+      // objective levels (exact unless the level table overflowed)
+      std::vector<LevelSlot> lv(kLevelSlots);
+      CUDA_CHECK(cudaMemcpy(lv.data(), static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots,
+                            kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost));
+      std::vector<LevelSlot> used;
+      for (auto& x : lv)
+        if (x.key) used.push_back(x);
+      std::sort(used.begin(), used.end(), [](const LevelSlot& a, const LevelSlot& b) { return a.key < b.key; });
+      r.levels_exact = cnt[j * kNumCounters + kLevelOverflow] == 0;
+      for (size_t k = 0; k < used.size() && k <= pjs[j].keep; ++k) {
+        r.level_value.push_back(from_ord(used[k].key));
+        r.level_count.push_back(used[k].count);
+        r.level_checksum.push_back(static_cast<uint64_t>(used[k].sum_a) | (static_cast<uint64_t>(used[k].sum_b) << 32));
+      }
+      const bool have_tstar = r.levels_exact;
+      const double tstar = used.size() > pjs[j].keep ? from_ord(used[pjs[j].keep].key)
+                                                     : std::numeric_limits<double>::infinity();
+      r.candidates = cnt[j * kNumCounters + kCandidates];
+      r.truncated = r.candidates > capacity[j];
+      const uint64_t stored = std::min<uint64_t>(n, capacity[j]);
+      if (pjs[j].prec == 1)
+        select_results<double>(pjs[j], recs, stored, r, have_tstar, tstar);
+      else
+        select_results<float>(pjs[j], recs, stored, r, have_tstar, tstar);
+      r.stats.finished = cnt[j * kNumCounters + kFinished];
+      r.stats.working = 0;
+      if (r.count) {
+        r.stats.best_objective =
+            pjs[j].prec == 1 ? read_t<double>(r.objective.data()) : static_cast<double>(read_t<float>(r.objective.data()));
+        r.stats.best_rank = r.id[0];
+      } else {
+        r.stats.best_objective = std::numeric_limits<double>::infinity();
+      }
+    }
+    if (trace && trace->capacity) {
+      const PreparedJob& pj = pjs[0];
+      const uint64_t n = std::min<uint64_t>(pj.total, trace->capacity);
+      if (trace->count) *trace->count = pj.total;
+      const JobDesc& d = pj.desc;
+      if (trace->species)
+        CUDA_CHECK(cudaMemcpy(trace->species, ws->trace_sp.p, n * d.trace_species_stride, cudaMemcpyDeviceToHost));
+      if (trace->bonds)
+        CUDA_CHECK(cudaMemcpy(trace->bonds, ws->trace_bd.p, n * d.trace_bonds_stride * 4, cudaMemcpyDeviceToHost));
+      if (trace->objective)
+        CUDA_CHECK(cudaMemcpy(trace->objective, ws->trace_obj.p, n * pj.tsz, cudaMemcpyDeviceToHost));
+      if (trace->id) CUDA_CHECK(cudaMemcpy(trace->id, ws->trace_id.p, n * 8, cudaMemcpyDeviceToHost));
+    }
+    const uint64_t t_end = now_ns();
+    for (auto& r : runs) {
+      r.stats.timings_ns[SQSG_TIMING_TOTAL] = t_end - t0;
+      r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = t_setup - t0;
+      r.stats.timings_ns[SQSG_TIMING_LOOP] = static_cast<uint64_t>(loop_ms_total * 1e6);
+      r.stats.timings_ns[SQSG_TIMING_COMM] = t_end - t_loop;
+    }
+    return;
+  }
+}
+
+}  // namespace sqsg
+
+using namespace sqsg;
+
+struct sqsg_run {
+  Run r;
+};
+
+extern "C" {
+
+const char* sqsg_version(void) { return "sqsgen_b200 0.1.0 (abi 1, sm_100a)"; }
+
+size_t sqsg_last_error(char* buf, size_t len) {
+  const std::string& e = g_last_error;
+  if (buf && len) {
+    size_t n = std::min(len - 1, e.size());
+    std::memcpy(buf, e.data(), n);
+    buf[n] = 0;
+  }
+  return e.size();
+}
+
+int sqsg_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+sqsg_status sqsg_num_permutations(const uint8_t* conf, uint32_t n, uint64_t* out) {
+  return guarded([&] {
+    if ((!conf && n) || !out) throw std::invalid_argument("null pointer");
+    uint32_t counts[256] = {0};
+    for (uint32_t i = 0; i < n; ++i) counts[conf[i]]++;
+    std::vector<uint32_t> dense;
+    for (uint32_t v = 0; v < 256; ++v)
+      if (counts[v]) dense.push_back(counts[v]);
+    if (!num_permutations_counts(dense.data(), static_cast<int>(dense.size()), out))
+      throw std::out_of_range("The number of permutations does not fit in 64 bits");
+  });
+}
+
+sqsg_status sqsg_rank_permutation(const uint8_t* conf, uint32_t n, uint64_t* rank) {
+  return guarded([&] {
+    if ((!conf && n) || !rank) throw std::invalid_argument("null pointer");
+    int k = 0;
+    for (uint32_t i = 0; i < n; ++i) k = std::max(k, conf[i] + 1);
+    uint64_t total;
+    sqsg_status s = sqsg_num_permutations(conf, n, &total);
+    if (s != SQSG_OK) throw std::out_of_range("The number of permutations does not fit in 64 bits");
+    std::vector<uint32_t> hist(std::max(k, 1));
+    *rank = rank_permutation(conf, n, hist.data(), k);
+  });
+}
+
+sqsg_status sqsg_unrank_permutation(uint8_t* conf, uint32_t n, uint64_t rank) {
+  return guarded([&] {
+    if (!conf && n) throw std::invalid_argument("null pointer");
+    uint32_t counts[256] = {0};
+    for (uint32_t i = 0; i < n; ++i) counts[conf[i]]++;
+    std::vector<uint32_t> h;
+    for (uint32_t v = 0; v < 256; ++v)
+      if (counts[v]) h.push_back(counts[v]);
+    uint64_t total;
+    if (!num_permutations_counts(h.data(), static_cast<int>(h.size()), &total))
+      throw std::out_of_range("The number of permutations does not fit in 64 bits");
+    if (rank > total) throw std::out_of_range("The rank is larger than the total number of permutations");
+    uint32_t pos = 0;
+    for (uint32_t i = 0; i < n; i++)
+      for (uint32_t j = 0; j < h.size(); j++) {
+        uint64_t suffix = div_96x32(mul_64x32(total, h[j]), n - i, nullptr);
+        if (rank <= suffix) {
+          conf[pos++] = static_cast<uint8_t>(j);
+          total = suffix;
+          h[j]--;
+          break;
+        }
+        rank -= suffix;
+      }
+  });
+}
+
+static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, const TraceOut* trace) {
+  return guarded([&] {
+    if (!jobs || !out || n == 0) throw std::invalid_argument("null pointer");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      throw cuda_error("no CUDA device is available (the optimiser has no CPU path)");
+    }
+    const int device = jobs[0].device;
+    if (device < 0 || device >= ndev) throw std::invalid_argument("invalid device ordinal");
+    std::vector<PreparedJob> pjs;
+    std::vector<const sqsg_job*> srcs;
+    for (uint32_t j = 0; j < n; ++j) {
+      if (jobs[j].device != device) throw std::invalid_argument("a batch runs on one device");
+      pjs.push_back(prepare(jobs[j], trace ? trace->capacity : 0));
+      srcs.push_back(&jobs[j]);
+    }
+    std::vector<Run> runs;
+    execute(pjs, srcs, device, runs, trace);
+    for (uint32_t j = 0; j < n; ++j) out[j] = new sqsg_run{std::move(runs[j])};
+  });
+}
+
+sqsg_status sqsg_optimize(const sqsg_job* job, sqsg_run** run) { return run_jobs(job, 1, run, nullptr); }
+
+sqsg_status sqsg_optimize_batch(const sqsg_job* jobs, uint32_t n_jobs, sqsg_run** runs) {
+  return run_jobs(jobs, n_jobs, runs, nullptr);
+}
+
+sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t capacity, uint64_t* count,
+                                uint8_t* species, uint32_t* bonds, void* objective, uint64_t* id) {
+  TraceOut t;
+  t.capacity = capacity;
+  t.count = count;
+  t.species = species;
+  t.bonds = bonds;
+  t.objective = objective;
+  t.id = id;
+  if (capacity == 0) {
+    set_error("trace capacity must be positive");
+    return SQSG_ERR_INVALID_ARGUMENT;
+  }
+  sqsg_status s = run_jobs(job, 1, run, &t);
+  if (s == SQSG_OK && count && *count > capacity) {
+    set_error("trace capacity smaller than the number of evaluated configurations");
+    return SQSG_ERR_CAPACITY;
+  }
+  return s;
+}
+
+uint64_t sqsg_run_count(const sqsg_run* run) { return run ? run->r.count : 0; }
+
+sqsg_status sqsg_run_copy(const sqsg_run* run, uint64_t first, uint64_t n, void* objective, void* sub_objectives,
+                          uint8_t* species, void* sro, uint64_t* id) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("null run");
+    const Run& r = run->r;
+    if (first > r.count || n > r.count - first) throw std::out_of_range("record range out of bounds");
+    size_t sp = 0, skk = 0;
+    for (auto& p : r.parts) {
+      sp += p.N;
+      skk += static_cast<size_t>(p.S) * p.K * p.K;
+    }
+    if (objective) std::memcpy(objective, r.objective.data() + first * r.tsz, n * r.tsz);
+    if (sub_objectives)
+      std::memcpy(sub_objectives, r.sub_objective.data() + first * r.n_parts * r.tsz, n * r.n_parts * r.tsz);
+    if (species) std::memcpy(species, r.species.data() + first * sp, n * sp);
+    if (sro) std::memcpy(sro, r.sro.data() + first * skk * r.tsz, n * skk * r.tsz);
+    if (id) std::memcpy(id, r.id.data() + first, n * 8);
+  });
+}
+
+sqsg_status sqsg_run_statistics(const sqsg_run* run, sqsg_statistics* stats) {
+  return guarded([&] {
+    if (!run || !stats) throw std::invalid_argument("null pointer");
+    *stats = run->r.stats;
+  });
+}
+
+void sqsg_run_free(sqsg_run* run) { delete run; }
+
+sqsg_status sqsg_run_levels(const sqsg_run* run, uint32_t* n, double* values, uint64_t* counts,
+                            uint64_t* checksums) {
+  return guarded([&] {
+    if (!run || !n) throw std::invalid_argument("null pointer");
+    const Run& r = run->r;
+    const uint32_t cap = *n;
+    *n = static_cast<uint32_t>(r.level_value.size());
+    if (r.level_value.size() > cap) throw std::length_error("level capacity too small");
+    for (size_t k = 0; k < r.level_value.size(); ++k) {
+      if (values) values[k] = r.level_value[k];
+      if (counts) counts[k] = r.level_count[k];
+      if (checksums) checksums[k] = r.level_checksum[k];
+    }
+  });
+}
+
+sqsg_status sqsg_run_info(const sqsg_run* run, uint64_t* candidates, int32_t* truncated, int32_t* levels_exact) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("null run");
+    if (candidates) *candidates = run->r.candidates;
+    if (truncated) *truncated = run->r.truncated ? 1 : 0;
+    if (levels_exact) *levels_exact = run->r.levels_exact ? 1 : 0;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// Device engine of the SQS optimisation: job/tile descriptors and the persistent tile kernel.
+//
+// One CTA of kBlock threads works on one tile at a time. A tile is a slice of one job's
+// configuration space: in random mode kBlock independent Philox chains, in systematic mode a
+// contiguous interval of 1-based permutation ranks. Every thread owns one configuration at a time,
+// stored as one byte per site in its own column of shared memory. Bond counting walks a per-shell,
+// per-site grouped pair stream that every lane reads at the same address (a shared-memory
+// broadcast), accumulates the species of the neighbours of site i in a packed register row, and adds
+// the row to the lane's private histogram of ordered bond counts (s, species[i], species[j]) —
+// exactly the counts of include/sqsgen/core/optimization.h:74-77. No global atomics in the loop.
+#pragma once
+
+#include <cstdint>
+
+namespace sqsg {
+
+constexpr int kBlock = 128;       // threads per CTA (each owns one configuration)
+constexpr int kMaxParts = 8;      // sublattices of a split-mode job
+constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
+constexpr int kMaxSpecies = 8;    // K per part handled by the packed-row counter
+constexpr int kMaxGroup = 255;    // neighbours per (shell, site) group (8-bit row fields)
+constexpr uint32_t kWaitLimit = 1u << 26;  // bounded mbarrier wait (iterations)
+constexpr int kCtaLevelSlots = 64;       // per-CTA objective-level hash (shared memory)
+constexpr int kLevelSlots = 4096;        // per-job objective-level hash (global memory)
+
+// Counters of one job in device memory (unsigned long long each).
+enum Counter : int {
+  kCandidates = 0,  // candidate records appended (may exceed capacity: overflow)
+  kThreshold = 1,   // ordered bits (double) of the search threshold, atomicMin
+  kFinished = 2,    // configurations evaluated
+  kError = 3,       // device error code (0 = none)
+  kBest = 4,        // ordered bits (double) of the best objective seen, atomicMin
+  kTilesDone = 5,   // tiles completed
+  kLevelOverflow = 6,  // the job's level table ran out of slots
+  kNumCounters = 8
+};
+
+enum DeviceError : unsigned long long { kErrNone = 0, kErrStageTimeout = 1, kErrBadJob = 2 };
+
+// One distinct objective value seen at or below the search threshold, with the number of
+// evaluations that produced it and two order-independent 32-bit sums of hashes of their ids.
+struct LevelSlot {
+  unsigned long long key;    // ord_bits(objective as double); 0 = empty
+  unsigned long long count;
+  unsigned int sum_a, sum_b;
+};
+
+// One optimised structure: the whole cell in interact mode, one sublattice in split mode.
+struct PartDesc {
+  uint32_t n_sites, n_species, n_shells, n_windows;
+  uint32_t hw;            // histogram words per (shell, species) row: ceil(K/2) 16-bit fields pairs
+  uint32_t stream_words;  // words of the grouped pair stream
+  uint32_t blob_off;      // staged section: offset in the job blob (16-byte aligned)
+  uint32_t static_bytes;  // staged section size (multiple of 16)
+  uint32_t smem_off;      // part base in dynamic shared memory
+  // offsets inside the staged section (identical in the blob and in shared memory)
+  uint32_t cube_off;      // prefactors, pair weights, targets: 3 x S*K*K of T
+  uint32_t win_off;       // 2 x n_windows u32
+  uint32_t stream_off;    // stream u32 words
+  uint32_t species_off;   // N packed species codes (8 * species index)
+  // shared-memory-only regions, relative to the part base
+  uint32_t col_off;       // ceil(N/4) * kBlock words of species columns
+  uint32_t hist_off;      // S*K*hw * kBlock words of histogram
+  // candidate record layout
+  uint32_t rec_species_off, rec_obj_off, rec_sro_off;
+  // systematic mode: dense remap of the window values (core/shuffle.h:73-87)
+  uint32_t unrank_k;
+  uint32_t unrank_hist[kMaxSpecies];
+  uint8_t unrank_rev[kMaxSpecies];
+  // bond-trace layout
+  uint32_t trace_species_off, trace_bonds_off;
+};
+
+struct JobDesc {
+  uint32_t prec;          // 0 float, 1 double
+  uint32_t mode;          // 0 random, 1 systematic
+  uint32_t n_parts;
+  uint32_t kw;            // 1: every part has K <= 4 (32-bit row), 2: K <= 8 (64-bit row)
+  uint32_t keep;
+  uint32_t record_bytes;
+  uint32_t smem_bytes;
+  uint32_t trace;         // 1: write every evaluated configuration to the trace buffers
+  uint32_t trace_species_stride, trace_bonds_stride;
+  uint64_t seed;
+  uint64_t total;         // random: configurations; systematic: number of permutations
+  const uint8_t* blob;
+  uint8_t* records;
+  uint64_t capacity;
+  unsigned long long* counters;
+  LevelSlot* levels;      // kLevelSlots
+  uint8_t* trace_species;
+  uint32_t* trace_bonds;
+  void* trace_obj;
+  uint64_t* trace_id;
+  uint64_t trace_capacity;
+  PartDesc parts[kMaxParts];
+};
+
+struct Tile {
+  uint32_t job;
+  uint32_t reserved;
+  uint64_t start;       // random: global index of the tile's first configuration; systematic: first rank
+  uint64_t count;       // configurations in the tile
+  uint64_t chain_base;  // random: Philox chain id of thread 0
+};
+
+// Queue control block for the persistent kernel (device memory, or host-mapped for serving).
+struct QueueCtl {
+  unsigned int head;    // next tile to take (atomicAdd)
+  unsigned int pad[3];
+};
+
+}  // namespace sqsg

@@ -1,0 +1,588 @@
+// Device side of the SQS engine (included once, by engine.cu).
+//
+// Per configuration a thread
+//   1. (random mode) Fisher-Yates-shuffles every window of every part with Philox4x32-10 draws and
+//      the reference's bounded draw p = (x * i) >> 32 (include/sqsgen/core/shuffle.h:28-50);
+//   2. counts ordered bonds (s, species[i], species[j]) over the part's pairs (optimization.h:74-77);
+//   3. evaluates the objective in T with the reference's loop order and no FMA contraction
+//      (optimization.h:79-103), summing parts left to right from T(0) (sqs.h:417-418, fold.h:51-53);
+//   4. takes part in the warp's best-N bookkeeping (results.h:42-99, sqs.h:421-438);
+//   5. (systematic mode) steps to the lexicographically next multiset permutation
+//      (permutation.h:80-102) inside the window.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cstring>
+
+#include "engine.cuh"
+#include "permutation.h"
+#include "philox.cuh"
+
+namespace sqsg {
+
+template <class T> struct FP;
+template <> struct FP<double> {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double cvt(uint32_t n) { return __uint2double_rn(n); }
+  static __device__ __forceinline__ double maxv() { return DBL_MAX; }
+};
+template <> struct FP<float> {
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float cvt(uint32_t n) { return __uint2float_rn(n); }
+  static __device__ __forceinline__ float maxv() { return FLT_MAX; }
+};
+
+// Order-preserving map of doubles onto unsigned 64-bit integers (for atomicMin).
+__host__ __device__ __forceinline__ unsigned long long ord_bits(double x) {
+#ifdef __CUDA_ARCH__
+  unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+#else
+  unsigned long long b;
+  std::memcpy(&b, &x, 8);
+#endif
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
+  unsigned long long b = (u >> 63) ? (u & 0x7fffffffffffffffull) : ~u;
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(static_cast<long long>(b));
+#else
+  double x;
+  std::memcpy(&x, &b, 8);
+  return x;
+#endif
+}
+
+// Byte offset of site x inside a lane's species column: words of four sites are interleaved across
+// the kBlock lanes, so both a uniform site (bond counting) and per-lane random sites (shuffling) hit
+// distinct banks.
+__device__ __forceinline__ uint32_t site_off(uint32_t x) { return (x >> 2) * (kBlock * 4) + (x & 3); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// ------------------------------------------------------------------------------ bulk-copy staging
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Non-multicast 1D bulk copy global -> this CTA's shared memory (TMA unit), completing on bar.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Bounded wait for the phase `parity` of bar; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// ------------------------------------------------------------------------------ per-part kernels
+__device__ __forceinline__ uint8_t* part_base(uint8_t* smem, const PartDesc& P) { return smem + P.smem_off; }
+
+__device__ __forceinline__ void init_column(uint8_t* smem, const PartDesc& P, int t) {
+  const uint32_t* sp = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.species_off);
+  uint32_t* col = reinterpret_cast<uint32_t*>(part_base(smem, P) + P.col_off) + t;
+  const uint32_t words = (P.n_sites + 3) >> 2;
+  for (uint32_t w = 0; w < words; ++w) col[w * kBlock] = sp[w];
+}
+
+// Ordered bond counts of the lane's configuration into its histogram (16-bit fields).
+template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, const PartDesc& P, int t) {
+  uint8_t* part = part_base(smem, P);
+  const uint8_t* col = part + P.col_off + 4 * t;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(part + P.hist_off) + t;
+  const uint32_t* st = reinterpret_cast<const uint32_t*>(part + P.stream_off);
+  const uint32_t K = P.n_species, hw = P.hw, words = P.stream_words;
+  const uint32_t nh = P.n_shells * K * hw;
+  for (uint32_t w = 0; w < nh; ++w) hist[w * kBlock] = 0;
+  uint32_t pos = 0;
+  while (pos < words) {
+    const uint32_t hdr = st[pos];
+    const uint32_t ioff = st[pos + 1];
+    const uint32_t s = hdr & 0xffu, cnt = (hdr >> 8) & 0xffu;
+    const uint32_t ci = col[ioff] >> 3;
+    const uint32_t* js = st + pos + 2;
+    uint32_t* h = hist + ((s * K + ci) * hw) * kBlock;
+    if (KW == 1) {
+      uint32_t row = 0;
+#pragma unroll 4
+      for (uint32_t e = 0; e < cnt; ++e) row += 1u << col[js[e]];
+      h[0] += __byte_perm(row, 0, 0x4140);
+      if (hw > 1) h[kBlock] += __byte_perm(row, 0, 0x4342);
+    } else {
+      unsigned long long row = 0;
+#pragma unroll 4
+      for (uint32_t e = 0; e < cnt; ++e) row += 1ull << col[js[e]];
+      const uint32_t lo = static_cast<uint32_t>(row), hi = static_cast<uint32_t>(row >> 32);
+      h[0] += __byte_perm(lo, 0, 0x4140);
+      if (hw > 1) h[kBlock] += __byte_perm(lo, 0, 0x4342);
+      if (hw > 2) h[2 * kBlock] += __byte_perm(hi, 0, 0x4140);
+      if (hw > 3) h[3 * kBlock] += __byte_perm(hi, 0, 0x4342);
+    }
+    pos += 2 + cnt;
+  }
+}
+
+__device__ __forceinline__ uint32_t bond(const uint32_t* hist, uint32_t K, uint32_t hw, uint32_t s, uint32_t a,
+                                         uint32_t b) {
+  return (hist[((s * K + a) * hw + (b >> 1)) * kBlock] >> ((b & 1u) * 16u)) & 0xffffu;
+}
+
+// core/optimization.h:79-103 on the lane's histogram. With `sro` non-null the SRO cube is written
+// row-major (the reference's sro tensor, symmetric in the species indices).
+template <class T>
+__device__ __forceinline__ T objective_part(uint8_t* smem, const PartDesc& P, int t, T* sro = nullptr) {
+  using F = FP<T>;
+  const uint8_t* part = part_base(smem, P);
+  const uint32_t* hist = reinterpret_cast<const uint32_t*>(part + P.hist_off) + t;
+  const uint32_t S = P.n_shells, K = P.n_species, hw = P.hw, skk = S * K * K;
+  const T* f = reinterpret_cast<const T*>(part + P.cube_off);
+  const T* w = f + skk;
+  const T* tg = w + skk;
+  T obj = T(0);
+  for (uint32_t s = 0; s < S; ++s)
+    for (uint32_t xi = 0; xi < K; ++xi) {
+      const uint32_t d = (s * K + xi) * K + xi;
+      const T sig = F::sub(T(1), F::mul(F::cvt(bond(hist, K, hw, s, xi, xi)), f[d]));
+      if (sro) sro[d] = sig;
+      T diff = F::sub(sig, tg[d]);
+      diff = diff > T(0) ? diff : -diff;
+      obj = F::add(obj, F::mul(w[d], diff));
+      for (uint32_t eta = xi + 1; eta < K; ++eta) {
+        const uint32_t u = (s * K + xi) * K + eta;
+        const uint32_t nb = bond(hist, K, hw, s, xi, eta) + bond(hist, K, hw, s, eta, xi);
+        const T sg = F::sub(T(1), F::mul(F::cvt(nb), f[u]));
+        if (sro) {
+          sro[u] = sg;
+          sro[(s * K + eta) * K + xi] = sg;
+        }
+        T df = F::sub(sg, tg[u]);
+        df = df > T(0) ? df : -df;
+        obj = F::add(obj, F::mul(w[u], df));
+      }
+    }
+  return obj;
+}
+
+__device__ __forceinline__ void swap_draw(uint8_t* col, uint32_t lo, uint32_t i, uint32_t x) {
+  const uint32_t p = __umulhi(x, i);  // (x * i) >> 32, core/shuffle.h:28-32 on a Philox word
+  const uint32_t a = site_off(lo + i - 1), b = site_off(lo + p);
+  const uint8_t va = col[a], vb = col[b];
+  col[a] = vb;
+  col[b] = va;
+}
+
+// core/shuffle.h:39-50 with Philox4x32-10 words: counter (block, iteration, chain, part), key = seed.
+__device__ __forceinline__ void shuffle_part(uint8_t* smem, const PartDesc& P, int t, uint32_t it,
+                                             unsigned long long chain, uint32_t part, uint32_t k0, uint32_t k1) {
+  uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
+  const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
+  const uint32_t c_lo = static_cast<uint32_t>(chain);
+  const uint32_t c_hi = (static_cast<uint32_t>(chain >> 32) << 8) | part;
+  uint32_t blk = 0;
+  for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
+    const uint32_t lo = win[2 * wi];
+    uint32_t i = win[2 * wi + 1] - lo;
+    while (i > 1) {
+      const philox_ctr r = philox4x32_10(philox_ctr{blk++, it, c_lo, c_hi}, k0, k1);
+      swap_draw(col, lo, i, r.x);
+      if (--i <= 1) break;
+      swap_draw(col, lo, i, r.y);
+      if (--i <= 1) break;
+      swap_draw(col, lo, i, r.z);
+      if (--i <= 1) break;
+      swap_draw(col, lo, i, r.w);
+      --i;
+    }
+  }
+}
+
+// core/permutation.h:80-102 on the lane's window bytes.
+__device__ __forceinline__ void next_permutation(uint8_t* col, uint32_t lo, uint32_t n) {
+  if (n < 2) return;
+  int k = static_cast<int>(n) - 2;
+  uint8_t right = col[site_off(lo + n - 1)];
+  uint8_t ak = col[site_off(lo + k)];
+  while (ak >= right) {
+    if (--k < 0) return;
+    right = ak;
+    ak = col[site_off(lo + k)];
+  }
+  int l = static_cast<int>(n) - 1;
+  uint8_t al = col[site_off(lo + l)];
+  while (ak >= al) al = col[site_off(lo + --l)];
+  col[site_off(lo + k)] = al;
+  col[site_off(lo + l)] = ak;
+  for (int a = k + 1, b = static_cast<int>(n) - 1; a < b; ++a, --b) {
+    const uint32_t oa = site_off(lo + a), ob = site_off(lo + b);
+    const uint8_t va = col[oa];
+    col[oa] = col[ob];
+    col[ob] = va;
+  }
+}
+
+// core/permutation.h:52-78 inside the window with the dense remap of core/shuffle.h:73-87.
+__device__ __forceinline__ void unrank_window(uint8_t* col, const PartDesc& P, uint32_t lo, uint32_t n,
+                                              uint64_t rank, uint64_t total) {
+  uint32_t h[kMaxSpecies];
+  const uint32_t k = P.unrank_k;
+  for (uint32_t j = 0; j < kMaxSpecies; ++j) h[j] = P.unrank_hist[j];
+  for (uint32_t i = 0; i < n; ++i) {
+    for (uint32_t j = 0; j < k; ++j) {
+      const uint64_t suffix = div_96x32(mul_64x32(total, h[j]), n - i, nullptr);
+      if (rank <= suffix) {
+        col[site_off(lo + i)] = static_cast<uint8_t>(P.unrank_rev[j] << 3);
+        total = suffix;
+        h[j]--;
+        break;
+      }
+      rank -= suffix;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ objective levels
+// splitmix64 finalizer (Steele, Lea, Flood 2014): the per-id hash behind the order-independent level
+// checksums.
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ uint32_t level_hash(unsigned long long key, uint32_t mask) {
+  return static_cast<uint32_t>(mix64(key)) & mask;
+}
+
+__device__ __forceinline__ void global_level_add(const JobDesc& J, unsigned long long key, unsigned long long count,
+                                                 unsigned int sa, unsigned int sb) {
+  uint32_t h = level_hash(key, kLevelSlots - 1);
+  for (int probe = 0; probe < kLevelSlots; ++probe, h = (h + 1) & (kLevelSlots - 1)) {
+    LevelSlot& slot = J.levels[h];
+    const unsigned long long prev = atomicCAS(&slot.key, 0ull, key);
+    if (prev == 0ull || prev == key) {
+      atomicAdd(&slot.count, count);
+      atomicAdd(&slot.sum_a, sa);
+      atomicAdd(&slot.sum_b, sb);
+      return;
+    }
+  }
+  atomicAdd(&J.counters[kLevelOverflow], 1ull);
+}
+
+__device__ __forceinline__ void cta_level_add(LevelSlot* tab, const JobDesc& J, unsigned long long key,
+                                              unsigned long long count, unsigned int sa, unsigned int sb) {
+  uint32_t h = level_hash(key, kCtaLevelSlots - 1);
+  for (int probe = 0; probe < kCtaLevelSlots; ++probe, h = (h + 1) & (kCtaLevelSlots - 1)) {
+    const unsigned long long prev = atomicCAS(&tab[h].key, 0ull, key);
+    if (prev == 0ull || prev == key) {
+      atomicAdd(&tab[h].count, count);
+      atomicAdd(&tab[h].sum_a, sa);
+      atomicAdd(&tab[h].sum_b, sb);
+      return;
+    }
+  }
+  global_level_add(J, key, count, sa, sb);
+}
+
+// Moves the CTA's level entries that are still at or below the job's threshold into the job table.
+__device__ __forceinline__ void flush_levels(LevelSlot* tab, const JobDesc& J) {
+  for (int i = threadIdx.x; i < kCtaLevelSlots; i += kBlock) {
+    LevelSlot& slot = tab[i];
+    if (slot.key) {
+      const unsigned long long thr = *reinterpret_cast<volatile unsigned long long*>(&J.counters[kThreshold]);
+      if (slot.key <= thr) global_level_add(J, slot.key, slot.count, slot.sum_a, slot.sum_b);
+      slot.key = 0;
+      slot.count = 0;
+      slot.sum_a = 0;
+      slot.sum_b = 0;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ best-N bookkeeping
+// Each warp keeps the up-to-32 best distinct objectives it has seen, one per lane, ascending. Its
+// (keep+1)-th entry bounds the job's (keep+1)-th best distinct objective from above, like the
+// reference's search threshold nth_best(keep) (results.h:78-82, sqs.h:203-206); the minimum over
+// warps is kept in the job's threshold counter. Every configuration whose objective is at or below
+// the current bound is appended to the candidate buffer, so the buffer holds every configuration at
+// or below the final (keep+1)-th best distinct objective.
+struct WarpState {
+  double list;          // lane's entry of the warp list (+inf = empty)
+  double list_thr;      // warp-uniform (keep+1)-th entry
+  unsigned long long published_thr, published_best;
+  __device__ void reset() {
+    list = __longlong_as_double(0x7ff0000000000000ll);
+    list_thr = list;
+    published_thr = ~0ull;
+    published_best = ~0ull;
+  }
+};
+
+template <class T>
+__device__ __forceinline__ void write_record(const JobDesc& J, uint8_t* smem, uint64_t idx, T total, uint64_t id,
+                                             int t) {
+  uint8_t* rec = J.records + idx * J.record_bytes;
+  *reinterpret_cast<T*>(rec) = total;
+  *reinterpret_cast<uint64_t*>(rec + 8) = id;
+  for (uint32_t p = 0; p < J.n_parts; ++p) {
+    const PartDesc& P = J.parts[p];
+    const uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
+    for (uint32_t x = 0; x < P.n_sites; ++x) rec[P.rec_species_off + x] = col[site_off(x)] >> 3;
+    T* sro = reinterpret_cast<T*>(rec + P.rec_sro_off);
+    *reinterpret_cast<T*>(rec + P.rec_obj_off) = objective_part<T>(smem, P, t, sro);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void write_trace(const JobDesc& J, uint8_t* smem, uint64_t g, T total, uint64_t id,
+                                            int t) {
+  if (g >= J.trace_capacity) return;
+  uint8_t* sp = J.trace_species + g * J.trace_species_stride;
+  uint32_t* bd = J.trace_bonds + g * J.trace_bonds_stride;
+  for (uint32_t p = 0; p < J.n_parts; ++p) {
+    const PartDesc& P = J.parts[p];
+    const uint8_t* part = part_base(smem, P);
+    const uint8_t* col = part + P.col_off + 4 * t;
+    const uint32_t* hist = reinterpret_cast<const uint32_t*>(part + P.hist_off) + t;
+    for (uint32_t x = 0; x < P.n_sites; ++x) sp[P.trace_species_off + x] = col[site_off(x)] >> 3;
+    const uint32_t S = P.n_shells, K = P.n_species;
+    for (uint32_t s = 0; s < S; ++s)
+      for (uint32_t a = 0; a < K; ++a)
+        for (uint32_t b = 0; b < K; ++b) bd[P.trace_bonds_off + (s * K + a) * K + b] = bond(hist, K, P.hw, s, a, b);
+  }
+  static_cast<T*>(J.trace_obj)[g] = total;
+  J.trace_id[g] = id;
+}
+
+template <class T>
+__device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, WarpState& ws,
+                                                  bool pass, T total, T thr_g, uint64_t id, int t) {
+  const int lane = t & 31;
+  unsigned m = __ballot_sync(0xffffffffu, pass);
+  if (!m) return;
+  const double v_mine = static_cast<double>(total);
+  unsigned mm = m;
+  while (mm) {
+    const int src = __ffs(mm) - 1;
+    mm &= mm - 1;
+    const double v = __shfl_sync(0xffffffffu, v_mine, src);
+    if (v < ws.list_thr) {
+      if (!__any_sync(0xffffffffu, ws.list == v)) {
+        const int pos = __popc(__ballot_sync(0xffffffffu, ws.list < v));
+        const double up = __shfl_up_sync(0xffffffffu, ws.list, 1);
+        if (lane == pos)
+          ws.list = v;
+        else if (lane > pos)
+          ws.list = up;
+        ws.list_thr = __shfl_sync(0xffffffffu, ws.list, J.keep);
+      }
+    }
+  }
+  if (lane == 0) {
+    const unsigned long long ot = ord_bits(ws.list_thr);
+    if (ot < ws.published_thr) {
+      atomicMin(&J.counters[kThreshold], ot);
+      ws.published_thr = ot;
+    }
+    const unsigned long long ob = ord_bits(ws.list);
+    if (ob < ws.published_best) {
+      atomicMin(&J.counters[kBest], ob);
+      ws.published_best = ob;
+    }
+  }
+  // The refreshed warp bound still dominates the final (keep+1)-th best, so it may filter.
+  const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
+  const bool keep_it = pass && v_mine <= bound;
+  const unsigned km = __ballot_sync(0xffffffffu, keep_it);
+  if (!km) return;
+  // objective levels: one shared-memory update per distinct value per warp
+  {
+    const unsigned long long mykey = ord_bits(v_mine);
+    const unsigned long long h = mix64(id);
+    unsigned pending = km;
+    while (pending) {
+      const int leader = __ffs(pending) - 1;
+      const unsigned long long key = __shfl_sync(0xffffffffu, mykey, leader);
+      const bool in = keep_it && mykey == key;
+      const unsigned gm = __ballot_sync(0xffffffffu, in);
+      const unsigned sa = __reduce_add_sync(0xffffffffu, in ? static_cast<unsigned>(h) : 0u);
+      const unsigned sb = __reduce_add_sync(0xffffffffu, in ? static_cast<unsigned>(h >> 32) : 0u);
+      if (lane == leader) cta_level_add(ctab, J, key, __popc(gm), sa, sb);
+      pending &= ~gm;
+    }
+  }
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(&J.counters[kCandidates], static_cast<unsigned long long>(__popc(km)));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (keep_it) {
+    const uint64_t idx = base + __popc(km & ((1u << lane) - 1u));
+    if (idx < J.capacity) write_record<T>(J, smem, idx, total, id, t);
+  }
+}
+
+template <class T> __device__ __forceinline__ T load_threshold(const JobDesc& J) {
+  const unsigned long long u = *reinterpret_cast<volatile unsigned long long*>(&J.counters[kThreshold]);
+  return static_cast<T>(from_ord(u));
+}
+
+// ------------------------------------------------------------------------------ one tile
+template <class T, int KW>
+__device__ __noinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                      WarpState& ws) {
+  using F = FP<T>;
+  const int t = threadIdx.x;
+  const uint64_t base = tile.count / kBlock, rem = tile.count % kBlock;
+  const uint64_t my_count = base + (static_cast<uint64_t>(t) < rem ? 1 : 0);
+  const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
+  const uint64_t max_count = base + (rem ? 1 : 0);
+  const bool systematic = J.mode == 1;
+  const unsigned long long chain = tile.chain_base + static_cast<unsigned long long>(t);
+  const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
+
+  for (uint32_t p = 0; p < J.n_parts; ++p) init_column(smem, J.parts[p], t);
+  uint32_t wlo = 0, wn = 0;
+  if (systematic) {
+    const PartDesc& P = J.parts[0];
+    const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
+    wlo = win[0];
+    wn = win[1] - win[0];
+    if (my_count > 0)
+      unrank_window(part_base(smem, P) + P.col_off + 4 * t, P, wlo, wn, tile.start + my_off, J.total);
+  }
+  T thr_g = load_threshold<T>(J);
+  for (uint64_t it = 0; it < max_count; ++it) {
+    const bool active = it < my_count;
+    T total = T(0);
+    if (active) {
+      for (uint32_t p = 0; p < J.n_parts; ++p) {
+        const PartDesc& P = J.parts[p];
+        if (!systematic) shuffle_part(smem, P, t, static_cast<uint32_t>(it), chain, p, k0, k1);
+        count_part<KW>(smem, P, t);
+        const T o = objective_part<T>(smem, P, t);
+        total = p == 0 ? o : F::add(total, o);
+      }
+    }
+    if ((it & 15) == 0) thr_g = load_threshold<T>(J);
+    const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
+    const bool pass = active && static_cast<double>(total) <= bound;
+    const uint64_t id = systematic ? tile.start + my_off + it : ((chain << 32) | it);
+    handle_candidates<T>(J, smem, ctab, ws, pass, total, thr_g, id, t);
+    if (J.trace && active) {
+      const uint64_t g = systematic ? tile.start + my_off + it - 1 : tile.start + my_off + it;
+      write_trace<T>(J, smem, g, total, id, t);
+    }
+    if (systematic && active && it + 1 < my_count)
+      next_permutation(part_base(smem, J.parts[0]) + J.parts[0].col_off + 4 * t, wlo, wn);
+  }
+}
+
+// ------------------------------------------------------------------------------ persistent kernel
+// Tiles are taken from q->head with one atomicAdd per tile. A CTA stages a job's read-only data
+// (cubes, windows, pair stream, packed species) into shared memory with non-multicast bulk copies
+// whenever its next tile belongs to a different job.
+__global__ void __launch_bounds__(kBlock) sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
+                                                      uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
+                                                      unsigned long long* status) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ JobDesc sj;
+  __shared__ LevelSlot ctab[kCtaLevelSlots];
+  __shared__ uint32_t s_tile, s_fail;
+  __shared__ __align__(8) uint64_t s_bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    s_fail = 0;
+  }
+  for (int i = threadIdx.x; i < kCtaLevelSlots; i += kBlock) ctab[i] = LevelSlot{0ull, 0ull, 0u, 0u};
+  __syncthreads();
+  int cur = -1;
+  uint32_t phase = 0;
+  WarpState ws;
+  ws.reset();
+  for (;;) {
+    if (threadIdx.x == 0) {
+      uint32_t ti = n_tiles;
+      if (!(cancel && *cancel)) ti = atomicAdd(&q->head, 1u);
+      s_tile = ti;
+    }
+    __syncthreads();
+    const uint32_t ti = s_tile;
+    if (ti >= n_tiles) break;
+    const Tile tile = tiles[ti];
+    if (static_cast<int>(tile.job) != cur) {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(&jobs[tile.job]);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&sj);
+      for (uint32_t i = threadIdx.x; i < sizeof(JobDesc) / 4; i += kBlock) dst[i] = src[i];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        uint32_t bytes = 0;
+        for (uint32_t p = 0; p < sj.n_parts; ++p) bytes += sj.parts[p].static_bytes;
+        mbar_expect_tx(&s_bar, bytes);
+        for (uint32_t p = 0; p < sj.n_parts; ++p)
+          bulk_copy_g2s(smem + sj.parts[p].smem_off, sj.blob + sj.parts[p].blob_off, sj.parts[p].static_bytes,
+                        &s_bar);
+      }
+      if (!mbar_wait(&s_bar, phase)) atomicOr(&s_fail, 1u);
+      phase ^= 1u;
+      __syncthreads();
+      if (s_fail) {
+        if (threadIdx.x == 0) {
+          atomicMax(status, static_cast<unsigned long long>(kErrStageTimeout));
+          atomicMax(&sj.counters[kError], static_cast<unsigned long long>(kErrStageTimeout));
+        }
+        break;
+      }
+      cur = static_cast<int>(tile.job);
+      ws.reset();
+    }
+    if (sj.prec == 1) {
+      if (sj.kw == 1)
+        run_tile<double, 1>(sj, smem, ctab, tile, ws);
+      else
+        run_tile<double, 2>(sj, smem, ctab, tile, ws);
+    } else {
+      if (sj.kw == 1)
+        run_tile<float, 1>(sj, smem, ctab, tile, ws);
+      else
+        run_tile<float, 2>(sj, smem, ctab, tile, ws);
+    }
+    __syncthreads();
+    flush_levels(ctab, sj);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      atomicAdd(&sj.counters[kFinished], static_cast<unsigned long long>(tile.count));
+      atomicAdd(&sj.counters[kTilesDone], 1ull);
+    }
+  }
+}
+
+}  // namespace sqsg

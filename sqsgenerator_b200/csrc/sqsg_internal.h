@@ -1,0 +1,57 @@
+// Internal declarations shared by the host precompute, the device engine and the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <exception>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/sqsgen_b200.h"
+
+namespace sqsg {
+
+void set_error(const std::string& msg);
+
+// An error raised by the CUDA runtime or a device-side status word.
+struct cuda_error : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct unsupported_error : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct timeout_error : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+
+// Runs fn, translating C++ exceptions into an sqsg_status plus the thread's last-error message.
+template <class Fn> sqsg_status guarded(Fn&& fn) {
+  try {
+    fn();
+    return SQSG_OK;
+  } catch (std::out_of_range const& e) {
+    set_error(e.what());
+    return SQSG_ERR_OUT_OF_RANGE;
+  } catch (std::length_error const& e) {
+    set_error(e.what());
+    return SQSG_ERR_CAPACITY;
+  } catch (std::invalid_argument const& e) {
+    set_error(e.what());
+    return SQSG_ERR_INVALID_ARGUMENT;
+  } catch (unsupported_error const& e) {
+    set_error(e.what());
+    return SQSG_ERR_UNSUPPORTED;
+  } catch (timeout_error const& e) {
+    set_error(e.what());
+    return SQSG_ERR_TIMEOUT;
+  } catch (std::bad_alloc const&) {
+    set_error("out of host memory");
+    return SQSG_ERR_CAPACITY;
+  } catch (std::exception const& e) {
+    set_error(e.what());
+    return SQSG_ERR_CUDA;
+  }
+}
+
+}  // namespace sqsg
