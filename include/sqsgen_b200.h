@@ -131,7 +131,7 @@ typedef struct {
 typedef struct {
   uint64_t finished;          /* configurations evaluated */
   uint64_t working;           /* configurations in flight */
-  uint64_t best_rank;         /* systematic: rank of the best; random: (chain << 32) | iteration */
+  uint64_t best_rank;         /* systematic: rank of the best; random: its configuration index */
   double best_objective;
   uint64_t timings_ns[4];     /* SQSG_TIMING_* */
 } sqsg_statistics;
@@ -159,6 +159,9 @@ typedef struct {
   void* user;
   uint64_t max_results;       /* record capacity of the result set (0: library default, grown on demand
                                  within a 4 GiB device budget) */
+  uint64_t range_first;       /* evaluate only configurations [range_first, range_first + range_count) of the */
+  uint64_t range_count;       /* job (0 = to the end): one GPU's share, like optimizer_base::iteration_range
+                                 (include/sqsgen/sqs.h:226-238). Systematic: rank range_first+1 onwards. */
 } sqsg_job;
 
 typedef struct sqsg_run sqsg_run;
@@ -174,7 +177,8 @@ sqsg_status sqsg_optimize(const sqsg_job* job, sqsg_run** run);
 uint64_t sqsg_run_count(const sqsg_run* run);
 /* Copies records [first, first+n). Any output pointer may be NULL. Per record: objective (prec),
  * sub_objectives (n_sublattices, prec), species (sum of N, packed, sorted order), sro
- * (sum of S*K*K, prec, row-major), id (systematic: 1-based rank; random: (chain << 32) | iteration). */
+ * (sum of S*K*K, prec, row-major), id (systematic: 1-based rank; random: 0-based configuration index;
+ * configuration i is the (i - c)-th shuffle of the chain that starts at index c). */
 sqsg_status sqsg_run_copy(const sqsg_run* run, uint64_t first, uint64_t n, void* objective,
                           void* sub_objectives, uint8_t* species, void* sro, uint64_t* id);
 sqsg_status sqsg_run_statistics(const sqsg_run* run, sqsg_statistics* stats);
@@ -190,6 +194,9 @@ sqsg_status sqsg_run_levels(const sqsg_run* run, uint32_t* n, double* values, ui
 /* candidates: records the device appended; truncated: 1 when the record set hit its capacity;
  * levels_exact: 0 when the level table overflowed (then only the records define the result). */
 sqsg_status sqsg_run_info(const sqsg_run* run, uint64_t* candidates, int32_t* truncated, int32_t* levels_exact);
+/* Bytes the call copied host->device (job blob, tiles, descriptors) and device->host (records,
+ * level table, counters). */
+sqsg_status sqsg_run_transfer(const sqsg_run* run, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
 /* Debug/parity trace: like sqsg_optimize, but additionally records every evaluated configuration
  * (at most `capacity`; SQSG_ERR_CAPACITY otherwise) with its packed species, ordered bond counts
@@ -197,6 +204,10 @@ sqsg_status sqsg_run_info(const sqsg_run* run, uint64_t* candidates, int32_t* tr
  * capacity x sum N; bonds capacity x sum S*K*K; objective capacity (prec); id capacity. */
 sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t capacity, uint64_t* count,
                                 uint8_t* species, uint32_t* bonds, void* objective, uint64_t* id);
+
+/* Peak-rate microbenchmarks used as roofline denominators (no reference counterpart).
+ * kind 0: shared-memory load bandwidth (bytes/s); kind 1: 32-bit integer lane operations per second. */
+sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds);
 
 /* ------------------------------------------------------------------------------------------------
  * Batched form: many independent jobs in one persistent launch fed by a device tile queue

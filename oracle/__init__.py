@@ -105,6 +105,11 @@ def lib():
         L.oracle_result_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.oracle_result_get.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_last_error.restype = C.c_char_p
+        L.oracle_sort_by_sublattice.restype = C.c_int
+        L.oracle_sort_by_sublattice.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.oracle_systematic_levels.restype = C.c_int
+        L.oracle_systematic_levels.argtypes = [C.POINTER(Sublattice), C.c_int, C.c_int, C.c_uint64, C.c_uint64,
+                                               C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         _LIB = L
     return _LIB
 
@@ -288,3 +293,32 @@ def optimize(sublattices, *, prec="double", iteration_mode="random", sublattice_
         return out, stats
     finally:
         L.oracle_result_free(h)
+
+
+def systematic_levels(sd, *, prec="double", keep=1, threads=None, first=0, count=0):
+    """Exhaustive enumeration of the single window (ranks first+1 .. first+count, all when count is
+    0): the keep+1 best distinct objectives with their configuration counts and rank checksums
+    (sums of the low / high halves of splitmix64(rank), mod 2^32).
+    """
+    T = np.float64 if prec in ("double", 1, np.float64) else np.float32
+    s, keepalive = make_sublattice(sd, T)
+    cap = int(keep) + 1
+    vals = np.zeros(cap, dtype=np.float64)
+    cnts = np.zeros(cap, dtype=np.uint64)
+    sums = np.zeros(cap, dtype=np.uint64)
+    n = lib().oracle_systematic_levels(C.byref(s), 1 if T is np.float64 else 0, int(threads or os.cpu_count() or 1),
+                                       int(keep), int(first), int(count), _ptr(vals), _ptr(cnts), _ptr(sums), cap)
+    if n < 0:
+        raise RuntimeError(lib().oracle_last_error().decode())
+    return [(float(vals[i]), int(cnts[i]), int(sums[i])) for i in range(n)]
+
+
+def sort_by_sublattice(sl_of_site, n_sublattices):
+    """(sort_order, windows) exactly as the reference's std::sort-based compute_shuffling_bounds."""
+    s = np.ascontiguousarray(sl_of_site, dtype=np.uint32)
+    n = len(s)
+    order = np.zeros(n, dtype=np.uint32)
+    cap = n_sublattices + 2
+    win = np.zeros(2 * cap, dtype=np.uint32)
+    k = lib().oracle_sort_by_sublattice(_ptr(s), n, int(n_sublattices), _ptr(order), _ptr(win), cap)
+    return order.tolist(), [(int(win[2 * i]), int(win[2 * i + 1])) for i in range(k)]

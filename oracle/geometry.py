@@ -253,28 +253,16 @@ def apply_composition(species, composition):
 def shuffling_bounds(n_sites, composition):
     """``core/optimization.h:35-72`` — sort sites by sublattice index and cut windows.
 
-    The reference sorts with ``std::sort`` (not stable). The permutation of equal keys only
-    relabels sites inside a window; tests compare everything in original site order.
+    The reference sorts with libstdc++ ``std::sort`` (not stable), which permutes sites with equal
+    keys; the oracle library restates the step with the same call (``oracle.sort_by_sublattice``).
     """
-    def sl_index(site):
-        for k, (sites, _) in enumerate(composition):
-            if site in sites:
-                return k
-        return len(composition)
+    from . import sort_by_sublattice
 
-    order = sorted(range(n_sites), key=sl_index)
-    idx = [sl_index(s) for s in order]
-    bounds = []
-    lower = 0
-    for i in range(n_sites):
-        if idx[i] != idx[lower]:
-            bounds.append((lower, i))
-            lower = i
-            if idx[i] == len(composition):
-                break
-        elif i == n_sites - 1:
-            bounds.append((lower, i + 1))
-    return order, bounds
+    sl_of = []
+    for site in range(n_sites):
+        k = next((i for i, (sites, _) in enumerate(composition) if site in sites), len(composition))
+        sl_of.append(k)
+    return sort_by_sublattice(sl_of, len(composition))
 
 
 def default_shell_weights(n_radii, T=np.float64):

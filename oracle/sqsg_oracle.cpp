@@ -546,6 +546,84 @@ static void copy_result(Output<T>* o, uint64_t index, void* objective, void* sub
   }
 }
 
+// Exhaustive enumeration of one window (core/permutation.h + core/optimization.h restated above),
+// keeping per distinct objective the number of configurations and two order-independent 32-bit sums
+// of splitmix64(rank). Used to compare result sets too large to materialise. Every thread keeps only
+// its keep+1 smallest distinct objectives: a value beyond a thread's (keep+1)-th smallest cannot be
+// among the (keep+1) smallest overall.
+static inline uint64_t splitmix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+struct LevelAcc {
+  uint64_t count = 0;
+  uint32_t sa = 0, sb = 0;
+};
+
+template <class T>
+static std::map<T, LevelAcc> systematic_levels(const oracle_sublattice& d, int threads, uint64_t keep,
+                                               uint64_t first, uint64_t count) {
+  Sublattice<T> sl;
+  sl.load(d);
+  const uint32_t lo = sl.bounds[0], hi = sl.bounds[1];
+  std::vector<uint8_t> win(sl.species_packed.begin() + lo, sl.species_packed.begin() + hi);
+  uint64_t total;
+  {
+    std::vector<uint64_t> h = histogram(win.data(), static_cast<int>(win.size()), nullptr), f;
+    for (uint64_t x : h)
+      if (x) f.push_back(x);
+    if (!num_permutations_counts(f, &total)) throw std::out_of_range("too many permutations");
+  }
+  if (first > total) throw std::out_of_range("first rank beyond the permutation count");
+  const uint64_t span = count ? std::min(count, total - first) : total - first;
+  const int nt = std::max(1, threads);
+  const uint64_t nblocks = std::max<uint64_t>(1, std::min<uint64_t>(span, static_cast<uint64_t>(nt) * 64));
+  std::atomic<uint64_t> next{0};
+  std::vector<std::map<T, LevelAcc>> per(nt);
+  auto work = [&](int tid) {
+    std::vector<uint64_t> bonds(static_cast<size_t>(sl.S) * sl.K * sl.K);
+    std::vector<T> sro(bonds.size());
+    std::map<T, LevelAcc>& m = per[tid];
+    while (true) {
+      uint64_t b = next.fetch_add(1);
+      if (b >= nblocks) break;
+      uint64_t r0 = 1 + first + span / nblocks * b + std::min(b, span % nblocks);
+      uint64_t r1 = 1 + first + span / nblocks * (b + 1) + std::min(b + 1, span % nblocks);
+      std::vector<uint8_t> sp = sl.species_packed;
+      unrank_window(sp.data(), sl.n_sites, lo, hi, r0);
+      for (uint64_t r = r0; r < r1; ++r) {
+        count_bonds(bonds, sl.pairs, sp.data(), sl.S, sl.K);
+        T o = compute_objective(sro, bonds, sl);
+        if (m.size() <= keep || o <= std::prev(m.end())->first) {
+          LevelAcc& a = m[o];
+          uint64_t h = splitmix64(r);
+          a.count++;
+          a.sa += static_cast<uint32_t>(h);
+          a.sb += static_cast<uint32_t>(h >> 32);
+          if (m.size() > keep + 1) m.erase(std::prev(m.end()));
+        }
+        next_permutation(sp.data() + lo, static_cast<int64_t>(hi - lo));
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(work, t);
+  for (auto& th : pool) th.join();
+  std::map<T, LevelAcc> all;
+  for (auto& m : per)
+    for (auto& [v, a] : m) {
+      LevelAcc& x = all[v];
+      x.count += a.count;
+      x.sa += a.sa;
+      x.sb += a.sb;
+    }
+  while (all.size() > keep + 1) all.erase(std::prev(all.end()));
+  return all;
+}
+
 struct Handle {
   int prec;
   void* out;
@@ -663,6 +741,69 @@ void oracle_result_stats(void* hp, oracle_stats* st) {
   auto* h = static_cast<Handle*>(hp);
   *st = h->prec == 1 ? static_cast<Output<double>*>(h->out)->stats
                      : static_cast<Output<float>*>(h->out)->stats;
+}
+
+// core/optimization.h:35-72 — sites sorted by sublattice index with std::sort (libstdc++, not
+// stable) and the same comparator, then the windows cut between sublattices. Returns the window
+// count (windows holds up to 2 * cap entries).
+int oracle_sort_by_sublattice(const uint32_t* sl_of_site, int n, int n_sublattices, uint32_t* order,
+                              uint32_t* windows, int cap) {
+  struct Site {
+    uint64_t index;
+    uint64_t pad[4];  // sites are moved as whole objects in the reference; layout does not matter
+  };
+  std::vector<Site> sites(n);
+  for (int i = 0; i < n; ++i) sites[i].index = static_cast<uint64_t>(i);
+  std::sort(sites.begin(), sites.end(),
+            [&](const Site& a, const Site& b) { return sl_of_site[a.index] < sl_of_site[b.index]; });
+  std::vector<uint32_t> idx(n);
+  for (int i = 0; i < n; ++i) {
+    order[i] = static_cast<uint32_t>(sites[i].index);
+    idx[i] = sl_of_site[sites[i].index];
+  }
+  int count = 0, lower = 0;
+  auto push = [&](int lo, int hi) {
+    if (count < cap) {
+      windows[2 * count] = static_cast<uint32_t>(lo);
+      windows[2 * count + 1] = static_cast<uint32_t>(hi);
+    }
+    ++count;
+  };
+  for (int i = 0; i < n; ++i) {
+    if (idx[i] != idx[lower]) {
+      push(lower, i);
+      lower = i;
+      if (idx[i] == static_cast<uint32_t>(n_sublattices)) break;
+    } else if (i == n - 1) {
+      push(lower, i + 1);
+    }
+  }
+  return count;
+}
+
+// Writes up to *n levels (value as double, count, checksum = sa | sb << 32); returns the count.
+int oracle_systematic_levels(const oracle_sublattice* d, int prec, int threads, uint64_t keep, uint64_t first,
+                             uint64_t count, double* values, uint64_t* counts, uint64_t* checksums, int cap) {
+  try {
+    int k = 0;
+    auto emit = [&](auto const& m) {
+      for (auto& [v, a] : m) {
+        if (k >= cap) break;
+        values[k] = static_cast<double>(v);
+        counts[k] = a.count;
+        checksums[k] = static_cast<uint64_t>(a.sa) | (static_cast<uint64_t>(a.sb) << 32);
+        ++k;
+      }
+    };
+    if (prec == 1)
+      emit(systematic_levels<double>(*d, threads, keep, first, count));
+    else
+      emit(systematic_levels<float>(*d, threads, keep, first, count));
+    return k;
+  } catch (std::exception const& e) {
+    g_error = e.what();
+    return -1;
+  }
 }
 
 void oracle_result_get(void* hp, uint64_t index, void* objective, void* sub_objectives,

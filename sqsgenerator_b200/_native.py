@@ -34,6 +34,7 @@ EXPORTED = (
     "sqsg_num_permutations", "sqsg_rank_permutation", "sqsg_unrank_permutation",
     "sqsg_optimize", "sqsg_run_count", "sqsg_run_copy", "sqsg_run_statistics", "sqsg_run_free",
     "sqsg_optimize_trace", "sqsg_optimize_batch", "sqsg_run_levels", "sqsg_run_info",
+    "sqsg_microbench", "sqsg_run_transfer",
 )
 
 
@@ -94,6 +95,8 @@ class SqsgJob(C.Structure):
         ("callback", CALLBACK),
         ("user", C.c_void_p),
         ("max_results", C.c_uint64),
+        ("range_first", C.c_uint64),
+        ("range_count", C.c_uint64),
     ]
 
 
@@ -139,6 +142,8 @@ def lib():
         L.sqsg_run_free.argtypes = [vp]
         L.sqsg_run_levels.argtypes = [vp, C.POINTER(u32), vp, vp, vp]
         L.sqsg_run_info.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.sqsg_run_transfer.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
+        L.sqsg_microbench.argtypes = [C.c_int, C.c_int, C.POINTER(dbl), C.POINTER(dbl)]
         for name in EXPORTED:
             if name not in ("sqsg_version", "sqsg_last_error", "sqsg_device_count", "sqsg_run_count",
                             "sqsg_run_free"):
@@ -278,3 +283,11 @@ def unrank_permutation(conf, rank):
     c = np.ascontiguousarray(conf, dtype=np.uint8).copy()
     check(lib().sqsg_unrank_permutation(ptr(c), len(c), int(rank)))
     return c
+
+
+def microbench(kind: int, device: int = 0):
+    """(rate, seconds) of the shared-memory (kind 0, bytes/s) or INT32 (kind 1, ops/s) microbenchmark."""
+    r = C.c_double()
+    t = C.c_double()
+    check(lib().sqsg_microbench(kind, device, C.byref(r), C.byref(t)))
+    return r.value, t.value

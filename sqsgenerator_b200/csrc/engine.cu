@@ -58,6 +58,7 @@ struct PreparedJob {
   size_t tsz = 8;               // sizeof(T)
   uint32_t configs_per_thread = 1;
   uint64_t max_results = 0;     // caller's record capacity (0 = default)
+  uint64_t range_first = 0, range_count = 0;  // share of the configuration space to evaluate
 };
 
 template <class T> static void copy_cube(std::vector<uint8_t>& blob, size_t off, const void* src, size_t n) {
@@ -218,6 +219,11 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   }
   if (!pj.systematic) pj.total = job.iterations;
   d.total = pj.total;
+  if (job.range_first > pj.total) throw std::out_of_range("range_first beyond the configuration space");
+  pj.range_first = job.range_first;
+  pj.range_count = job.range_count ? job.range_count : pj.total - job.range_first;
+  if (pj.range_count > pj.total - pj.range_first) throw std::out_of_range("range beyond the configuration space");
+  d.trace_base = pj.range_first + (pj.systematic ? 1 : 0);
   d.record_bytes = static_cast<uint32_t>(align_up(rec, 16));
   pj.record_bytes = d.record_bytes;
   d.smem_bytes = static_cast<uint32_t>(smem);
@@ -251,23 +257,22 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
 // configurations on every GPU: about 16384 tiles of kBlock threads, each thread running
 // configs_per_thread configurations.
 static void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles) {
-  const uint64_t total = pj.total;
+  const uint64_t first = pj.range_first;
+  const uint64_t total = pj.range_count;
   if (total == 0) return;
   const uint64_t per_tile_target = (total + 16383) / 16384;
   uint64_t cpt = std::max<uint64_t>(1, (per_tile_target + kBlock - 1) / kBlock);
   cpt = std::min<uint64_t>(cpt, 1u << 16);
   pj.configs_per_thread = static_cast<uint32_t>(cpt);
   const uint64_t tile_configs = cpt * kBlock;
-  uint64_t start = 0, chain = 0;
-  while (start < total) {
+  uint64_t done = 0;
+  while (done < total) {
     Tile t{};
     t.job = job_index;
-    t.count = std::min(tile_configs, total - start);
-    t.start = pj.systematic ? start + 1 : start;
-    t.chain_base = chain;
+    t.count = std::min(tile_configs, total - done);
+    t.start = first + done + (pj.systematic ? 1 : 0);
     tiles.push_back(t);
-    start += t.count;
-    chain += kBlock;
+    done += t.count;
   }
 }
 
@@ -413,6 +418,7 @@ struct Run {
   std::vector<uint64_t> level_count, level_checksum;
   bool truncated = false, levels_exact = true;
   uint64_t candidates = 0;
+  uint64_t h2d_bytes = 0, d2h_bytes = 0;
 };
 
 // The reference accepts a configuration when its objective is <= the search threshold, which only
@@ -427,54 +433,60 @@ template <class T>
 static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& recs, uint64_t n, Run& run,
                            bool have_tstar, double tstar_levels) {
   const size_t rb = pj.record_bytes;
-  std::vector<uint64_t> order(n);
-  for (uint64_t i = 0; i < n; ++i) order[i] = i;
-  std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) {
-    const T oa = read_t<T>(&recs[a * rb]), ob = read_t<T>(&recs[b * rb]);
-    if (oa != ob) return oa < ob;
-    return read_t<uint64_t>(&recs[a * rb + 8]) < read_t<uint64_t>(&recs[b * rb + 8]);
-  });
+  struct Key {
+    T obj;
+    uint64_t id;
+    uint64_t idx;
+  };
+  std::vector<Key> keys(n);
+  for (uint64_t i = 0; i < n; ++i) keys[i] = Key{read_t<T>(&recs[i * rb]), read_t<uint64_t>(&recs[i * rb + 8]), i};
   T tstar = std::numeric_limits<T>::infinity();
   if (have_tstar) {
     tstar = static_cast<T>(tstar_levels);
-  } else {
+    keys.erase(std::remove_if(keys.begin(), keys.end(), [&](const Key& k) { return !(k.obj <= tstar); }), keys.end());
+  }
+  std::sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) {
+    if (a.obj != b.obj) return a.obj < b.obj;
+    return a.id < b.id;
+  });
+  if (!have_tstar) {
     uint64_t distinct = 0;
-    bool have = false;
-    T last = T(0);
-    for (uint64_t k = 0; k < n; ++k) {
-      const T o = read_t<T>(&recs[order[k] * rb]);
-      if (!have || o != last) {
+    for (size_t k = 0; k < keys.size(); ++k)
+      if (k == 0 || keys[k].obj != keys[k - 1].obj) {
         if (distinct == pj.keep) {
-          tstar = o;
+          tstar = keys[k].obj;
           break;
         }
         ++distinct;
-        last = o;
-        have = true;
       }
-    }
   }
   const JobDesc& d = pj.desc;
-  size_t sp_total = 0, sro_total = 0;
+  size_t sp_total = 0, skk_total = 0;
   for (auto& p : pj.parts) {
     sp_total += p.N;
-    sro_total += static_cast<size_t>(p.S) * p.K * p.K;
+    skk_total += static_cast<size_t>(p.S) * p.K * p.K;
   }
+  // Systematic ranks are unique, so only random runs can return one configuration twice.
+  const bool dedup = !pj.systematic;
   std::unordered_set<std::string> seen;
+  std::string key;
+  run.objective.reserve(keys.size() * sizeof(T));
+  run.species.reserve(keys.size() * sp_total);
+  run.sro.reserve(keys.size() * skk_total * sizeof(T));
   T cur_obj = T(0);
   bool have_cur = false;
   uint64_t cur_count = 0;
-  std::string key;
-  for (uint64_t k = 0; k < n; ++k) {
-    const uint8_t* r = &recs[order[k] * rb];
-    const T o = read_t<T>(r);
-    if (!(o <= tstar)) break;
-    key.clear();
-    for (uint32_t p = 0; p < d.n_parts; ++p)
-      key.append(reinterpret_cast<const char*>(r + d.parts[p].rec_species_off), d.parts[p].n_sites);
-    if (!seen.insert(key).second) continue;
-    if (!have_cur || o != cur_obj) {
-      cur_obj = o;
+  for (const Key& k : keys) {
+    if (!(k.obj <= tstar)) break;
+    const uint8_t* r = &recs[k.idx * rb];
+    if (dedup) {
+      key.clear();
+      for (uint32_t p = 0; p < d.n_parts; ++p)
+        key.append(reinterpret_cast<const char*>(r + d.parts[p].rec_species_off), d.parts[p].n_sites);
+      if (!seen.insert(key).second) continue;
+    }
+    if (!have_cur || k.obj != cur_obj) {
+      cur_obj = k.obj;
       have_cur = true;
       cur_count = 0;
     }
@@ -488,11 +500,9 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
       const size_t skk = static_cast<size_t>(P.n_shells) * P.n_species * P.n_species;
       run.sro.insert(run.sro.end(), r + P.rec_sro_off, r + P.rec_sro_off + skk * sizeof(T));
     }
-    run.id.push_back(read_t<uint64_t>(r + 8));
+    run.id.push_back(k.id);
     run.count++;
   }
-  (void)sp_total;
-  (void)sro_total;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -589,6 +599,8 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     if (!tiles.empty())
       CUDA_CHECK(cudaMemcpyAsync(ws->tiles.p, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice,
                                  ws->stream));
+    uint64_t h2d_bytes = init.size() * sizeof(unsigned long long) + nj * sizeof(JobDesc) + tiles.size() * sizeof(Tile);
+    for (size_t j = 0; j < nj; ++j) h2d_bytes += pjs[j].blob.size();
     CUDA_CHECK(cudaMemsetAsync(ws->levels.p, 0, nj * kLevelSlots * sizeof(LevelSlot), ws->stream));
     CUDA_CHECK(cudaMemsetAsync(ws->queue.p, 0, sizeof(QueueCtl), ws->stream));
     CUDA_CHECK(cudaMemsetAsync(ws->status.p, 0, sizeof(unsigned long long), ws->stream));
@@ -639,7 +651,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
           while (next_cb[j] <= fin) next_cb[j] += chunk;
           sqsg_statistics st{};
           st.finished = fin;
-          st.working = pjs[j].total > fin ? pjs[j].total - fin : 0;
+          st.working = pjs[j].range_count > fin ? pjs[j].range_count - fin : 0;
           st.best_objective = from_ord(ws->mirror[j * kNumCounters + kBest]);
           st.timings_ns[SQSG_TIMING_TOTAL] = now_ns() - t0;
           if (srcs[j]->callback(&st, srcs[j]->user) != 0) stop = true;
@@ -681,6 +693,8 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
         CUDA_CHECK(cudaMemcpy(recs.data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], recs.size(),
                               cudaMemcpyDeviceToHost));
       Run& r = runs[j];
+      r.h2d_bytes = h2d_bytes / nj;
+      r.d2h_bytes = recs.size() + kLevelSlots * sizeof(LevelSlot) + (cnt.size() * sizeof(unsigned long long) + 8) / nj;
       r.prec = pjs[j].prec;
       r.n_parts = pjs[j].desc.n_parts;
       r.parts = pjs[j].parts;
@@ -721,8 +735,8 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     }
     if (trace && trace->capacity) {
       const PreparedJob& pj = pjs[0];
-      const uint64_t n = std::min<uint64_t>(pj.total, trace->capacity);
-      if (trace->count) *trace->count = pj.total;
+      const uint64_t n = std::min<uint64_t>(pj.range_count, trace->capacity);
+      if (trace->count) *trace->count = pj.range_count;
       const JobDesc& d = pj.desc;
       if (trace->species)
         CUDA_CHECK(cudaMemcpy(trace->species, ws->trace_sp.p, n * d.trace_species_stride, cudaMemcpyDeviceToHost));
@@ -921,6 +935,14 @@ sqsg_status sqsg_run_levels(const sqsg_run* run, uint32_t* n, double* values, ui
       if (counts) counts[k] = r.level_count[k];
       if (checksums) checksums[k] = r.level_checksum[k];
     }
+  });
+}
+
+sqsg_status sqsg_run_transfer(const sqsg_run* run, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("null run");
+    if (h2d_bytes) *h2d_bytes = run->r.h2d_bytes;
+    if (d2h_bytes) *d2h_bytes = run->r.d2h_bytes;
   });
 }
 

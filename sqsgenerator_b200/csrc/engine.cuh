@@ -93,15 +93,16 @@ struct JobDesc {
   void* trace_obj;
   uint64_t* trace_id;
   uint64_t trace_capacity;
+  uint64_t trace_base;    // id of the first traced configuration
   PartDesc parts[kMaxParts];
 };
 
 struct Tile {
   uint32_t job;
   uint32_t reserved;
-  uint64_t start;       // random: global index of the tile's first configuration; systematic: first rank
+  uint64_t start;       // random: index of the tile's first configuration; systematic: its 1-based rank
   uint64_t count;       // configurations in the tile
-  uint64_t chain_base;  // random: Philox chain id of thread 0
+  uint64_t reserved2;
 };
 
 // Queue control block for the persistent kernel (device memory, or host-mapped for serving).

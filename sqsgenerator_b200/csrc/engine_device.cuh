@@ -465,7 +465,9 @@ __device__ __noinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelSlot
   const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
   const uint64_t max_count = base + (rem ? 1 : 0);
   const bool systematic = J.mode == 1;
-  const unsigned long long chain = tile.chain_base + static_cast<unsigned long long>(t);
+  // random mode: a chain is named by the index of its first configuration, so ids are unique for
+  // any split of the job into tiles or devices
+  const unsigned long long chain = tile.start + my_off;
   const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
 
   for (uint32_t p = 0; p < J.n_parts; ++p) init_column(smem, J.parts[p], t);
@@ -494,12 +496,9 @@ __device__ __noinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelSlot
     if ((it & 15) == 0) thr_g = load_threshold<T>(J);
     const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
     const bool pass = active && static_cast<double>(total) <= bound;
-    const uint64_t id = systematic ? tile.start + my_off + it : ((chain << 32) | it);
+    const uint64_t id = tile.start + my_off + it;
     handle_candidates<T>(J, smem, ctab, ws, pass, total, thr_g, id, t);
-    if (J.trace && active) {
-      const uint64_t g = systematic ? tile.start + my_off + it - 1 : tile.start + my_off + it;
-      write_trace<T>(J, smem, g, total, id, t);
-    }
+    if (J.trace && active) write_trace<T>(J, smem, id - J.trace_base, total, id, t);
     if (systematic && active && it + 1 < my_count)
       next_permutation(part_base(smem, J.parts[0]) + J.parts[0].col_off + 4 * t, wlo, wn);
   }

@@ -1,0 +1,140 @@
+"""Configurations shared by the tests (reference-schema dicts) and trace helpers."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+import oracle
+from oracle import geometry as G
+
+
+def fcc_coords():
+    return [[0.0, 0.0, 0.0], [0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]]
+
+
+def settings_16(prec="double"):
+    """python/tests/test_core.py:28-44 of the reference: a 16-site cell, Ti8Al8 on the H sites."""
+    return dict(
+        prec=prec,
+        iteration_mode="systematic",
+        structure=dict(lattice=np.diag([1, 2, 3]).tolist(),
+                       coords=[[0.0, 0.0, 0.0], [0.5, 0.5, 0.0], [0.0, 0.5, 0.5], [0.5, 0.0, 0.5]],
+                       species=[1] * 4, supercell=[2, 2, 1]),
+        pair_weights=0,
+        composition={"sites": "H", "Ti": 8, "Al": 8},
+        thread_config=1,
+    )
+
+
+def fcc32(prec="double", **kw):
+    """fcc 2x2x2 (32 sites, a = 4.0), A16B16, shells 1/2 weighted 1.0/0.5, all pair weights 1."""
+    a = 4.0
+    d = dict(prec=prec,
+             structure=dict(lattice=(np.eye(3) * a).tolist(), coords=fcc_coords(), species=[1] * 4, supercell=[2, 2, 2]),
+             composition={"Ti": 16, "Al": 16}, shell_weights={"1": 1.0, "2": 0.5}, pair_weights=1,
+             iterations=1000000, seed=42, thread_config=1, keep=10)
+    d.update(kw)
+    return {k: v for k, v in d.items() if v is not None}
+
+
+def quinary(prec="double", cells=(3, 3, 3), **kw):
+    a = 4.0
+    n = 4 * cells[0] * cells[1] * cells[2]
+    counts = [n // 5 + (1 if k < n % 5 else 0) for k in range(5)]
+    comp = dict(zip(["Ti", "Al", "Nb", "V", "Zr"], counts))
+    d = dict(prec=prec,
+             structure=dict(lattice=(np.eye(3) * a).tolist(), coords=fcc_coords(), species=[1] * 4, supercell=list(cells)),
+             composition=comp, shell_weights={"1": 1.0, "2": 0.5, "3": 0.25}, iterations=20000, seed=7,
+             thread_config=1, keep=5)
+    d.update(kw)
+    return d
+
+
+def rocksalt_split(prec="double", cells=(2, 2, 2), **kw):
+    L, F = G.rocksalt(4.2)
+    n = 4 * cells[0] * cells[1] * cells[2]
+    d = dict(prec=prec, sublattice_mode="split",
+             structure=dict(lattice=L.tolist(), coords=F.tolist(), species=[11] * 4 + [17] * 4, supercell=list(cells)),
+             composition=[{"sites": "Na", "Ti": n // 2, "Al": n - n // 2},
+                          {"sites": "Cl", "N": n - n // 8, "B": n // 8}],
+             shell_weights=[{"1": 1.0, "2": 0.5}, {"1": 1.0, "2": 0.5}], iterations=20000, seed=3, thread_config=1)
+    d.update(kw)
+    return d
+
+
+def trace(config, capacity):
+    """Run through sqsg_optimize_trace; returns (config, data, pack, species, bonds, objective, ids)."""
+    import sqsgenerator_b200 as S
+    from sqsgenerator_b200 import _native as N
+    from sqsgenerator_b200.optimize import build_job, collect
+
+    c = S.parse_config(config)
+    assert not isinstance(c, S.ParseError), c
+    d = S.prepare(c)
+    job, bufs = build_job(c, d)
+    T = np.float64 if int(c.prec) == 1 else np.float32
+    sp_w = sum(len(x.species_packed) for x in d)
+    bd_w = sum(x.prefactors.size for x in d)
+    sp = np.zeros(capacity * sp_w, np.uint8)
+    bd = np.zeros(capacity * bd_w, np.uint32)
+    ob = np.zeros(capacity, T)
+    ids = np.zeros(capacity, np.uint64)
+    cnt = C.c_uint64(0)
+    run = C.c_void_p()
+    N.check(N.lib().sqsg_optimize_trace(C.byref(job), C.byref(run), capacity, C.byref(cnt), N.ptr(sp), N.ptr(bd),
+                                        N.ptr(ob), N.ptr(ids)))
+    try:
+        pack = collect(c, d, run)
+    finally:
+        N.lib().sqsg_run_free(run)
+    n = min(cnt.value, capacity)
+    return c, d, pack, sp[: n * sp_w].reshape(n, sp_w), bd[: n * bd_w].reshape(n, bd_w), ob[:n], ids[:n]
+
+
+def trace_mismatches(d, sp, bd, ob, prec, limit=None):
+    """Recompute bonds and objective of every traced configuration with the oracle; count mismatches."""
+    bad = []
+    rows = range(len(ob)) if limit is None else range(min(limit, len(ob)))
+    for k in rows:
+        o1 = o2 = 0
+        total = None
+        for part in d:
+            n = len(part.species_packed)
+            skk = part.prefactors.size
+            species = sp[k, o1:o1 + n]
+            b = oracle.count_bonds(part, species).reshape(-1)
+            if not np.array_equal(b.astype(np.uint32), bd[k, o2:o2 + skk]):
+                bad.append((k, "bonds"))
+                break
+            o, _ = oracle.evaluate(part, species, prec)
+            total = o if total is None else type(o)(total + o)
+            o1 += n
+            o2 += skk
+        else:
+            if total.tobytes() != ob[k].tobytes():
+                bad.append((k, "objective", total, ob[k]))
+    return bad
+
+
+def run_levels(run):
+    """(values, counts, checksums) of a native run handle."""
+    from sqsgenerator_b200 import _native as N
+
+    n = C.c_uint32(64)
+    v = np.zeros(64, np.float64)
+    cnt = np.zeros(64, np.uint64)
+    cs = np.zeros(64, np.uint64)
+    N.check(N.lib().sqsg_run_levels(run, C.byref(n), N.ptr(v), N.ptr(cnt), N.ptr(cs)))
+    return [(float(v[i]), int(cnt[i]), int(cs[i])) for i in range(n.value)]
+
+
+def oracle_fcc32(T=np.float64):
+    """The fcc 2x2x2 A16B16 benchmark cell built by the oracle's own geometry (independent of the
+    product's precompute): shells 1/2 weighted 1.0/0.5, all pair weights 1."""
+    lat, frac = G.fcc(4.0)
+    L, F, species = G.supercell(lat, frac, [1] * 4, 2, 2, 2, T)
+    comp = [(set(range(32)), {13: 16, 22: 16})]
+    radii = G.distances_histogram(G.distance_matrix(L, F, T), 0.05, 0.25, T)
+    return G.prepare_interact(L, F, species, comp, radii, {1: T(1.0), 2: T(0.5)}, T,
+                              pair_weights=np.ones((2, 2, 2), dtype=T))
