@@ -168,6 +168,7 @@ def run_b200(args):
     job, bufs = build_job(c, d, device=device)
     job.range_first = first
     job.range_count = count
+    job.max_results = args.max_results
     L = N.lib()
     P = len(d[0].pairs)
     nsp = len(d[0].species_packed)
@@ -272,6 +273,7 @@ def run_b200(args):
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "configs_per_step": total, "sites": nsp, "pairs": P,
                        "l2": "flushed between timed steps (256 MiB device write)",
+                       "max_results": args.max_results,
                        "parallelism": f"rank space split into {world} contiguous ranges"},
             "e2e": {"value": e2e, "unit": "configs/s", "h2d_bytes_per_step": out[-1]["h2d"],
                     "d2h_bytes_per_step": out[-1]["d2h"], "ms_per_step": wall / args.steps * 1e3},
@@ -293,6 +295,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--limit", type=int, default=0, help="evaluate only the first LIMIT ranks (profiling)")
+    ap.add_argument("--max-results", type=int, default=1 << 20,
+                    help="record capacity per step; the exact objective levels do not depend on it")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -153,6 +153,7 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   size_t blob_size = 0, smem = 0;
   size_t rec = 16, tsp = 0, tbd = 0;
   std::vector<std::vector<uint32_t>> streams(job.n_sublattices);
+  std::vector<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>> k2_data;
   for (uint32_t p = 0; p < job.n_sublattices; ++p) {
     const sqsg_sublattice& sl = job.sublattices[p];
     PartDesc& P = d.parts[p];
@@ -183,7 +184,34 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     streams[p] = build_stream(sl);
     P.stream_words = static_cast<uint32_t>(streams[p].size());
     const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
-    // staged section layout: cubes | windows | stream | species codes
+    // binary fast path data: per (shell, site) mask of the neighbours j > i (bit N-1-j)
+    const bool k2 = job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64;
+    std::vector<uint32_t> k2_entries, k2_shells;
+    if (k2) {
+      const uint32_t N = sl.n_sites;
+      std::vector<unsigned long long> nb(static_cast<size_t>(sl.n_shells) * N, 0ull);
+      std::vector<uint32_t> ps(sl.n_shells, 0);
+      for (uint32_t e = 0; e < sl.n_pairs; ++e) {
+        uint32_t i = sl.pairs[3 * e], j = sl.pairs[3 * e + 1];
+        const uint32_t sh = sl.pairs[3 * e + 2];
+        if (i > j) std::swap(i, j);
+        nb[static_cast<size_t>(sh) * N + i] |= 1ull << (N - 1 - j);
+        ps[sh]++;
+      }
+      for (uint32_t sh = 0; sh < sl.n_shells; ++sh) {
+        for (uint32_t i = 0; i < N; ++i) {
+          const unsigned long long m = nb[static_cast<size_t>(sh) * N + i];
+          if (!m) continue;
+          k2_entries.push_back(static_cast<uint32_t>(m));
+          k2_entries.push_back(static_cast<uint32_t>(m >> 32));
+          k2_entries.push_back(N - 1 - i);
+          k2_entries.push_back(static_cast<uint32_t>(__builtin_popcountll(m)));
+        }
+        k2_shells.push_back(ps[sh]);
+        k2_shells.push_back(static_cast<uint32_t>(k2_entries.size() / 4));
+      }
+    }
+    // staged section layout: cubes | windows | stream | species codes | binary-path masks
     size_t off = 0;
     P.cube_off = 0;
     off = align_up(3 * skk * pj.tsz, 16);
@@ -193,6 +221,16 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     off = align_up(off + 4ull * streams[p].size(), 16);
     P.species_off = static_cast<uint32_t>(off);
     off = align_up(off + sl.n_sites, 16);
+    if (k2) {
+      P.k2_off = static_cast<uint32_t>(off);
+      P.k2_entries = static_cast<uint32_t>(k2_entries.size() / 4);
+      off = align_up(off + 4 * k2_entries.size(), 16);
+      P.k2_shell_off = static_cast<uint32_t>(off);
+      off = align_up(off + 4 * k2_shells.size(), 16);
+      k2_data.emplace_back(std::move(k2_entries), std::move(k2_shells));
+    } else {
+      k2_data.emplace_back();
+    }
     P.static_bytes = static_cast<uint32_t>(off);
     P.blob_off = static_cast<uint32_t>(blob_size);
     blob_size += off;
@@ -216,6 +254,8 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     tbd += skk;
     pj.parts.push_back(PartMeta{sl.n_sites, sl.n_species, sl.n_shells});
     if (pj.systematic) pj.total = window_permutations(sl, P);
+    if (k2 && (!pj.systematic || (P.unrank_k == 2 && P.unrank_rev[0] == 0 && P.unrank_rev[1] == 1)))
+      d.k2 = sl.n_sites <= 32 ? 1 : 2;
   }
   if (!pj.systematic) pj.total = job.iterations;
   d.total = pj.total;
@@ -249,6 +289,9 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     std::memcpy(base + P.win_off, sl.windows, 8ull * sl.n_windows);
     std::memcpy(base + P.stream_off, streams[p].data(), 4ull * streams[p].size());
     for (uint32_t x = 0; x < sl.n_sites; ++x) base[P.species_off + x] = static_cast<uint8_t>(sl.species[x] << 3);
+    const auto& k2d = k2_data[p];
+    if (!k2d.first.empty()) std::memcpy(base + P.k2_off, k2d.first.data(), 4 * k2d.first.size());
+    if (!k2d.second.empty()) std::memcpy(base + P.k2_shell_off, k2d.second.data(), 4 * k2d.second.size());
   }
   return pj;
 }
@@ -534,6 +577,8 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
   size_t smem = 0, blob_total = 0;
   std::vector<size_t> blob_off(nj), rec_off(nj);
   std::vector<uint64_t> capacity(nj);
+  std::vector<double> start_threshold(nj, 0.0);
+  std::vector<bool> fixed_threshold(nj, false);
   size_t rec_total = 0;
   for (size_t j = 0; j < nj; ++j) {
     if (pjs[j].desc.smem_bytes > smem_limit)
@@ -576,7 +621,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       d.levels = static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots;
       const double maxv = pjs[j].prec == 1 ? std::numeric_limits<double>::max()
                                            : static_cast<double>(std::numeric_limits<float>::max());
-      init[j * kNumCounters + kThreshold] = ord_bits(maxv);
+      init[j * kNumCounters + kThreshold] = ord_bits(fixed_threshold[j] ? start_threshold[j] : maxv);
       init[j * kNumCounters + kBest] = ord_bits(std::numeric_limits<double>::infinity());
       if (trace && trace->capacity) {
         const size_t sp = d.trace_species_stride, bd = d.trace_bonds_stride;
@@ -672,13 +717,27 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     // A candidate overflow re-runs the job with a larger buffer when the caller left the capacity
     // to the library and the records fit the memory budget (tiles and Philox counters make the
     // re-run evaluate the same configurations); otherwise the record set is cut and flagged.
+    // The re-run starts at the exact final threshold T* (the (keep+1)-th smallest level) and needs
+    // exactly the evaluations at or below it, which the level table counts.
     bool rerun = false;
     for (size_t j = 0; j < nj; ++j) {
-      const uint64_t need = cnt[j * kNumCounters + kCandidates];
-      if (need <= capacity[j] || pjs[j].max_results) continue;
+      const bool full = cnt[j * kNumCounters + kRecordsFull] != 0 || cnt[j * kNumCounters + kCandidates] > capacity[j];
+      if (!full || pjs[j].max_results || attempt >= 2 || cnt[j * kNumCounters + kLevelOverflow]) continue;
+      std::vector<LevelSlot> lv(kLevelSlots);
+      CUDA_CHECK(cudaMemcpy(lv.data(), static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots,
+                            kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost));
+      std::vector<LevelSlot> used;
+      for (auto& x : lv)
+        if (x.key) used.push_back(x);
+      std::sort(used.begin(), used.end(), [](const LevelSlot& a, const LevelSlot& b) { return a.key < b.key; });
+      uint64_t need = 0;
+      for (size_t k = 0; k < used.size() && k <= pjs[j].keep; ++k) need += used[k].count;
       const uint64_t budget = (4ull << 30) / pjs[j].record_bytes;
-      if (need + need / 4 <= budget && attempt < 2) {
-        capacity[j] = need + need / 4;
+      if (need <= budget) {
+        capacity[j] = std::max<uint64_t>(need + 64, 1024);
+        fixed_threshold[j] = true;
+        start_threshold[j] = used.size() > pjs[j].keep ? from_ord(used[pjs[j].keep].key)
+                                                       : std::numeric_limits<double>::infinity();
         rerun = true;
       }
     }
@@ -717,7 +776,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       const double tstar = used.size() > pjs[j].keep ? from_ord(used[pjs[j].keep].key)
                                                      : std::numeric_limits<double>::infinity();
       r.candidates = cnt[j * kNumCounters + kCandidates];
-      r.truncated = r.candidates > capacity[j];
+      r.truncated = cnt[j * kNumCounters + kRecordsFull] != 0 || r.candidates > capacity[j];
       const uint64_t stored = std::min<uint64_t>(n, capacity[j]);
       if (pjs[j].prec == 1)
         select_results<double>(pjs[j], recs, stored, r, have_tstar, tstar);

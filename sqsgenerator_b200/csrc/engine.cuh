@@ -32,6 +32,7 @@ enum Counter : int {
   kBest = 4,        // ordered bits (double) of the best objective seen, atomicMin
   kTilesDone = 5,   // tiles completed
   kLevelOverflow = 6,  // the job's level table ran out of slots
+  kRecordsFull = 7,    // set once the candidate buffer is full (appends stop)
   kNumCounters = 8
 };
 
@@ -69,6 +70,10 @@ struct PartDesc {
   uint8_t unrank_rev[kMaxSpecies];
   // bond-trace layout
   uint32_t trace_species_off, trace_bonds_off;
+  // binary fast path (K == 2, N <= 64): per (shell, site) neighbour masks, see run_tile_k2
+  uint32_t k2_off;        // entries: uint4 {mask lo, mask hi, site | shell << 8, popcount}
+  uint32_t k2_entries;
+  uint32_t k2_shell_off;  // S u32: pairs per shell
 };
 
 struct JobDesc {
@@ -76,6 +81,7 @@ struct JobDesc {
   uint32_t mode;          // 0 random, 1 systematic
   uint32_t n_parts;
   uint32_t kw;            // 1: every part has K <= 4 (32-bit row), 2: K <= 8 (64-bit row)
+  uint32_t k2;            // 0: general path; 1: binary bitmask path with N <= 32; 2: with N <= 64
   uint32_t keep;
   uint32_t record_bytes;
   uint32_t smem_bytes;

@@ -383,9 +383,16 @@ __device__ __forceinline__ void write_trace(const JobDesc& J, uint8_t* smem, uin
   J.trace_id[g] = id;
 }
 
-template <class T>
+struct NoPrep {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+// `prep` runs right before a record is written (the binary path materialises the lane's species and
+// bond counts in shared memory only then).
+template <class T, class Prep = NoPrep>
 __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, WarpState& ws,
-                                                  bool pass, T total, T thr_g, uint64_t id, int t) {
+                                                  bool pass, T total, T thr_g, uint64_t id, int t,
+                                                  const Prep& prep = Prep()) {
   const int lane = t & 31;
   unsigned m = __ballot_sync(0xffffffffu, pass);
   if (!m) return;
@@ -440,12 +447,24 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
       pending &= ~gm;
     }
   }
+  // Once the record buffer is full, appends stop (the level table stays exact) and the contended
+  // candidate counter is left alone.
   unsigned long long base = 0;
-  if (lane == 0) base = atomicAdd(&J.counters[kCandidates], static_cast<unsigned long long>(__popc(km)));
+  if (lane == 0) {
+    if (*reinterpret_cast<volatile unsigned long long*>(&J.counters[kRecordsFull]) != 0ull) {
+      base = ~0ull;
+    } else {
+      base = atomicAdd(&J.counters[kCandidates], static_cast<unsigned long long>(__popc(km)));
+      if (base + __popc(km) > J.capacity) J.counters[kRecordsFull] = 1ull;
+    }
+  }
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (keep_it) {
+  if (keep_it && base != ~0ull) {
     const uint64_t idx = base + __popc(km & ((1u << lane) - 1u));
-    if (idx < J.capacity) write_record<T>(J, smem, idx, total, id, t);
+    if (idx < J.capacity) {
+      prep();
+      write_record<T>(J, smem, idx, total, id, t);
+    }
   }
 }
 
@@ -501,6 +520,192 @@ __device__ __noinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelSlot
     if (J.trace && active) write_trace<T>(J, smem, id - J.trace_base, total, id, t);
     if (systematic && active && it + 1 < my_count)
       next_permutation(part_base(smem, J.parts[0]) + J.parts[0].col_off + 4 * t, wlo, wn);
+  }
+}
+
+// ------------------------------------------------------------------------------ binary fast path
+// A configuration of a binary (K == 2) structure with N <= 64 sites is one word v: site x holds
+// species 1 when bit N-1-x is set. The first site of a window is its most significant bit, so the
+// lexicographic order of core/permutation.h:80-102 is the integer order and next_permutation is the
+// next larger word with the same popcount (Gosper's hack). With NB_s[i] the mask of the sites j > i
+// in shell s and b_i the species of site i,
+//   D = sum_i popc(NB_s[i] & v)      = n(s,1,1) + n(s,0,1)
+//   A = sum_i b_i popc(NB_s[i] & v)  = n(s,1,1)
+//   E = sum_i b_i popc(NB_s[i])      = n(s,1,1) + n(s,1,0)
+// and n(s,0,0) = P_s minus the rest: the ordered counts of optimization.h:74-77, exactly. The
+// Fisher-Yates draws and the visiting order are the general path's, so both evaluate the same
+// configurations for a job.
+template <int W> struct Word;
+template <> struct Word<1> {
+  using type = uint32_t;
+  static __device__ __forceinline__ uint32_t pc(type v, uint32_t lo, uint32_t) { return __popc(v & lo); }
+  static __device__ __forceinline__ int ctz(type v) { return __ffs(static_cast<int>(v)) - 1; }
+};
+template <> struct Word<2> {
+  using type = unsigned long long;
+  static __device__ __forceinline__ uint32_t pc(type v, uint32_t lo, uint32_t hi) {
+    return __popc(static_cast<uint32_t>(v) & lo) + __popc(static_cast<uint32_t>(v >> 32) & hi);
+  }
+  static __device__ __forceinline__ int ctz(type v) { return __ffsll(static_cast<long long>(v)) - 1; }
+};
+
+template <class V> __device__ __forceinline__ V low_mask(uint32_t n) {
+  return n >= sizeof(V) * 8 ? ~V(0) : ((V(1) << n) - V(1));
+}
+
+// Ordered bond counts of shell s for word v.
+template <class V, int W>
+__device__ __forceinline__ void k2_counts(const uint4* ent, uint32_t e0, uint32_t e1, uint32_t ps, V v,
+                                          uint32_t& n00, uint32_t& n01, uint32_t& n10, uint32_t& n11) {
+  uint32_t A = 0, D = 0, E = 0;
+  for (uint32_t e = e0; e < e1; ++e) {
+    const uint4 q = ent[e];
+    const uint32_t c = Word<W>::pc(v, q.x, q.y);
+    const uint32_t b = static_cast<uint32_t>(v >> q.z) & 1u;
+    D += c;
+    A += b * c;
+    E += b * q.w;
+  }
+  n11 = A;
+  n01 = D - A;
+  n10 = E - A;
+  n00 = ps - n11 - n01 - n10;
+}
+
+template <class T>
+__device__ __forceinline__ T k2_term(T obj, uint32_t n, const T* f, const T* w, const T* tg, uint32_t d) {
+  using F = FP<T>;
+  const T sig = F::sub(T(1), F::mul(F::cvt(n), f[d]));
+  T diff = F::sub(sig, tg[d]);
+  diff = diff > T(0) ? diff : -diff;
+  return F::add(obj, F::mul(w[d], diff));
+}
+
+// Writes the lane's species codes and bond histogram like the general path keeps them, so that the
+// general record and trace writers can be used.
+template <class V, int W>
+__device__ __forceinline__ void k2_materialize(uint8_t* smem, const PartDesc& P, int t, V v) {
+  uint8_t* part = part_base(smem, P);
+  uint8_t* col = part + P.col_off + 4 * t;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(part + P.hist_off) + t;
+  const uint32_t N = P.n_sites;
+  for (uint32_t x = 0; x < N; ++x) col[site_off(x)] = static_cast<uint8_t>((static_cast<uint32_t>(v >> (N - 1 - x)) & 1u) << 3);
+  const uint4* ent = reinterpret_cast<const uint4*>(part + P.k2_off);
+  const uint32_t* sh = reinterpret_cast<const uint32_t*>(part + P.k2_shell_off);
+  uint32_t e0 = 0;
+  for (uint32_t s = 0; s < P.n_shells; ++s) {
+    uint32_t n00, n01, n10, n11;
+    k2_counts<V, W>(ent, e0, sh[2 * s + 1], sh[2 * s], v, n00, n01, n10, n11);
+    e0 = sh[2 * s + 1];
+    hist[(s * 2 + 0) * kBlock] = n00 | (n01 << 16);
+    hist[(s * 2 + 1) * kBlock] = n10 | (n11 << 16);
+  }
+}
+
+template <class T, int W>
+__device__ __noinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                         WarpState& ws) {
+  using V = typename Word<W>::type;
+  const int t = threadIdx.x;
+  const PartDesc& P = J.parts[0];
+  const uint64_t base = tile.count / kBlock, rem = tile.count % kBlock;
+  const uint64_t my_count = base + (static_cast<uint64_t>(t) < rem ? 1 : 0);
+  const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
+  const uint64_t max_count = base + (rem ? 1 : 0);
+  const bool systematic = J.mode == 1;
+  const unsigned long long chain = tile.start + my_off;
+  const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
+  const uint8_t* part = part_base(smem, P);
+  const uint32_t N = P.n_sites, S = P.n_shells;
+  const uint4* ent = reinterpret_cast<const uint4*>(part + P.k2_off);
+  const uint32_t* sh = reinterpret_cast<const uint32_t*>(part + P.k2_shell_off);
+  const T* f = reinterpret_cast<const T*>(part + P.cube_off);
+  const T* w = f + 4 * S;
+  const T* tg = w + 4 * S;
+  const uint32_t* win = reinterpret_cast<const uint32_t*>(part + P.win_off);
+  V v = 0;
+  for (uint32_t x = 0; x < N; ++x)
+    if (part[P.species_off + x]) v |= V(1) << (N - 1 - x);
+  uint32_t wn = 0, wshift = 0;
+  V wmask = 0;
+  if (systematic) {
+    wn = win[1] - win[0];
+    wshift = N - win[1];
+    wmask = low_mask<V>(wn) << wshift;
+    if (my_count > 0) {  // core/permutation.h:52-78 for two species
+      uint64_t rank = tile.start + my_off, total = J.total;
+      uint32_t h0 = P.unrank_hist[0], h1 = P.unrank_hist[1];
+      V word = 0;
+      for (uint32_t k = 0; k < wn; ++k) {
+        const uint64_t s0 = div_96x32(mul_64x32(total, h0), wn - k, nullptr);
+        if (rank <= s0) {
+          total = s0;
+          --h0;
+        } else {
+          rank -= s0;
+          total = div_96x32(mul_64x32(total, h1), wn - k, nullptr);
+          --h1;
+          word |= V(1) << (wn - 1 - k);
+        }
+      }
+      v = (v & ~wmask) | (word << wshift);
+    }
+  }
+  T thr_g = load_threshold<T>(J);
+  for (uint64_t it = 0; it < max_count; ++it) {
+    const bool active = it < my_count;
+    T total = T(0);
+    if (active) {
+      if (!systematic) {  // core/shuffle.h:39-50 on bits, same Philox words as the general path
+        const uint32_t c_lo = static_cast<uint32_t>(chain), c_hi = static_cast<uint32_t>(chain >> 32) << 8;
+        uint32_t blk = 0;
+        for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
+          const uint32_t lo = win[2 * wi];
+          uint32_t i = win[2 * wi + 1] - lo;
+          const uint32_t top = N - 1 - lo;  // bit of the window's first site
+          while (i > 1) {
+            const philox_ctr r = philox4x32_10(philox_ctr{blk++, static_cast<uint32_t>(it), c_lo, c_hi}, k0, k1);
+            const uint32_t xs[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              if (i <= 1) break;
+              const uint32_t pp = __umulhi(xs[q], i);
+              const uint32_t ba = top - (i - 1), bb = top - pp;
+              const V dlt = ((v >> ba) ^ (v >> bb)) & V(1);
+              v ^= (dlt << ba) | (dlt << bb);
+              --i;
+            }
+          }
+        }
+      }
+      uint32_t e0 = 0;
+      for (uint32_t s = 0; s < S; ++s) {
+        uint32_t n00, n01, n10, n11;
+        const uint32_t e1 = sh[2 * s + 1];
+        k2_counts<V, W>(ent, e0, e1, sh[2 * s], v, n00, n01, n10, n11);
+        e0 = e1;
+        total = k2_term<T>(total, n00, f, w, tg, s * 4 + 0);
+        total = k2_term<T>(total, n01 + n10, f, w, tg, s * 4 + 1);
+        total = k2_term<T>(total, n11, f, w, tg, s * 4 + 3);
+      }
+    }
+    if ((it & 15) == 0) thr_g = load_threshold<T>(J);
+    const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
+    const bool pass = active && static_cast<double>(total) <= bound;
+    const uint64_t id = tile.start + my_off + it;
+    const V vv = v;
+    handle_candidates<T>(J, smem, ctab, ws, pass, total, thr_g, id, t,
+                         [&]() { k2_materialize<V, W>(smem, P, t, vv); });
+    if (J.trace && active) {
+      k2_materialize<V, W>(smem, P, t, v);
+      write_trace<T>(J, smem, id - J.trace_base, total, id, t);
+    }
+    if (systematic && active && it + 1 < my_count) {  // Gosper's hack inside the window
+      const V x = (v & wmask) >> wshift;
+      const V tt = x | (x - 1);
+      const V nx = (tt + 1) | (((~tt & (tt + 1)) - 1) >> (Word<W>::ctz(x) + 1));
+      v = (v & ~wmask) | ((nx << wshift) & wmask);
+    }
   }
 }
 
@@ -563,7 +768,17 @@ __global__ void __launch_bounds__(kBlock) sqsg_engine(const JobDesc* __restrict_
       cur = static_cast<int>(tile.job);
       ws.reset();
     }
-    if (sj.prec == 1) {
+    if (sj.k2 == 1) {
+      if (sj.prec == 1)
+        run_tile_k2<double, 1>(sj, smem, ctab, tile, ws);
+      else
+        run_tile_k2<float, 1>(sj, smem, ctab, tile, ws);
+    } else if (sj.k2 == 2) {
+      if (sj.prec == 1)
+        run_tile_k2<double, 2>(sj, smem, ctab, tile, ws);
+      else
+        run_tile_k2<float, 2>(sj, smem, ctab, tile, ws);
+    } else if (sj.prec == 1) {
       if (sj.kw == 1)
         run_tile<double, 1>(sj, smem, ctab, tile, ws);
       else

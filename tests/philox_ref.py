@@ -1,0 +1,51 @@
+"""Test-side Philox4x32-10 (Salmon et al., SC'11) and the Fisher-Yates chain the device runs.
+
+Used to predict, configuration by configuration, what the random mode evaluates: configuration g of
+a job is the (g - c)-th shuffle of the chain that starts at index c, each shuffle drawing Philox words
+with counter (block, iteration, chain_lo, chain_hi << 8 | part) and key (seed_lo, seed_hi), bounded
+like core/shuffle.h:28-32 of the reference: p = (x * i) >> 32.
+"""
+M0, M1 = 0xD2511F53, 0xCD9E8D57
+W0, W1 = 0x9E3779B9, 0xBB67AE85
+MASK = 0xFFFFFFFF
+
+# Published known-answer vectors of philox4x32-10 (Random123 distribution).
+KATS = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((MASK, MASK, MASK, MASK), (MASK, MASK), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+def philox4x32_10(ctr, key):
+    c0, c1, c2, c3 = ctr
+    k0, k1 = key
+    for _ in range(10):
+        p0 = M0 * c0
+        p1 = M1 * c2
+        c0, c1, c2, c3 = ((p1 >> 32) ^ c1 ^ k0) & MASK, p1 & MASK, ((p0 >> 32) ^ c3 ^ k1) & MASK, p0 & MASK
+        k0 = (k0 + W0) & MASK
+        k1 = (k1 + W1) & MASK
+    return c0, c1, c2, c3
+
+
+def shuffle(species, windows, seed, chain, iteration, part=0):
+    """One Fisher-Yates pass over every window, in place on a list."""
+    k = (seed & MASK, (seed >> 32) & MASK)
+    c_lo = chain & MASK
+    c_hi = (((chain >> 32) << 8) | part) & MASK
+    blk = 0
+    for lo, hi in windows:
+        i = hi - lo
+        while i > 1:
+            words = philox4x32_10((blk, iteration & MASK, c_lo, c_hi), k)
+            blk += 1
+            for x in words:
+                if i <= 1:
+                    break
+                p = (x * i) >> 32
+                a, b = lo + i - 1, lo + p
+                species[a], species[b] = species[b], species[a]
+                i -= 1
+    return species

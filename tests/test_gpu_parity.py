@@ -322,3 +322,74 @@ def test_fcc32_systematic_full_space_levels(prec):
         o, _ = oracle.evaluate(d[0], recs["species"][k], prec)
         assert o.tobytes() == recs["objective"][k].tobytes()
         assert oracle.rank_permutation(recs["species"][k]) == int(recs["id"][k])
+
+
+# --------------------------------------------------------------------------- RNG stream and fast path
+def _chain_starts(total):
+    """Chain start indices of the tile decomposition (16384 tiles of 128 threads)."""
+    per_tile = -(-total // 16384)
+    cpt = max(1, -(-per_tile // 128))
+    tc = cpt * 128
+    starts = []
+    for t0 in range(0, total, tc):
+        c = min(tc, total - t0)
+        base, rem = divmod(c, 128)
+        for t in range(128):
+            n = base + (1 if t < rem else 0)
+            if n:
+                starts.append((t0 + t * base + min(t, rem), n))
+    return starts
+
+
+@pytest.mark.parametrize("composition", [{"Ti": 16, "Al": 16}, {"Ti": 11, "Al": 11, "Nb": 10}],
+                         ids=["binary_fast_path", "ternary_general_path"])
+def test_random_stream_is_philox_fisher_yates(composition):
+    """Configuration g is the (g - c)-th Philox Fisher-Yates shuffle of the chain starting at c."""
+    import philox_ref
+
+    total = 2_097_153  # two configurations per chain
+    cfg = cases.fcc32("double", composition=composition, iterations=total, seed=0x1234_5678_9ABC)
+    c, d, pack, sp, bd, ob, ids = cases.trace(cfg, total)
+    assert np.array_equal(ids, np.arange(total, dtype=np.uint64))
+    starts = _chain_starts(total)
+    windows = [tuple(w) for w in d[0].windows.tolist()]
+    rng = np.random.default_rng(0)
+    for k in rng.choice(len(starts), size=48, replace=False):
+        start, n = starts[k]
+        conf = d[0].species_packed.tolist()
+        for it in range(n):
+            philox_ref.shuffle(conf, windows, cfg["seed"], start, it)
+            assert conf == sp[start + it].tolist(), (start, it)
+    assert cases.trace_mismatches(d, sp[:1500], bd[:1500], ob[:1500], "double") == []
+
+
+def test_fast_path_64_sites():
+    cfg = cases.fcc32("double", iterations=20000, pair_weights=None)
+    cfg["structure"]["supercell"] = [2, 2, 4]
+    cfg["composition"] = {"Ti": 32, "Al": 32}
+    c, d, pack, sp, bd, ob, ids = cases.trace(cfg, 20000)
+    assert len(d[0].species_packed) == 64
+    assert cases.trace_mismatches(d, sp, bd, ob, "double") == []
+
+
+@pytest.mark.parametrize("prec", ["double", "single"])
+def test_fast_path_partial_window_systematic(prec):
+    """A 20-site window inside a 64-site cell of the same background species (two species overall)."""
+    cfg = cases.fcc32(prec, iteration_mode="systematic", seed=None, iterations=None, keep=4, pair_weights=None)
+    cfg["structure"]["supercell"] = [2, 2, 4]
+    cfg["structure"]["species"] = [1] * 4
+    cfg["composition"] = {"sites": list(range(20)), "Ti": 10, "H": 10}
+    c, d, pack, sp, bd, ob, ids = cases.trace(cfg, 184756)
+    assert c.iterations == 184756 and len(ob) == 184756
+    assert sorted(ids.tolist()) == list(range(1, 184757))
+    rows = np.random.default_rng(1).choice(184756, size=3000, replace=False)
+    assert cases.trace_mismatches(d, sp[rows], bd[rows], ob[rows], prec) == []
+    for k in rows[:200]:
+        exp = oracle.unrank_permutation(d[0].species_packed[d[0].windows[0][0]:d[0].windows[0][1]], int(ids[k]))
+        lo, hi = d[0].windows[0]
+        got = sp[k, lo:hi]
+        uniq = sorted(set(d[0].species_packed[lo:hi].tolist()))
+        assert np.array_equal(got, np.array([uniq[x] for x in exp], np.uint8))
+    c2, d2, recs, levels, info = native_run(cfg)
+    lv = oracle.systematic_levels(d2[0], prec=prec, keep=4)
+    assert levels == lv
