@@ -209,6 +209,22 @@ sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t ca
  * kind 0: shared-memory load bandwidth (bytes/s); kind 1: 32-bit integer lane operations per second. */
 sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds);
 
+/* Allocation-free variant of sqsg_optimize, for callers that cannot allocate device memory (a host
+ * framework that owns the whole device budget through its own pool, a process whose memory is capped
+ * once work starts). No counterpart in the reference. It runs the same engine kernel, but all of its
+ * device scratch lives in one static __device__ array of about 3.6 MiB that every GPU loading this
+ * library holds until exit, and it calls no cudaMalloc/cudaFree or other allocating routine.
+ * Outputs: the keep+1 best objectives with exact counts and id checksums (*n_levels: in = capacity,
+ * out = count) and the statistics — the values sqsg_run_levels / sqsg_run_statistics give for the same
+ * job — but no configuration records. Limits: staged job data <= 3 MiB, <= 16448 tiles; no callback
+ * or cancellation; `stream` may be NULL (legacy default stream). The first call on a device looks up
+ * the array's device address, so make it before any stream capture. Calls share the array: the call
+ * resets what must start at zero and serialises calls from one process, but calls that overlap on the
+ * GPU (another process, or work still running on the same context) race. Messages go to err. */
+sqsg_status sqsg_optimize_levels_noalloc(const sqsg_job* job, void* stream, uint32_t* n_levels, double* values,
+                                         uint64_t* counts, uint64_t* checksums, sqsg_statistics* stats, char* err,
+                                         size_t err_len);
+
 /* ------------------------------------------------------------------------------------------------
  * Batched form: many independent jobs in one persistent launch fed by a device tile queue
  * (no reference counterpart; the reference runs one configuration per call).

@@ -34,7 +34,7 @@ EXPORTED = (
     "sqsg_num_permutations", "sqsg_rank_permutation", "sqsg_unrank_permutation",
     "sqsg_optimize", "sqsg_run_count", "sqsg_run_copy", "sqsg_run_statistics", "sqsg_run_free",
     "sqsg_optimize_trace", "sqsg_optimize_batch", "sqsg_run_levels", "sqsg_run_info",
-    "sqsg_microbench", "sqsg_run_transfer",
+    "sqsg_microbench", "sqsg_run_transfer", "sqsg_optimize_levels_noalloc",
 )
 
 
@@ -143,6 +143,8 @@ def lib():
         L.sqsg_run_levels.argtypes = [vp, C.POINTER(u32), vp, vp, vp]
         L.sqsg_run_info.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.sqsg_run_transfer.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
+        L.sqsg_optimize_levels_noalloc.argtypes = [C.POINTER(SqsgJob), vp, C.POINTER(u32), vp, vp, vp,
+                                                   C.POINTER(SqsgStatistics), C.c_char_p, C.c_size_t]
         L.sqsg_microbench.argtypes = [C.c_int, C.c_int, C.POINTER(dbl), C.POINTER(dbl)]
         for name in EXPORTED:
             if name not in ("sqsg_version", "sqsg_last_error", "sqsg_device_count", "sqsg_run_count",
