@@ -44,6 +44,16 @@ def workload_config(name: str):
         return cases.fcc32("double", iterations=1_000_000, seed=42), (
             "fcc 2x2x2 (32 sites) A16B16 random, 1e6 Philox Fisher-Yates configurations, 2 shells, weights 1.0/0.5, "
             "pair weights 1, keep 10, float64")
+    if name == "quinary":
+        return cases.quinary("double", cells=(4, 4, 4), iterations=20_000_000, seed=0, keep=10,
+                             composition={"Ti": 52, "Al": 51, "Nb": 51, "V": 51, "Zr": 51}), (
+            "fcc 4x4x4 (256 sites) A52B51C51D51E51 random, 3 shells (12/6/24, P=5376), weights 1.0/0.5/0.25, "
+            "64 independent chains of 2e7 configurations (seeds 0..63) in one batched launch, float64")
+    if name == "split":
+        return cases.rocksalt_split("double", cells=(3, 3, 3), iterations=500_000_000, seed=1,
+                                    composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}]), (
+            "rocksalt 3x3x3 (216 sites) split: Ti54Al54 cations and N96B12 anions optimised together, 2 shells per "
+            "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations, float64")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -93,22 +103,43 @@ class ClockSampler:
                 "samples": len(rows), "reasons": reasons}
 
 
-def cpu_sample(seconds: float, keep: int):
-    """The restated reference loop (oracle, oracle geometry) over a bounded contiguous rank range, all
-    host threads."""
+def cpu_sample(seconds: float, keep: int, workload: str = "systematic"):
+    """The restated reference loop (oracle, on oracle geometry for the systematic cell) over a bounded
+    sample, all host threads. Returns (configurations, seconds, threads, description)."""
     import cases
     import oracle
 
-    sd = cases.oracle_fcc32()
     threads = os.cpu_count() or 1
+    if workload == "systematic":
+        sd = cases.oracle_fcc32()
+        t = time.perf_counter()
+        oracle.systematic_levels(sd, keep=keep, threads=threads, first=0, count=2_000_000)
+        rate = 2_000_000 / (time.perf_counter() - t)
+        count = int(min(rate * seconds, 601_080_390))
+        t = time.perf_counter()
+        oracle.systematic_levels(sd, keep=keep, threads=threads, first=0, count=count)
+        dt = time.perf_counter() - t
+        return count, dt, threads, (
+            f"ranks 1..{count} (contiguous prefix) of the 601,080,390-rank space through the restated reference loop "
+            f"(unrank + count_bonds + compute_objective + next_permutation) on {threads} threads; the result "
+            "collection is replaced by per-objective counting")
+    import sqsgenerator_b200 as S
+
+    cfg, _ = workload_config(workload)
+    c = S.parse_config(cfg)
+    d = S.prepare(c)
+    mode = "split" if workload == "split" else "interact"
+    probe = 20_000
     t = time.perf_counter()
-    oracle.systematic_levels(sd, keep=keep, threads=threads, first=0, count=2_000_000)
-    rate = 2_000_000 / (time.perf_counter() - t)
-    count = int(min(rate * seconds, 601_080_390))
+    oracle.optimize(d, iterations=probe, keep=c.keep, threads=threads, sublattice_mode=mode)
+    rate = probe / (time.perf_counter() - t)
+    count = max(probe, int(rate * seconds))
     t = time.perf_counter()
-    oracle.systematic_levels(sd, keep=keep, threads=threads, first=0, count=count)
+    _, st = oracle.optimize(d, iterations=count, keep=c.keep, threads=threads, sublattice_mode=mode)
     dt = time.perf_counter() - t
-    return count, dt, threads
+    return count, dt, threads, (
+        f"{count} random configurations through the restated reference optimizer loop (rapidrand shuffler shared by "
+        f"{threads} threads, chunk 100000, result collection) of the same structure")
 
 
 def run_reference(args):
@@ -119,16 +150,12 @@ def run_reference(args):
     cfg, desc = workload_config(args.workload)
     per_step = []
     for step in range(args.warmup + args.steps):
-        count, dt, threads = cpu_sample(args.ref_seconds, cfg["keep"])
+        count, dt, threads, sample = cpu_sample(args.ref_seconds, cfg["keep"], args.workload)
         if step >= args.warmup:
             per_step.append((count, dt))
     configs = sum(x[0] for x in per_step)
     secs = sum(x[1] for x in per_step)
     value = configs / secs
-    sample = (f"ranks 1..{per_step[0][0]} of the 601,080,390-rank space per step (contiguous prefix), restated "
-              "reference loop: unrank + count_bonds + compute_objective + next_permutation; the result collection "
-              "is replaced by per-objective counting (the reference would store every configuration at or below "
-              "the 11th best objective)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "configs/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / len(per_step) * 1e3,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -142,6 +169,7 @@ def run_b200(args):
     import numpy as np
     import torch
 
+    import cases as _cases
     import sqsgenerator_b200 as S
     from sqsgenerator_b200 import _native as N
     from sqsgenerator_b200.optimize import build_job
@@ -161,41 +189,67 @@ def run_b200(args):
     cfg, desc = workload_config(args.workload)
     c = S.parse_config(cfg)
     d = S.prepare(c)
-    total = c.iterations if not args.limit else min(args.limit, c.iterations)
-    share, rem = divmod(total, world)
+    n_jobs = 64 if args.workload == "quinary" else 1
+    per_job = c.iterations if not args.limit else min(args.limit, c.iterations)
+    total = per_job * n_jobs
+    # one GPU's share: contiguous ranges of the configuration space (jobs keep their own seeds)
+    share, rem = divmod(per_job, world)
     first = rank * share + min(rank, rem)
     count = share + (1 if rank < rem else 0)
-    job, bufs = build_job(c, d, device=device)
-    job.range_first = first
-    job.range_count = count
-    job.max_results = args.max_results
+    jobs = (N.SqsgJob * n_jobs)()
+    keep_alive = []
+    for k in range(n_jobs):
+        if n_jobs > 1:
+            cfg_k = dict(cfg, seed=k)
+            ck = S.parse_config(cfg_k)
+        else:
+            ck = c
+        job, bufs = build_job(ck, d, device=device)
+        job.range_first = first
+        job.range_count = count
+        job.max_results = args.max_results
+        jobs[k] = job
+        keep_alive.append(bufs)
     L = N.lib()
-    P = len(d[0].pairs)
-    nsp = len(d[0].species_packed)
-    nsro = d[0].prefactors.size
+    P_total = sum(len(x.pairs) for x in d)
+    nsp = sum(len(x.species_packed) for x in d)
+    nsro = sum(x.prefactors.size for x in d)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
 
     def step():
-        run = C.c_void_p()
+        runs = (C.c_void_p * n_jobs)()
         t0 = time.perf_counter()
-        N.check(L.sqsg_optimize(C.byref(job), C.byref(run)))
-        n = int(L.sqsg_run_count(run))
-        obj = np.empty(max(n, 1), np.float64)
-        sp = np.empty(max(n, 1) * nsp, np.uint8)
-        sro = np.empty(max(n, 1) * nsro, np.float64)
-        ids = np.empty(max(n, 1), np.uint64)
-        N.check(L.sqsg_run_copy(run, 0, n, N.ptr(obj), None, N.ptr(sp), N.ptr(sro), N.ptr(ids)))
+        if n_jobs == 1:
+            N.check(L.sqsg_optimize(C.byref(jobs[0]), C.cast(runs, C.POINTER(C.c_void_p))))
+        else:
+            N.check(L.sqsg_optimize_batch(jobs, n_jobs, C.cast(runs, C.POINTER(C.c_void_p))))
+        results = 0
+        for k in range(n_jobs):
+            run = runs[k]
+            n = int(L.sqsg_run_count(run))
+            obj = np.empty(max(n, 1), np.float64)
+            sp = np.empty(max(n, 1) * nsp, np.uint8)
+            sro = np.empty(max(n, 1) * nsro, np.float64)
+            ids = np.empty(max(n, 1), np.uint64)
+            N.check(L.sqsg_run_copy(run, 0, n, N.ptr(obj), None, N.ptr(sp), N.ptr(sro), N.ptr(ids)))
+            results += n
         wall = time.perf_counter() - t0
-        st = N.SqsgStatistics()
-        N.check(L.sqsg_run_statistics(run, C.byref(st)))
-        h2d, d2h = C.c_uint64(), C.c_uint64()
-        N.check(L.sqsg_run_transfer(run, C.byref(h2d), C.byref(d2h)))
-        import cases as _cases
-
-        levels = _cases.run_levels(run)
-        L.sqsg_run_free(run)
-        return dict(wall=wall, loop=st.timings_ns[2] * 1e-9, finished=int(st.finished), results=n,
-                    h2d=h2d.value, d2h=d2h.value, levels=levels)
+        finished = 0
+        h2d = d2h = 0
+        for k in range(n_jobs):
+            st = N.SqsgStatistics()
+            N.check(L.sqsg_run_statistics(runs[k], C.byref(st)))
+            finished += int(st.finished)
+            a, b = C.c_uint64(), C.c_uint64()
+            N.check(L.sqsg_run_transfer(runs[k], C.byref(a), C.byref(b)))
+            h2d += a.value
+            d2h += b.value
+            if k == 0:
+                loop = st.timings_ns[2] * 1e-9
+        levels = _cases.run_levels(runs[0])
+        for k in range(n_jobs):
+            L.sqsg_run_free(runs[k])
+        return dict(wall=wall, loop=loop, finished=finished, results=results, h2d=h2d, d2h=d2h, levels=levels)
 
     for _ in range(args.warmup):
         step()
@@ -250,31 +304,29 @@ def run_b200(args):
     int_rate, _ = N.microbench(1, device)
     launch_s = loop / args.steps
     configs_per_launch = finished / args.steps / world
-    alg_bytes = 2 * P * configs_per_launch
+    alg_bytes = 2 * P_total * configs_per_launch
     achieved = alg_bytes / launch_s / 1e9
-    prof = os.path.join(ROOT, "profiles", "sqsg_engine_fcc32_systematic.json")
+    prof = os.path.join(ROOT, "profiles", f"sqsg_engine_{args.workload}.json")
     traffic = None
     if os.path.exists(prof):
         traffic = json.load(open(prof)).get("dram_bytes_per_launch")
     roofline = {"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
                 "frac": achieved / (smem_bw / 1e9), "traffic": traffic,
                 "peak_source": "measured in this run: conflict-free LDS.32 microbenchmark (sqsg_microbench kind 0)",
-                "algorithmic": f"2*P = {2 * P} B of shared-memory species reads per configuration",
-                "int32_frac": (3 * P * configs_per_launch / launch_s) / int_rate,
+                "algorithmic": f"2*P = {2 * P_total} B of shared-memory species reads per configuration",
+                "int32_frac": (3 * P_total * configs_per_launch / launch_s) / int_rate,
                 "int32_peak_ops": int_rate}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        n, dt, threads = cpu_sample(args.cpu_seconds, c.keep)
-        cpu = {"value": n / dt, "unit": "configs/s", "cores": threads, "kind": "port",
-               "sample": f"ranks 1..{n} (contiguous prefix) through the restated reference loop on {threads} threads; "
-                         "result collection replaced by per-objective counting"}
+        n, dt, threads, sample = cpu_sample(args.cpu_seconds, c.keep, args.workload)
+        cpu = {"value": n / dt, "unit": "configs/s", "cores": threads, "kind": "port", "sample": sample}
     line = {"metric": METRIC, "value": value, "unit": "configs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": loop / args.steps * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "configs_per_step": total, "sites": nsp, "pairs": P,
+            "config": {"workload": desc, "configs_per_step": total, "sites": nsp, "pairs": P_total, "jobs": n_jobs,
                        "l2": "flushed between timed steps (256 MiB device write)",
                        "max_results": args.max_results,
-                       "parallelism": f"rank space split into {world} contiguous ranges"},
+                       "parallelism": f"configuration space split into {world} contiguous ranges"},
             "e2e": {"value": e2e, "unit": "configs/s", "h2d_bytes_per_step": out[-1]["h2d"],
                     "d2h_bytes_per_step": out[-1]["d2h"], "ms_per_step": wall / args.steps * 1e3},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": args.steps,
@@ -290,12 +342,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="systematic", choices=["systematic"])
+    ap.add_argument("--workload", default="systematic", choices=["systematic", "random", "quinary", "split"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--limit", type=int, default=0, help="evaluate only the first LIMIT ranks (profiling)")
-    ap.add_argument("--max-results", type=int, default=1 << 20,
+    ap.add_argument("--max-results", type=int, default=1 << 16,
                     help="record capacity per step; the exact objective levels do not depend on it")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -23,6 +23,7 @@
 
 #include "engine_device.cuh"
 #include "sqsg_internal.h"
+#include "tiles.h"
 
 namespace sqsg {
 
@@ -293,30 +294,28 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     if (!k2d.first.empty()) std::memcpy(base + P.k2_off, k2d.first.data(), 4 * k2d.first.size());
     if (!k2d.second.empty()) std::memcpy(base + P.k2_shell_off, k2d.second.data(), 4 * k2d.second.size());
   }
+  // binary systematic path: binomials C(m, j) for m <= window size, j <= ones in the window, kept in
+  // global memory after the staged sections (read through the L1 by the per-thread unrank)
+  if (d.k2 && pj.systematic) {
+    PartDesc& P = d.parts[0];
+    const uint32_t n = job.sublattices[0].windows[1] - job.sublattices[0].windows[0];
+    const uint32_t ones = P.unrank_hist[1], cols = ones + 1;
+    const size_t off = align_up(pj.blob.size(), 16);
+    pj.blob.resize(off + 8ull * (n + 1) * cols, 0);
+    P.k2_binom_off = static_cast<uint32_t>(off);
+    unsigned long long* b = reinterpret_cast<unsigned long long*>(pj.blob.data() + off);
+    for (uint32_t m = 0; m <= n; ++m)
+      for (uint32_t j = 0; j <= ones; ++j)
+        b[m * cols + j] = (j == 0) ? 1ull : (m == 0 ? 0ull : b[(m - 1) * cols + j - 1] + b[(m - 1) * cols + j]);
+  }
   return pj;
 }
 
-// Tiles depend only on the job, never on the device, so a seeded run evaluates the same
-// configurations on every GPU: about 16384 tiles of kBlock threads, each thread running
-// configs_per_thread configurations.
 static void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles) {
-  const uint64_t first = pj.range_first;
-  const uint64_t total = pj.range_count;
-  if (total == 0) return;
-  const uint64_t per_tile_target = (total + 16383) / 16384;
-  uint64_t cpt = std::max<uint64_t>(1, (per_tile_target + kBlock - 1) / kBlock);
-  cpt = std::min<uint64_t>(cpt, 1u << 16);
-  pj.configs_per_thread = static_cast<uint32_t>(cpt);
-  const uint64_t tile_configs = cpt * kBlock;
-  uint64_t done = 0;
-  while (done < total) {
-    Tile t{};
+  for_each_tile(pj.range_first, pj.range_count, pj.systematic, [&](Tile t) {
     t.job = job_index;
-    t.count = std::min(tile_configs, total - done);
-    t.start = first + done + (pj.systematic ? 1 : 0);
     tiles.push_back(t);
-    done += t.count;
-  }
+  });
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -15,6 +15,7 @@
 namespace sqsg {
 
 constexpr int kBlock = 128;       // threads per CTA (each owns one configuration)
+constexpr int kMinBlocks = 5;     // CTAs per SM the register budget must allow (<= 102 registers)
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
 constexpr int kMaxSpecies = 8;    // K per part handled by the packed-row counter
@@ -73,7 +74,8 @@ struct PartDesc {
   // binary fast path (K == 2, N <= 64): per (shell, site) neighbour masks, see run_tile_k2
   uint32_t k2_off;        // entries: uint4 {mask lo, mask hi, site | shell << 8, popcount}
   uint32_t k2_entries;
-  uint32_t k2_shell_off;  // S u32: pairs per shell
+  uint32_t k2_shell_off;  // S x (pairs in shell, end of its entries)
+  uint32_t k2_binom_off;  // blob offset (global, not staged) of C(m, j), m <= window, j <= ones
 };
 
 struct JobDesc {

@@ -475,7 +475,7 @@ template <class T> __device__ __forceinline__ T load_threshold(const JobDesc& J)
 
 // ------------------------------------------------------------------------------ one tile
 template <class T, int KW>
-__device__ __noinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+__device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                       WarpState& ws) {
   using F = FP<T>;
   const int t = threadIdx.x;
@@ -603,7 +603,7 @@ __device__ __forceinline__ void k2_materialize(uint8_t* smem, const PartDesc& P,
 }
 
 template <class T, int W>
-__device__ __noinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+__device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                          WarpState& ws) {
   using V = typename Word<W>::type;
   const int t = threadIdx.x;
@@ -632,18 +632,19 @@ __device__ __noinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, LevelS
     wn = win[1] - win[0];
     wshift = N - win[1];
     wmask = low_mask<V>(wn) << wshift;
-    if (my_count > 0) {  // core/permutation.h:52-78 for two species
-      uint64_t rank = tile.start + my_off, total = J.total;
-      uint32_t h0 = P.unrank_hist[0], h1 = P.unrank_hist[1];
+    if (my_count > 0) {
+      // core/permutation.h:52-78 for two species: the arrangements of the remaining m positions that
+      // start with species 0 number total*h0/m = C(m-1, h1), read from the job's binomial table.
+      const unsigned long long* binom = reinterpret_cast<const unsigned long long*>(J.blob + P.k2_binom_off);
+      const uint32_t cols = P.unrank_hist[1] + 1;
+      uint64_t rank = tile.start + my_off;
+      uint32_t h1 = P.unrank_hist[1];
       V word = 0;
       for (uint32_t k = 0; k < wn; ++k) {
-        const uint64_t s0 = div_96x32(mul_64x32(total, h0), wn - k, nullptr);
-        if (rank <= s0) {
-          total = s0;
-          --h0;
-        } else {
+        const uint32_t m = wn - k;
+        const uint64_t s0 = h1 <= m - 1 ? __ldg(&binom[(m - 1) * cols + h1]) : 0ull;
+        if (rank > s0) {
           rank -= s0;
-          total = div_96x32(mul_64x32(total, h1), wn - k, nullptr);
           --h1;
           word |= V(1) << (wn - 1 - k);
         }
@@ -713,7 +714,7 @@ __device__ __noinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, LevelS
 // Tiles are taken from q->head with one atomicAdd per tile. A CTA stages a job's read-only data
 // (cubes, windows, pair stream, packed species) into shared memory with non-multicast bulk copies
 // whenever its next tile belongs to a different job.
-__global__ void __launch_bounds__(kBlock) sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(kBlock, kMinBlocks) sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
                                                       uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
                                                       unsigned long long* status) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -731,17 +732,18 @@ __global__ void __launch_bounds__(kBlock) sqsg_engine(const JobDesc* __restrict_
   uint32_t phase = 0;
   WarpState ws;
   ws.reset();
+  if (threadIdx.x == 0) s_tile = (cancel && *cancel) ? n_tiles : atomicAdd(&q->head, 1u);
   for (;;) {
-    if (threadIdx.x == 0) {
-      uint32_t ti = n_tiles;
-      if (!(cancel && *cancel)) ti = atomicAdd(&q->head, 1u);
-      s_tile = ti;
-    }
-    __syncthreads();
+    __syncthreads();  // s_tile visible; every thread is done with the previous tile
     const uint32_t ti = s_tile;
     if (ti >= n_tiles) break;
+    // the next tile index is fetched now and only consumed after this tile: its latency hides
+    uint32_t next = n_tiles;
+    if (threadIdx.x == 0 && !(cancel && *cancel)) next = atomicAdd(&q->head, 1u);
     const Tile tile = tiles[ti];
     if (static_cast<int>(tile.job) != cur) {
+      if (cur >= 0) flush_levels(ctab, sj);  // the previous job's levels leave before its descriptor
+      __syncthreads();
       const uint32_t* src = reinterpret_cast<const uint32_t*>(&jobs[tile.job]);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&sj);
       for (uint32_t i = threadIdx.x; i < sizeof(JobDesc) / 4; i += kBlock) dst[i] = src[i];
@@ -789,14 +791,14 @@ __global__ void __launch_bounds__(kBlock) sqsg_engine(const JobDesc* __restrict_
       else
         run_tile<float, 2>(sj, smem, ctab, tile, ws);
     }
-    __syncthreads();
-    flush_levels(ctab, sj);
-    __syncthreads();
+    __syncthreads();  // every thread is done with this tile before s_tile changes
     if (threadIdx.x == 0) {
+      s_tile = next;
       atomicAdd(&sj.counters[kFinished], static_cast<unsigned long long>(tile.count));
       atomicAdd(&sj.counters[kTilesDone], 1ull);
     }
   }
+  if (cur >= 0) flush_levels(ctab, sj);
 }
 
 }  // namespace sqsg

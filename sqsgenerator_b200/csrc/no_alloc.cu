@@ -27,10 +27,11 @@
 #include "engine.cuh"
 #include "permutation.h"
 #include "sqsg_internal.h"
+#include "tiles.h"
 
 namespace sqsg {
 
-__global__ void __launch_bounds__(kBlock) sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(kBlock, kMinBlocks) sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
                                                       uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
                                                       unsigned long long* status);
 
@@ -265,23 +266,17 @@ static Err prepare(const sqsg_job& job, JobDesc& d, size_t& blob_size, size_t& n
   const uint64_t count = job.range_count ? job.range_count : total - job.range_first;
   if (count > total - job.range_first) NA_FAIL(SQSG_ERR_OUT_OF_RANGE, "range beyond the configuration space");
   d.trace_base = job.range_first + (systematic ? 1 : 0);
-  // tiles: the same decomposition as sqsg_optimize
+  // tiles: the same decomposition as sqsg_optimize (tiles.h)
   n_tiles = 0;
-  if (count) {
-    const uint64_t per_tile_target = (count + 16383) / 16384;
-    uint64_t cpt = std::max<uint64_t>(1, (per_tile_target + kBlock - 1) / kBlock);
-    cpt = std::min<uint64_t>(cpt, 1u << 16);
-    const uint64_t tile_configs = cpt * kBlock;
-    if ((count + tile_configs - 1) / tile_configs > kMaxTiles)
-      NA_FAIL(SQSG_ERR_CAPACITY, "the job needs more tiles than the static tile list holds");
-    for (uint64_t done = 0; done < count;) {
-      Tile& t = g_stage_tiles[n_tiles++];
-      std::memset(&t, 0, sizeof(t));
-      t.count = std::min(tile_configs, count - done);
-      t.start = job.range_first + done + (systematic ? 1 : 0);
-      done += t.count;
-    }
-  }
+  bool too_many = false;
+  for_each_tile(job.range_first, count, systematic, [&](const Tile& t) {
+    if (n_tiles < kMaxTiles)
+      g_stage_tiles[n_tiles] = t;
+    else
+      too_many = true;
+    ++n_tiles;
+  });
+  if (too_many) NA_FAIL(SQSG_ERR_CAPACITY, "the job needs more tiles than the static tile list holds");
   return kOk;
 }
 

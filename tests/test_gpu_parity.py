@@ -326,18 +326,21 @@ def test_fcc32_systematic_full_space_levels(prec):
 
 # --------------------------------------------------------------------------- RNG stream and fast path
 def _chain_starts(total):
-    """Chain start indices of the tile decomposition (16384 tiles of 128 threads)."""
-    per_tile = -(-total // 16384)
-    cpt = max(1, -(-per_tile // 128))
-    tc = cpt * 128
+    """Chain start indices of the guided tile decomposition (csrc/tiles.h): each tile takes about
+    1/2048 of what is left, at least `floor` configurations per thread, 128 threads per tile."""
+    floor = max(1, min(16, total // (128 * 8192)))
     starts = []
-    for t0 in range(0, total, tc):
-        c = min(tc, total - t0)
+    done = 0
+    while done < total:
+        left = total - done
+        cpt = min(max(-(-left // (128 * 2048)), floor), 1 << 16)
+        c = min(cpt * 128, left)
         base, rem = divmod(c, 128)
         for t in range(128):
             n = base + (1 if t < rem else 0)
             if n:
-                starts.append((t0 + t * base + min(t, rem), n))
+                starts.append((done + t * base + min(t, rem), n))
+        done += c
     return starts
 
 
@@ -347,7 +350,7 @@ def test_random_stream_is_philox_fisher_yates(composition):
     """Configuration g is the (g - c)-th Philox Fisher-Yates shuffle of the chain starting at c."""
     import philox_ref
 
-    total = 2_097_153  # two configurations per chain
+    total = 2_097_153
     cfg = cases.fcc32("double", composition=composition, iterations=total, seed=0x1234_5678_9ABC)
     c, d, pack, sp, bd, ob, ids = cases.trace(cfg, total)
     assert np.array_equal(ids, np.arange(total, dtype=np.uint64))
