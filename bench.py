@@ -193,9 +193,9 @@ def run_b200(args):
     per_job = c.iterations if not args.limit else min(args.limit, c.iterations)
     total = per_job * n_jobs
     # one GPU's share: contiguous ranges of the configuration space (jobs keep their own seeds)
-    share, rem = divmod(per_job, world)
-    first = rank * share + min(rank, rem)
-    count = share + (1 if rank < rem else 0)
+    from sqsgenerator_b200.shard import merge_levels, shard_range
+
+    first, count = shard_range(per_job, world, rank)
     jobs = (N.SqsgJob * n_jobs)()
     keep_alive = []
     for k in range(n_jobs):
@@ -283,15 +283,7 @@ def run_b200(args):
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    # merge the ranks' objective levels (exact counts and checksums add up)
-    merged = {}
-    for lv in gathered:
-        for v, n, cs in lv:
-            a = merged.setdefault(v, [0, 0, 0])
-            a[0] += n
-            a[1] = (a[1] + (cs & 0xFFFFFFFF)) & 0xFFFFFFFF
-            a[2] = (a[2] + (cs >> 32)) & 0xFFFFFFFF
-    levels = [(v, a[0], a[1] | (a[2] << 32)) for v, a in sorted(merged.items())][: c.keep + 1]
+    levels = merge_levels(gathered, c.keep)  # exact: counts and checksum halves add up
     parity = None
     golden_path = os.path.join(ROOT, "tests", "golden", "fcc32_systematic_levels.json")
     if args.workload == "systematic" and not args.limit and os.path.exists(golden_path):

@@ -97,6 +97,8 @@ def lib():
         L.oracle_evaluate_d.argtypes = [C.POINTER(Sublattice), C.c_void_p, C.c_void_p]
         L.oracle_evaluate_f.restype = C.c_float
         L.oracle_evaluate_f.argtypes = [C.POINTER(Sublattice), C.c_void_p, C.c_void_p]
+        L.oracle_evaluate_many.argtypes = [C.POINTER(Sublattice), C.c_int, C.c_uint64, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]
         L.oracle_optimize.restype = C.c_void_p
         L.oracle_optimize.argtypes = [C.POINTER(Job)]
         L.oracle_result_free.argtypes = [C.c_void_p]
@@ -230,6 +232,19 @@ def evaluate(sd, species, prec="double"):
     else:
         o = lib().oracle_evaluate_f(C.byref(s), _ptr(sp), _ptr(sro))
     return T(o), sro.reshape(S, K, K)
+
+
+def evaluate_many(sd, species, prec="double"):
+    """(bonds[n, S, K, K] ordered counts, objectives[n]) of many configurations at once."""
+    T = np.float64 if prec in ("double", 1, np.float64) else np.float32
+    s, keep = make_sublattice(sd, T)
+    S, K = s.n_shells, s.n_species
+    sp = np.ascontiguousarray(species, dtype=np.uint8)
+    n = sp.shape[0]
+    bonds = np.zeros((n, S * K * K), dtype=np.uint64)
+    obj = np.zeros(n, dtype=T)
+    lib().oracle_evaluate_many(C.byref(s), 1 if T is np.float64 else 0, n, _ptr(sp), _ptr(bonds), _ptr(obj))
+    return bonds.reshape(n, S, K, K), obj
 
 
 def optimize(sublattices, *, prec="double", iteration_mode="random", sublattice_mode="interact",

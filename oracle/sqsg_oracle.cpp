@@ -624,6 +624,25 @@ static std::map<T, LevelAcc> systematic_levels(const oracle_sublattice& d, int t
   return all;
 }
 
+// count_bonds + compute_objective for n configurations (species n x N): ordered bonds row-major
+// (n x S*K*K) and objectives (n values of the job's precision).
+template <class T>
+static void evaluate_many(const oracle_sublattice* d, uint64_t n, const uint8_t* species, uint64_t* bonds_rm, T* obj) {
+  Sublattice<T> sl;
+  sl.load(*d);
+  const size_t skk = static_cast<size_t>(sl.S) * sl.K * sl.K;
+  std::vector<uint64_t> b(skk);
+  std::vector<T> sro(skk);
+  for (uint64_t k = 0; k < n; ++k) {
+    const uint8_t* sp = species + k * sl.n_sites;
+    count_bonds(b, sl.pairs, sp, sl.S, sl.K);
+    obj[k] = compute_objective(sro, b, sl);
+    for (int s = 0; s < sl.S; ++s)
+      for (int a = 0; a < sl.K; ++a)
+        for (int c = 0; c < sl.K; ++c) bonds_rm[k * skk + (static_cast<size_t>(s) * sl.K + a) * sl.K + c] = b[sl.cidx(s, a, c)];
+  }
+}
+
 struct Handle {
   int prec;
   void* out;
@@ -705,6 +724,14 @@ float oracle_evaluate_f(const oracle_sublattice* d, const uint8_t* species, floa
     for (int a = 0; a < sl.K; ++a)
       for (int c = 0; c < sl.K; ++c) sro_rm[(static_cast<size_t>(s) * sl.K + a) * sl.K + c] = sro[sl.cidx(s, a, c)];
   return o;
+}
+
+void oracle_evaluate_many(const oracle_sublattice* d, int prec, uint64_t n, const uint8_t* species, uint64_t* bonds,
+                          void* obj) {
+  if (prec == 1)
+    evaluate_many<double>(d, n, species, bonds, static_cast<double*>(obj));
+  else
+    evaluate_many<float>(d, n, species, bonds, static_cast<float*>(obj));
 }
 
 void* oracle_optimize(const oracle_job* job) {

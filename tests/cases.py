@@ -93,27 +93,26 @@ def trace(config, capacity):
 
 
 def trace_mismatches(d, sp, bd, ob, prec, limit=None):
-    """Recompute bonds and objective of every traced configuration with the oracle; count mismatches."""
+    """Recompute ordered bonds and objective of every traced configuration with the oracle; return
+    the mismatching rows."""
+    n = len(ob) if limit is None else min(limit, len(ob))
+    T = np.float64 if prec in ("double", 1) else np.float32
     bad = []
-    rows = range(len(ob)) if limit is None else range(min(limit, len(ob)))
-    for k in rows:
-        o1 = o2 = 0
-        total = None
-        for part in d:
-            n = len(part.species_packed)
-            skk = part.prefactors.size
-            species = sp[k, o1:o1 + n]
-            b = oracle.count_bonds(part, species).reshape(-1)
-            if not np.array_equal(b.astype(np.uint32), bd[k, o2:o2 + skk]):
-                bad.append((k, "bonds"))
-                break
-            o, _ = oracle.evaluate(part, species, prec)
-            total = o if total is None else type(o)(total + o)
-            o1 += n
-            o2 += skk
-        else:
-            if total.tobytes() != ob[k].tobytes():
-                bad.append((k, "objective", total, ob[k]))
+    total = None
+    bonds_ok = np.ones(n, dtype=bool)
+    o1 = o2 = 0
+    for part in d:
+        npart = len(part.species_packed)
+        skk = part.prefactors.size
+        b, o = oracle.evaluate_many(part, sp[:n, o1:o1 + npart], prec)
+        bonds_ok &= np.all(b.reshape(n, skk).astype(np.uint32) == bd[:n, o2:o2 + skk], axis=1)
+        total = o if total is None else (total + o).astype(T)
+        o1 += npart
+        o2 += skk
+    obj_ok = total.view(np.uint32 if T is np.float32 else np.uint64) == np.asarray(ob[:n], T).view(
+        np.uint32 if T is np.float32 else np.uint64)
+    for k in np.flatnonzero(~(bonds_ok & obj_ok))[:20]:
+        bad.append((int(k), "bonds" if not bonds_ok[k] else "objective", total[k], ob[k]))
     return bad
 
 
