@@ -231,6 +231,38 @@ sqsg_status sqsg_optimize_levels_noalloc(const sqsg_job* job, void* stream, uint
  */
 sqsg_status sqsg_optimize_batch(const sqsg_job* jobs, uint32_t n_jobs, sqsg_run** runs);
 
+/* ------------------------------------------------------------------------------------------------
+ * Served form: continuous batching (no reference counterpart). Jobs submitted while others run are
+ * admitted as job slots, ring space and device memory (data + records: the job's footprint) free up;
+ * their tiles join a persistent kernel that is already running. A job's result is the same as from
+ * sqsg_optimize: it depends only on the job.
+ */
+typedef struct sqsg_server sqsg_server;
+
+typedef struct {
+  int32_t device;
+  uint32_t max_jobs;              /* jobs admitted at once (0: 256) */
+  uint64_t arena_bytes;           /* device memory for admitted jobs' data and records (0: 4 GiB) */
+  uint64_t default_max_results;   /* record capacity of a job that leaves max_results at 0 (0: 65536) */
+} sqsg_server_options;
+
+typedef struct {
+  uint64_t submitted, admitted, completed, pending, active;
+  uint64_t configurations;        /* evaluated by completed jobs */
+  uint64_t launches;              /* persistent-kernel launches so far */
+  uint64_t arena_free_bytes;
+} sqsg_server_counters;
+
+sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server** server);
+/* Validates and prepares the job on the calling thread and queues it; returns at once with a ticket.
+ * Jobs with a callback or cancel flag are rejected; SQSG_ERR_CAPACITY when its footprint can never fit. */
+sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_t* ticket);
+/* Waits for a ticket (timeout_us < 0: forever; SQSG_ERR_TIMEOUT when not done in time). The run's
+ * statistics carry the job latency in timings_ns[SQSG_TIMING_TOTAL] (submission to result). */
+sqsg_status sqsg_server_wait(sqsg_server* server, uint64_t ticket, int64_t timeout_us, sqsg_run** run);
+sqsg_status sqsg_server_stats(sqsg_server* server, sqsg_server_counters* stats);
+sqsg_status sqsg_server_destroy(sqsg_server* server);
+
 #ifdef __cplusplus
 }
 #endif

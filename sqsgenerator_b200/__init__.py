@@ -8,9 +8,10 @@ from .config import parse_config
 from .core import (IterationMode, LogLevel, ParseError, ParseErrorCode, Prec, ShellRadiiDetection, SqsConfiguration,
                    SqsResult, SqsResultPack, SqsResultSplit, SqsStatistics, Structure, SublatticeMode)
 from .optimize import optimize, prepare
+from .serve import Server
 
 __all__ = [
     "parse_config", "optimize", "prepare", "IterationMode", "LogLevel", "ParseError", "ParseErrorCode", "Prec",
     "ShellRadiiDetection", "SqsConfiguration", "SqsResult", "SqsResultPack", "SqsResultSplit", "SqsStatistics",
-    "Structure", "SublatticeMode",
+    "Structure", "SublatticeMode", "Server",
 ]

@@ -35,6 +35,7 @@ EXPORTED = (
     "sqsg_optimize", "sqsg_run_count", "sqsg_run_copy", "sqsg_run_statistics", "sqsg_run_free",
     "sqsg_optimize_trace", "sqsg_optimize_batch", "sqsg_run_levels", "sqsg_run_info",
     "sqsg_microbench", "sqsg_run_transfer", "sqsg_optimize_levels_noalloc",
+    "sqsg_server_create", "sqsg_server_submit", "sqsg_server_wait", "sqsg_server_stats", "sqsg_server_destroy",
 )
 
 
@@ -100,6 +101,20 @@ class SqsgJob(C.Structure):
     ]
 
 
+class SqsgServerOptions(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("max_jobs", C.c_uint32),
+        ("arena_bytes", C.c_uint64),
+        ("default_max_results", C.c_uint64),
+    ]
+
+
+class SqsgServerCounters(C.Structure):
+    _fields_ = [(name, C.c_uint64) for name in ("submitted", "admitted", "completed", "pending", "active",
+                                                  "configurations", "launches", "arena_free_bytes")]
+
+
 _LIB = None
 _LOCK = threading.Lock()
 
@@ -145,6 +160,11 @@ def lib():
         L.sqsg_run_transfer.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
         L.sqsg_optimize_levels_noalloc.argtypes = [C.POINTER(SqsgJob), vp, C.POINTER(u32), vp, vp, vp,
                                                    C.POINTER(SqsgStatistics), C.c_char_p, C.c_size_t]
+        L.sqsg_server_create.argtypes = [C.POINTER(SqsgServerOptions), C.POINTER(vp)]
+        L.sqsg_server_submit.argtypes = [vp, C.POINTER(SqsgJob), C.POINTER(u64)]
+        L.sqsg_server_wait.argtypes = [vp, u64, C.c_int64, C.POINTER(vp)]
+        L.sqsg_server_stats.argtypes = [vp, C.POINTER(SqsgServerCounters)]
+        L.sqsg_server_destroy.argtypes = [vp]
         L.sqsg_microbench.argtypes = [C.c_int, C.c_int, C.POINTER(dbl), C.POINTER(dbl)]
         for name in EXPORTED:
             if name not in ("sqsg_version", "sqsg_last_error", "sqsg_device_count", "sqsg_run_count",

@@ -11,6 +11,8 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -343,7 +345,6 @@ struct Workspace {
   DevBuf blob, records, counters, levels, tiles, jobs, queue, status, trace_sp, trace_bd, trace_obj, trace_id;
   int32_t* ctrl_host = nullptr;  // mapped pinned: [0] = cancel
   int32_t* ctrl_dev = nullptr;
-  unsigned long long* mirror = nullptr;  // pinned copy of counters for progress
   explicit Workspace(int dev) : device(dev) {
     CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CUDA_CHECK(cudaStreamCreateWithFlags(&monitor, cudaStreamNonBlocking));
@@ -351,7 +352,6 @@ struct Workspace {
     CUDA_CHECK(cudaEventCreate(&ev_stop));
     CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&ctrl_host), 64, cudaHostAllocMapped));
     CUDA_CHECK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctrl_dev), ctrl_host, 0));
-    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&mirror), 64 * kNumCounters * sizeof(unsigned long long), 0));
     std::memset(ctrl_host, 0, 64);
   }
   ~Workspace() {
@@ -360,7 +360,6 @@ struct Workspace {
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
     if (ctrl_host) cudaFreeHost(ctrl_host);
-    if (mirror) cudaFreeHost(mirror);
   }
 };
 
@@ -547,6 +546,92 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
   }
 }
 
+// What one pass of a job left behind: its exact objective levels (keep+1 smallest distinct
+// objectives with evaluation counts and id checksums) and the final threshold T*, or a request to
+// run the job again.
+//  - The device level table is exact unless it ran out of slots (many distinct objectives while
+//    the threshold was still high). Then, if the record buffer held every candidate, the levels are
+//    rebuilt from the records: every evaluation at or below the threshold of its time — so every
+//    evaluation at or below T* — is a record.
+//  - A record buffer that overflowed asks for a re-run (same tiles, same Philox counters, same
+//    evaluations) whose threshold starts at T* (exact levels: the buffer is sized from their counts)
+//    or at the (keep+1)-th distinct objective of the stored records, an upper bound of T*.
+struct Outcome {
+  bool rerun = false;
+  uint64_t rerun_capacity = 0;
+  double rerun_threshold = 0.0;
+  bool levels_exact = false;
+  double tstar = std::numeric_limits<double>::infinity();
+  std::vector<double> value;
+  std::vector<uint64_t> count, checksum;
+};
+
+template <class T>
+static void levels_from_records(const PreparedJob& pj, const std::vector<uint8_t>& recs, uint64_t n, Outcome& o) {
+  const size_t rb = pj.record_bytes;
+  std::vector<std::pair<unsigned long long, uint64_t>> e(n);
+  for (uint64_t i = 0; i < n; ++i)
+    e[i] = {ord_bits(static_cast<double>(read_t<T>(&recs[i * rb]))), mix64(read_t<uint64_t>(&recs[i * rb + 8]))};
+  std::sort(e.begin(), e.end());
+  for (size_t i = 0; i < e.size() && o.value.size() <= pj.keep;) {
+    size_t k = i;
+    uint32_t sa = 0, sb = 0;
+    for (; k < e.size() && e[k].first == e[i].first; ++k) {
+      sa += static_cast<uint32_t>(e[k].second);
+      sb += static_cast<uint32_t>(e[k].second >> 32);
+    }
+    o.value.push_back(from_ord(e[i].first));
+    o.count.push_back(k - i);
+    o.checksum.push_back(static_cast<uint64_t>(sa) | (static_cast<uint64_t>(sb) << 32));
+    i = k;
+  }
+}
+
+static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, const std::vector<LevelSlot>& lv,
+                      const std::vector<uint8_t>& recs, uint64_t stored, uint64_t capacity, bool may_rerun,
+                      uint64_t max_capacity) {
+  Outcome o;
+  const bool full = cnt[kRecordsFull] != 0 || cnt[kCandidates] > capacity;
+  const bool overflow = cnt[kLevelOverflow] != 0;
+  if (!overflow) {
+    std::vector<LevelSlot> used;
+    for (auto& x : lv)
+      if (x.key) used.push_back(x);
+    std::sort(used.begin(), used.end(), [](const LevelSlot& a, const LevelSlot& b) { return a.key < b.key; });
+    uint64_t need = 0;
+    for (size_t k = 0; k < used.size() && k <= pj.keep; ++k) {
+      o.value.push_back(from_ord(used[k].key));
+      o.count.push_back(used[k].count);
+      o.checksum.push_back(static_cast<uint64_t>(used[k].sum_a) | (static_cast<uint64_t>(used[k].sum_b) << 32));
+      need += used[k].count;
+    }
+    o.levels_exact = true;
+    if (used.size() > pj.keep) o.tstar = from_ord(used[pj.keep].key);
+    if (full && may_rerun && need + 64 <= max_capacity) {
+      o.rerun = true;
+      o.rerun_capacity = std::max<uint64_t>(need + 64, 1024);
+      o.rerun_threshold = o.tstar;
+    }
+    return o;
+  }
+  if (pj.prec == 1)
+    levels_from_records<double>(pj, recs, stored, o);
+  else
+    levels_from_records<float>(pj, recs, stored, o);
+  if (!full) {
+    o.levels_exact = true;
+    if (o.value.size() > pj.keep) o.tstar = o.value[pj.keep];
+    return o;
+  }
+  // neither the table nor the records are complete
+  if (may_rerun && o.value.size() > pj.keep) {
+    o.rerun = true;
+    o.rerun_capacity = std::min<uint64_t>(max_capacity, std::max<uint64_t>(capacity * 2, 1024));
+    o.rerun_threshold = o.value[pj.keep];
+  }
+  return o;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Executing prepared jobs on one device.
 struct TraceOut {
@@ -656,7 +741,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       sqsg_engine<<<grid, kBlock, smem, ws->stream>>>(
           static_cast<const JobDesc*>(ws->jobs.p), static_cast<const Tile*>(ws->tiles.p),
           static_cast<uint32_t>(tiles.size()), static_cast<QueueCtl*>(ws->queue.p), ws->ctrl_dev,
-          static_cast<unsigned long long*>(ws->status.p));
+          static_cast<unsigned long long*>(ws->status.p), nullptr);
       CUDA_CHECK(cudaGetLastError());
     }
     CUDA_CHECK(cudaEventRecord(ws->ev_stop, ws->stream));
@@ -667,6 +752,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       const uint64_t chunk = srcs[j]->chunk_size ? srcs[j]->chunk_size : 100000;
       next_cb[j] = chunk;
     }
+    std::vector<unsigned long long> mirror;
     bool any_watch = false;
     for (size_t j = 0; j < nj; ++j) any_watch |= srcs[j]->cancel != nullptr || srcs[j]->callback != nullptr;
     while (true) {
@@ -684,19 +770,20 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       bool need_cb = false;
       for (size_t j = 0; j < nj; ++j) need_cb |= srcs[j]->callback != nullptr;
       if (need_cb) {
-        CUDA_CHECK(cudaMemcpyAsync(ws->mirror, counters, nj * kNumCounters * sizeof(unsigned long long),
+        mirror.resize(nj * kNumCounters);
+        CUDA_CHECK(cudaMemcpyAsync(mirror.data(), counters, nj * kNumCounters * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, ws->monitor));
         CUDA_CHECK(cudaStreamSynchronize(ws->monitor));
         for (size_t j = 0; j < nj; ++j) {
           if (!srcs[j]->callback) continue;
-          const uint64_t fin = ws->mirror[j * kNumCounters + kFinished];
+          const uint64_t fin = mirror[j * kNumCounters + kFinished];
           if (fin < next_cb[j]) continue;
           const uint64_t chunk = srcs[j]->chunk_size ? srcs[j]->chunk_size : 100000;
           while (next_cb[j] <= fin) next_cb[j] += chunk;
           sqsg_statistics st{};
           st.finished = fin;
           st.working = pjs[j].range_count > fin ? pjs[j].range_count - fin : 0;
-          st.best_objective = from_ord(ws->mirror[j * kNumCounters + kBest]);
+          st.best_objective = from_ord(mirror[j * kNumCounters + kBest]);
           st.timings_ns[SQSG_TIMING_TOTAL] = now_ns() - t0;
           if (srcs[j]->callback(&st, srcs[j]->user) != 0) stop = true;
         }
@@ -713,30 +800,29 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     CUDA_CHECK(cudaMemcpy(&status, ws->status.p, sizeof(status), cudaMemcpyDeviceToHost));
     if (status == kErrStageTimeout) throw timeout_error("shared-memory staging wait timed out on the device");
     if (status != 0) throw cuda_error("device error code " + std::to_string(status));
-    // A candidate overflow re-runs the job with a larger buffer when the caller left the capacity
-    // to the library and the records fit the memory budget (tiles and Philox counters make the
-    // re-run evaluate the same configurations); otherwise the record set is cut and flagged.
-    // The re-run starts at the exact final threshold T* (the (keep+1)-th smallest level) and needs
-    // exactly the evaluations at or below it, which the level table counts.
+    // Every job's counters, level table and records come back; a job whose record buffer overflowed
+    // is re-run (see assess) when the caller left the capacity to the library.
     bool rerun = false;
+    std::vector<std::vector<uint8_t>> recs(nj);
+    std::vector<Outcome> outc(nj);
+    uint64_t d2h_bytes = cnt.size() * sizeof(unsigned long long) + 8;
     for (size_t j = 0; j < nj; ++j) {
-      const bool full = cnt[j * kNumCounters + kRecordsFull] != 0 || cnt[j * kNumCounters + kCandidates] > capacity[j];
-      if (!full || pjs[j].max_results || attempt >= 2 || cnt[j * kNumCounters + kLevelOverflow]) continue;
+      const unsigned long long* cj = &cnt[j * kNumCounters];
       std::vector<LevelSlot> lv(kLevelSlots);
       CUDA_CHECK(cudaMemcpy(lv.data(), static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots,
                             kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost));
-      std::vector<LevelSlot> used;
-      for (auto& x : lv)
-        if (x.key) used.push_back(x);
-      std::sort(used.begin(), used.end(), [](const LevelSlot& a, const LevelSlot& b) { return a.key < b.key; });
-      uint64_t need = 0;
-      for (size_t k = 0; k < used.size() && k <= pjs[j].keep; ++k) need += used[k].count;
-      const uint64_t budget = (4ull << 30) / pjs[j].record_bytes;
-      if (need <= budget) {
-        capacity[j] = std::max<uint64_t>(need + 64, 1024);
+      const uint64_t n = std::min<uint64_t>(cj[kCandidates], capacity[j]);
+      recs[j].resize(n * pjs[j].record_bytes);
+      if (n)
+        CUDA_CHECK(cudaMemcpy(recs[j].data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], recs[j].size(),
+                              cudaMemcpyDeviceToHost));
+      d2h_bytes += kLevelSlots * sizeof(LevelSlot) + recs[j].size();
+      const bool may_rerun = !pjs[j].max_results && attempt < 2;
+      outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, (4ull << 30) / pjs[j].record_bytes);
+      if (outc[j].rerun) {
+        capacity[j] = outc[j].rerun_capacity;
         fixed_threshold[j] = true;
-        start_threshold[j] = used.size() > pjs[j].keep ? from_ord(used[pjs[j].keep].key)
-                                                       : std::numeric_limits<double>::infinity();
+        start_threshold[j] = outc[j].rerun_threshold;
         rerun = true;
       }
     }
@@ -745,43 +831,27 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     const uint64_t t_loop = now_ns();
     runs.assign(nj, Run{});
     for (size_t j = 0; j < nj; ++j) {
-      const uint64_t n = std::min<uint64_t>(cnt[j * kNumCounters + kCandidates], capacity[j]);
-      std::vector<uint8_t> recs(n * pjs[j].record_bytes);
-      if (n)
-        CUDA_CHECK(cudaMemcpy(recs.data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], recs.size(),
-                              cudaMemcpyDeviceToHost));
+      const unsigned long long* cj = &cnt[j * kNumCounters];
+      const uint64_t n = recs[j].size() / pjs[j].record_bytes;
       Run& r = runs[j];
       r.h2d_bytes = h2d_bytes / nj;
-      r.d2h_bytes = recs.size() + kLevelSlots * sizeof(LevelSlot) + (cnt.size() * sizeof(unsigned long long) + 8) / nj;
+      r.d2h_bytes = d2h_bytes / nj;
       r.prec = pjs[j].prec;
       r.n_parts = pjs[j].desc.n_parts;
       r.parts = pjs[j].parts;
       r.tsz = pjs[j].tsz;
-      // objective levels (exact unless the level table overflowed)
-      std::vector<LevelSlot> lv(kLevelSlots);
-      CUDA_CHECK(cudaMemcpy(lv.data(), static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots,
-                            kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost));
-      std::vector<LevelSlot> used;
-      for (auto& x : lv)
-        if (x.key) used.push_back(x);
-      std::sort(used.begin(), used.end(), [](const LevelSlot& a, const LevelSlot& b) { return a.key < b.key; });
-      r.levels_exact = cnt[j * kNumCounters + kLevelOverflow] == 0;
-      for (size_t k = 0; k < used.size() && k <= pjs[j].keep; ++k) {
-        r.level_value.push_back(from_ord(used[k].key));
-        r.level_count.push_back(used[k].count);
-        r.level_checksum.push_back(static_cast<uint64_t>(used[k].sum_a) | (static_cast<uint64_t>(used[k].sum_b) << 32));
-      }
-      const bool have_tstar = r.levels_exact;
-      const double tstar = used.size() > pjs[j].keep ? from_ord(used[pjs[j].keep].key)
-                                                     : std::numeric_limits<double>::infinity();
-      r.candidates = cnt[j * kNumCounters + kCandidates];
-      r.truncated = cnt[j * kNumCounters + kRecordsFull] != 0 || r.candidates > capacity[j];
-      const uint64_t stored = std::min<uint64_t>(n, capacity[j]);
+      Outcome& o = outc[j];
+      r.levels_exact = o.levels_exact;
+      r.level_value = std::move(o.value);
+      r.level_count = std::move(o.count);
+      r.level_checksum = std::move(o.checksum);
+      r.candidates = cj[kCandidates];
+      r.truncated = cj[kRecordsFull] != 0 || r.candidates > capacity[j];
       if (pjs[j].prec == 1)
-        select_results<double>(pjs[j], recs, stored, r, have_tstar, tstar);
+        select_results<double>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
       else
-        select_results<float>(pjs[j], recs, stored, r, have_tstar, tstar);
-      r.stats.finished = cnt[j * kNumCounters + kFinished];
+        select_results<float>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
+      r.stats.finished = cj[kFinished];
       r.stats.working = 0;
       if (r.count) {
         r.stats.best_objective =
@@ -812,6 +882,377 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       r.stats.timings_ns[SQSG_TIMING_COMM] = t_end - t_loop;
     }
     return;
+  }
+}
+
+
+// ------------------------------------------------------------------------------------------------
+// Served form: continuous batching on a live tile ring.
+//
+// Jobs are submitted at any time. The server's worker thread admits a job when a job slot, ring
+// space and device memory for its data and records are free (admission by footprint), uploads it
+// on a copy stream, appends its tiles to the ring of its shared-memory bucket and raises the ring's
+// tail; the bucket's persistent kernel, already running other jobs' tiles, picks them up. The CTA
+// that finishes a job's last tile marks the job's slot done in host-mapped memory; the worker then
+// downloads its records and levels, selects the result set and wakes the waiting caller. A job's
+// result does not depend on what else runs: its tiles and Philox counters depend only on the job.
+constexpr int kBuckets = 4;
+constexpr size_t kBucketSmem[kBuckets] = {24u << 10, 56u << 10, 112u << 10, 0};  // 0: device maximum
+constexpr uint64_t kRingCap = 1u << 20;
+constexpr uint32_t kIdlePolls = 250;         // ~0.5 ms of empty polls before a CTA leaves its ring
+constexpr int kLaunchSlots = 8;              // concurrent launches per ring
+constexpr uint64_t kRebalanceNs = 1000000;   // at most one shrink per ring per millisecond
+
+struct ServerJob {
+  uint64_t ticket = 0;
+  uint32_t slot = 0, gen = 0;
+  int bucket = 0;
+  PreparedJob pj;
+  std::vector<Tile> tiles;
+  size_t arena_off = 0, arena_bytes = 0, blob_bytes = 0;
+  uint64_t capacity = 0;
+  bool user_capacity = false;
+  int attempt = 0;
+  bool fixed_threshold = false;
+  double start_threshold = 0.0;
+  uint64_t ring_begin = 0, ring_end = 0;
+  uint64_t t_submit = 0, t_admit = 0;
+  uint64_t h2d_bytes = 0;
+};
+
+struct LaunchSlot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool busy = false;
+};
+
+// One ring of tiles per shared-memory class; several launches of sqsg_engine may serve a ring at once.
+struct Ring {
+  size_t smem = 0;
+  uint32_t full_grid = 0;     // CTAs that fill the device at this shared-memory size
+  uint64_t published = 0;     // tiles appended so far (the ring's tail)
+  uint32_t launched = 0;      // CTAs launched so far (wraps like QueueCtl::exited)
+  uint64_t last_shrink = 0;
+  LaunchSlot ls[kLaunchSlots];
+};
+
+struct ServerState {
+  int device = 0;
+  sqsg_server_options opt{};
+  cudaStream_t copy = nullptr;
+  Ring rings[kBuckets];
+  uint8_t* arena = nullptr;
+  std::map<size_t, size_t> free_list;  // offset -> size
+  JobDesc* d_jobs = nullptr;
+  unsigned long long* d_counters = nullptr;
+  LevelSlot* d_levels = nullptr;
+  Tile* d_ring[kBuckets] = {};
+  uint8_t* d_ctl = nullptr;   // kBuckets QueueCtl, then the device status word
+  uint8_t* h_ctl = nullptr;   // pinned mirror of d_ctl
+  uint32_t* h_yield = nullptr;  // pinned sources of yield writes
+  uint32_t* h_done = nullptr;
+  uint32_t* d_done = nullptr;
+  std::vector<std::unique_ptr<ServerJob>> slots;
+  std::vector<uint32_t> slot_gen;
+  std::deque<std::unique_ptr<ServerJob>> pending;
+  std::map<uint64_t, Run> finished;
+  std::map<uint64_t, std::pair<sqsg_status, std::string>> failed;
+  std::string broken;  // set after a device error: the server fails every job from then on
+  std::mutex m;
+  std::condition_variable cv_work, cv_done;
+  std::thread worker;
+  bool stop = false;
+  uint64_t next_ticket = 1;
+  sqsg_server_counters stats{};
+  QueueCtl* q(int b) const { return reinterpret_cast<QueueCtl*>(d_ctl) + b; }
+  const QueueCtl& hq(int b) const { return reinterpret_cast<const QueueCtl*>(h_ctl)[b]; }
+  unsigned long long device_status() const {
+    return *reinterpret_cast<const unsigned long long*>(h_ctl + kBuckets * sizeof(QueueCtl));
+  }
+};
+
+constexpr size_t kCtlBytes = kBuckets * sizeof(QueueCtl) + 64;
+
+static bool arena_alloc(ServerState& S, size_t bytes, size_t* off) {
+  bytes = align_up(bytes, 256);
+  for (auto it = S.free_list.begin(); it != S.free_list.end(); ++it) {
+    if (it->second >= bytes) {
+      *off = it->first;
+      const size_t rest = it->second - bytes;
+      const size_t roff = it->first + bytes;
+      S.free_list.erase(it);
+      if (rest) S.free_list[roff] = rest;
+      return true;
+    }
+  }
+  return false;
+}
+
+static void arena_free(ServerState& S, size_t off, size_t bytes) {
+  bytes = align_up(bytes, 256);
+  auto it = S.free_list.emplace(off, bytes).first;
+  auto next = std::next(it);
+  if (next != S.free_list.end() && it->first + it->second == next->first) {
+    it->second += next->second;
+    S.free_list.erase(next);
+  }
+  if (it != S.free_list.begin()) {
+    auto prev = std::prev(it);
+    if (prev->first + prev->second == it->first) {
+      prev->second += it->second;
+      S.free_list.erase(it);
+    }
+  }
+}
+
+static size_t job_footprint(const ServerJob& J) {
+  return align_up(J.pj.blob.size(), 256) + align_up(J.capacity * J.pj.record_bytes, 256);
+}
+
+// Admits the oldest pending job if a slot, ring space and arena memory are free: uploads its data,
+// counters, level table, descriptor and tiles on the copy stream, then raises its ring's tail.
+// Called with S.m held.
+static bool try_admit(ServerState& S) {
+  if (S.pending.empty()) return false;
+  ServerJob& J = *S.pending.front();
+  uint32_t slot = static_cast<uint32_t>(S.slots.size());
+  for (uint32_t k = 0; k < S.slots.size(); ++k)
+    if (!S.slots[k]) {
+      slot = k;
+      break;
+    }
+  if (slot == S.slots.size()) return false;
+  const int b = J.bucket;
+  Ring& R = S.rings[b];
+  uint64_t oldest = R.published;  // ring entries before the oldest live job's tiles are free
+  for (auto& x : S.slots)
+    if (x && x->bucket == b) oldest = std::min(oldest, x->ring_begin);
+  if (R.published + J.tiles.size() - oldest > kRingCap) return false;
+  J.blob_bytes = align_up(J.pj.blob.size(), 256);
+  J.arena_bytes = job_footprint(J);
+  if (!arena_alloc(S, J.arena_bytes, &J.arena_off)) return false;
+  J.slot = slot;
+  J.gen = ++S.slot_gen[slot];
+  if (J.gen == 0) J.gen = ++S.slot_gen[slot];
+  J.t_admit = now_ns();
+  JobDesc d = J.pj.desc;
+  d.blob = S.arena + J.arena_off;
+  d.records = S.arena + J.arena_off + J.blob_bytes;
+  d.capacity = J.capacity;
+  d.counters = S.d_counters + static_cast<size_t>(slot) * kNumCounters;
+  d.levels = S.d_levels + static_cast<size_t>(slot) * kLevelSlots;
+  std::vector<unsigned long long> init(kNumCounters, 0);
+  const double maxv = J.pj.prec == 1 ? std::numeric_limits<double>::max()
+                                     : static_cast<double>(std::numeric_limits<float>::max());
+  init[kThreshold] = ord_bits(J.fixed_threshold ? J.start_threshold : maxv);
+  init[kBest] = ord_bits(std::numeric_limits<double>::infinity());
+  init[kTilesLeft] = J.tiles.size();
+  for (auto& t : J.tiles) {
+    t.job = slot;
+    t.gen = J.gen;
+  }
+  CUDA_CHECK(cudaMemcpyAsync(S.arena + J.arena_off, J.pj.blob.data(), J.pj.blob.size(), cudaMemcpyHostToDevice, S.copy));
+  CUDA_CHECK(cudaMemcpyAsync(d.counters, init.data(), init.size() * 8, cudaMemcpyHostToDevice, S.copy));
+  CUDA_CHECK(cudaMemsetAsync(d.levels, 0, kLevelSlots * sizeof(LevelSlot), S.copy));
+  CUDA_CHECK(cudaMemcpyAsync(S.d_jobs + slot, &d, sizeof(d), cudaMemcpyHostToDevice, S.copy));
+  const uint64_t n = J.tiles.size();
+  const uint64_t pos = R.published % kRingCap;
+  const uint64_t first = std::min<uint64_t>(n, kRingCap - pos);
+  if (first)
+    CUDA_CHECK(cudaMemcpyAsync(S.d_ring[b] + pos, J.tiles.data(), first * sizeof(Tile), cudaMemcpyHostToDevice, S.copy));
+  if (n > first)
+    CUDA_CHECK(cudaMemcpyAsync(S.d_ring[b], J.tiles.data() + first, (n - first) * sizeof(Tile), cudaMemcpyHostToDevice,
+                               S.copy));
+  J.ring_begin = R.published;
+  R.published += n;
+  J.ring_end = R.published;
+  // the tail rises only after everything above is in device memory (same stream)
+  const unsigned long long tail = R.published;
+  CUDA_CHECK(cudaMemcpyAsync(&S.q(b)->tail, &tail, sizeof(tail), cudaMemcpyHostToDevice, S.copy));
+  CUDA_CHECK(cudaStreamSynchronize(S.copy));
+  J.h2d_bytes += J.pj.blob.size() + init.size() * 8 + sizeof(d) + n * sizeof(Tile) + sizeof(tail);
+  S.slots[slot] = std::move(S.pending.front());
+  S.pending.pop_front();
+  S.stats.admitted++;
+  return true;
+}
+
+// Collects a finished job: counters, level table and records come back on the copy stream and the
+// result set is selected like sqsg_optimize selects it. A job whose record buffer overflowed is
+// re-admitted at the front of the queue with the threshold and buffer that assess() asks for (the
+// same tiles and Philox counters give the same evaluations), as sqsg_optimize re-runs it. Returns
+// true when the job's result is final.
+static bool finalize(ServerState& S, uint32_t slot) {
+  ServerJob& J = *S.slots[slot];
+  std::vector<unsigned long long> cnt(kNumCounters);
+  CUDA_CHECK(cudaMemcpyAsync(cnt.data(), S.d_counters + static_cast<size_t>(slot) * kNumCounters, cnt.size() * 8,
+                             cudaMemcpyDeviceToHost, S.copy));
+  std::vector<LevelSlot> lv(kLevelSlots);
+  CUDA_CHECK(cudaMemcpyAsync(lv.data(), S.d_levels + static_cast<size_t>(slot) * kLevelSlots,
+                             kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost, S.copy));
+  CUDA_CHECK(cudaStreamSynchronize(S.copy));
+  const uint64_t n = std::min<uint64_t>(cnt[kCandidates], J.capacity);
+  std::vector<uint8_t> recs(n * J.pj.record_bytes);
+  if (n) {
+    CUDA_CHECK(cudaMemcpyAsync(recs.data(), S.arena + J.arena_off + J.blob_bytes, recs.size(), cudaMemcpyDeviceToHost,
+                               S.copy));
+    CUDA_CHECK(cudaStreamSynchronize(S.copy));
+  }
+  const uint64_t arena_records =
+      (S.opt.arena_bytes - std::min<uint64_t>(S.opt.arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) /
+      J.pj.record_bytes;
+  Outcome o = assess(J.pj, cnt.data(), lv, recs, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
+  if (o.rerun) {
+    arena_free(S, J.arena_off, J.arena_bytes);
+    J.capacity = o.rerun_capacity;
+    J.fixed_threshold = true;
+    J.start_threshold = o.rerun_threshold;
+    J.attempt++;
+    S.pending.push_front(std::move(S.slots[slot]));
+    return false;
+  }
+  Run r;
+  r.prec = J.pj.prec;
+  r.n_parts = J.pj.desc.n_parts;
+  r.parts = J.pj.parts;
+  r.tsz = J.pj.tsz;
+  r.levels_exact = o.levels_exact;
+  r.level_value = std::move(o.value);
+  r.level_count = std::move(o.count);
+  r.level_checksum = std::move(o.checksum);
+  r.candidates = cnt[kCandidates];
+  r.truncated = cnt[kRecordsFull] != 0 || r.candidates > J.capacity;
+  if (J.pj.prec == 1)
+    select_results<double>(J.pj, recs, n, r, o.levels_exact, o.tstar);
+  else
+    select_results<float>(J.pj, recs, n, r, o.levels_exact, o.tstar);
+  r.stats.finished = cnt[kFinished];
+  if (r.count) {
+    r.stats.best_objective =
+        J.pj.prec == 1 ? read_t<double>(r.objective.data()) : static_cast<double>(read_t<float>(r.objective.data()));
+    r.stats.best_rank = r.id[0];
+  } else {
+    r.stats.best_objective = std::numeric_limits<double>::infinity();
+  }
+  const uint64_t t_end = now_ns();
+  r.stats.timings_ns[SQSG_TIMING_TOTAL] = t_end - J.t_submit;  // latency: submission to result
+  r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = J.t_admit - J.t_submit;
+  r.stats.timings_ns[SQSG_TIMING_LOOP] = t_end - J.t_admit;
+  r.h2d_bytes = J.h2d_bytes;
+  r.d2h_bytes = kLevelSlots * sizeof(LevelSlot) + kNumCounters * 8 + recs.size();
+  S.stats.completed++;
+  S.stats.configurations += cnt[kFinished];
+  arena_free(S, J.arena_off, J.arena_bytes);
+  S.finished.emplace(J.ticket, std::move(r));
+  S.slots[slot].reset();
+  return true;
+}
+
+static void write_yield(ServerState& S, int b, uint32_t value) {
+  S.h_yield[b] = value;
+  CUDA_CHECK(cudaMemcpyAsync(&S.q(b)->yield, &S.h_yield[b], sizeof(uint32_t), cudaMemcpyHostToDevice, S.copy));
+  CUDA_CHECK(cudaStreamSynchronize(S.copy));
+}
+
+// Shares the device between the rings that hold unclaimed tiles: each gets an equal part of the
+// CTAs that would fill the GPU at its shared-memory size. A ring below its share gets a launch of
+// the missing CTAs; a ring above it (after another ring gained work) is asked to give CTAs back
+// through its yield counter, which CTAs honour between tiles. Rings without unclaimed tiles are
+// left alone: their CTAs finish their tiles and leave after kIdlePolls empty polls.
+static void schedule(ServerState& S) {
+  uint64_t unclaimed[kBuckets];
+  int n_want = 0;
+  for (int b = 0; b < kBuckets; ++b) {
+    const uint64_t head = S.hq(b).head;
+    unclaimed[b] = S.rings[b].published > head ? S.rings[b].published - head : 0;
+    n_want += unclaimed[b] ? 1 : 0;
+  }
+  if (!n_want) return;
+  const uint64_t now = now_ns();
+  for (int b = 0; b < kBuckets; ++b) {
+    if (!unclaimed[b]) continue;
+    Ring& R = S.rings[b];
+    const QueueCtl& q = S.hq(b);
+    const uint32_t live = R.launched - q.exited;
+    const uint32_t eff = live > q.yield ? live - q.yield : 0;
+    uint64_t target = std::max<uint32_t>(1, R.full_grid / n_want);
+    target = std::min<uint64_t>(target, eff + unclaimed[b]);
+    if (eff < target) {
+      for (auto& L : R.ls) {
+        if (L.busy) continue;
+        const uint32_t grid = static_cast<uint32_t>(target - eff);
+        if (q.yield) write_yield(S, b, 0);  // a pending yield would send the new CTAs away
+        sqsg_engine<<<grid, kBlock, R.smem, L.stream>>>(S.d_jobs, S.d_ring[b], 0, S.q(b), nullptr,
+                                                         reinterpret_cast<unsigned long long*>(
+                                                             S.d_ctl + kBuckets * sizeof(QueueCtl)),
+                                                         S.d_done);
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaEventRecord(L.done, L.stream));
+        L.busy = true;
+        R.launched += grid;
+        S.stats.launches++;
+        break;
+      }
+    } else if (n_want > 1 && eff > target + target / 8 && now - R.last_shrink > kRebalanceNs) {
+      write_yield(S, b, static_cast<uint32_t>(live - target));
+      R.last_shrink = now;
+    }
+  }
+}
+
+static void fail_all(ServerState& S, const std::string& why) {
+  for (auto& x : S.slots)
+    if (x) {
+      S.failed[x->ticket] = {SQSG_ERR_CUDA, why};
+      x.reset();
+    }
+  while (!S.pending.empty()) {
+    S.failed[S.pending.front()->ticket] = {SQSG_ERR_CUDA, why};
+    S.pending.pop_front();
+  }
+  S.cv_done.notify_all();
+}
+
+static void server_loop(ServerState* Sp) {
+  ServerState& S = *Sp;
+  cudaSetDevice(S.device);
+  std::unique_lock<std::mutex> lock(S.m);
+  while (!S.stop) {
+    bool progress = false;
+    if (S.broken.empty()) {
+      try {
+        CUDA_CHECK(cudaMemcpyAsync(S.h_ctl, S.d_ctl, kCtlBytes, cudaMemcpyDeviceToHost, S.copy));
+        CUDA_CHECK(cudaStreamSynchronize(S.copy));
+        if (const unsigned long long st = S.device_status())
+          throw cuda_error("device error " + std::to_string(st) + " in the serving kernel");
+        for (uint32_t k = 0; k < S.slots.size(); ++k) {
+          if (!S.slots[k]) continue;
+          if (*reinterpret_cast<volatile uint32_t*>(&S.h_done[k]) == S.slots[k]->gen) {
+            if (finalize(S, k)) S.cv_done.notify_all();
+            progress = true;
+          }
+        }
+        while (try_admit(S)) progress = true;
+        for (auto& R : S.rings)
+          for (auto& L : R.ls) {
+            if (!L.busy) continue;
+            const cudaError_t e = cudaEventQuery(L.done);
+            if (e == cudaErrorNotReady) continue;
+            CUDA_CHECK(e);
+            L.busy = false;
+            progress = true;
+          }
+        schedule(S);
+      } catch (std::exception const& ex) {
+        // A device error leaves CTAs of failed jobs possibly still running over arena memory that
+        // must not be handed out again: the server stops serving and fails every job.
+        S.broken = ex.what();
+        fail_all(S, S.broken);
+      }
+    } else if (!S.pending.empty()) {
+      fail_all(S, S.broken);
+    }
+    if (!progress) S.cv_work.wait_for(lock, std::chrono::microseconds(50));
   }
 }
 
@@ -1011,6 +1452,194 @@ sqsg_status sqsg_run_info(const sqsg_run* run, uint64_t* candidates, int32_t* tr
     if (truncated) *truncated = run->r.truncated ? 1 : 0;
     if (levels_exact) *levels_exact = run->r.levels_exact ? 1 : 0;
   });
+}
+
+
+
+struct sqsg_server {
+  ServerState s;
+};
+
+sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server** out) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("null pointer");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      throw cuda_error("no CUDA device is available (the optimiser has no CPU path)");
+    }
+    sqsg_server_options opt{};
+    if (options) opt = *options;
+    if (opt.device < 0 || opt.device >= ndev) throw std::invalid_argument("invalid device ordinal");
+    if (!opt.arena_bytes) opt.arena_bytes = 4ull << 30;
+    if (!opt.max_jobs) opt.max_jobs = 256;
+    if (!opt.default_max_results) opt.default_max_results = 1u << 16;
+    auto srv = std::unique_ptr<sqsg_server, sqsg_status (*)(sqsg_server*)>(new sqsg_server, sqsg_server_destroy);
+    ServerState& S = srv->s;
+    S.opt = opt;
+    S.device = opt.device;
+    CUDA_CHECK(cudaSetDevice(S.device));
+    CUDA_CHECK(cudaStreamCreateWithFlags(&S.copy, cudaStreamNonBlocking));
+    const size_t optin = max_dynamic_smem(S.device);
+    CUDA_CHECK(cudaMalloc(&S.d_ctl, kCtlBytes));
+    CUDA_CHECK(cudaMemset(S.d_ctl, 0, kCtlBytes));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_ctl), kCtlBytes, cudaHostAllocDefault));
+    std::memset(S.h_ctl, 0, kCtlBytes);
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_yield), kBuckets * sizeof(uint32_t), cudaHostAllocDefault));
+    for (int b = 0; b < kBuckets; ++b) {
+      Ring& R = S.rings[b];
+      R.smem = kBucketSmem[b] ? std::min(kBucketSmem[b], optin) : optin;
+      configure_kernel(R.smem);
+      R.full_grid = launch_grid(S.device, R.smem, 1u << 30);
+      for (auto& L : R.ls) {
+        CUDA_CHECK(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+        CUDA_CHECK(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+      }
+      CUDA_CHECK(cudaMalloc(&S.d_ring[b], kRingCap * sizeof(Tile)));
+      QueueCtl q{};
+      q.capacity = static_cast<unsigned int>(kRingCap);
+      q.idle_limit = kIdlePolls;
+      CUDA_CHECK(cudaMemcpy(S.q(b), &q, sizeof(q), cudaMemcpyHostToDevice));
+    }
+    CUDA_CHECK(cudaMalloc(&S.arena, S.opt.arena_bytes));
+    S.free_list[0] = S.opt.arena_bytes;
+    const size_t nslot = S.opt.max_jobs;
+    CUDA_CHECK(cudaMalloc(&S.d_jobs, nslot * sizeof(JobDesc)));
+    CUDA_CHECK(cudaMalloc(&S.d_counters, nslot * kNumCounters * 8));
+    CUDA_CHECK(cudaMalloc(&S.d_levels, nslot * kLevelSlots * sizeof(LevelSlot)));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_done), nslot * sizeof(uint32_t), cudaHostAllocMapped));
+    CUDA_CHECK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&S.d_done), S.h_done, 0));
+    std::memset(S.h_done, 0, nslot * sizeof(uint32_t));
+    S.slots.resize(nslot);
+    S.slot_gen.assign(nslot, 0);
+    S.worker = std::thread(server_loop, &S);
+    *out = srv.release();
+  });
+}
+
+sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_t* ticket) {
+  return guarded([&] {
+    if (!server || !job || !ticket) throw std::invalid_argument("null pointer");
+    ServerState& S = server->s;
+    if (job->device != S.device) throw std::invalid_argument("the job names another device than the server's");
+    if (job->callback || job->cancel) throw std::invalid_argument("served jobs take no callback or cancel flag");
+    auto J = std::make_unique<ServerJob>();
+    J->pj = prepare(*job, 0);
+    J->t_submit = now_ns();
+    const size_t need = J->pj.desc.smem_bytes;
+    if (need > S.rings[kBuckets - 1].smem)
+      throw unsupported_error("the job needs more shared memory per CTA than this device offers");
+    J->bucket = kBuckets - 1;
+    for (int b = 0; b < kBuckets; ++b)
+      if (need <= S.rings[b].smem) {
+        J->bucket = b;
+        break;
+      }
+    J->user_capacity = job->max_results != 0;
+    J->capacity = job->max_results ? job->max_results : S.opt.default_max_results;
+    make_tiles(J->pj, 0, J->tiles);
+    if (J->tiles.size() > kRingCap) throw unsupported_error("the job has more tiles than the ring holds");
+    if (job_footprint(*J) > S.opt.arena_bytes)
+      throw std::length_error("the job's device footprint exceeds the server's arena; lower max_results");
+    std::lock_guard<std::mutex> l(S.m);
+    if (!S.broken.empty()) throw cuda_error("the server stopped after a device error: " + S.broken);
+    J->ticket = S.next_ticket++;
+    *ticket = J->ticket;
+    S.stats.submitted++;
+    if (J->tiles.empty()) {  // nothing to evaluate: an empty result
+      Run r;
+      r.prec = J->pj.prec;
+      r.n_parts = J->pj.desc.n_parts;
+      r.parts = J->pj.parts;
+      r.tsz = J->pj.tsz;
+      r.stats.best_objective = std::numeric_limits<double>::infinity();
+      S.finished.emplace(J->ticket, std::move(r));
+      S.stats.completed++;
+      S.cv_done.notify_all();
+      return;
+    }
+    S.pending.push_back(std::move(J));
+    S.cv_work.notify_one();
+  });
+}
+
+sqsg_status sqsg_server_wait(sqsg_server* server, uint64_t ticket, int64_t timeout_us, sqsg_run** run) {
+  return guarded([&] {
+    if (!server || !run) throw std::invalid_argument("null pointer");
+    ServerState& S = server->s;
+    std::unique_lock<std::mutex> l(S.m);
+    auto ready = [&] { return S.finished.count(ticket) || S.failed.count(ticket); };
+    if (timeout_us < 0)
+      S.cv_done.wait(l, ready);
+    else if (!S.cv_done.wait_for(l, std::chrono::microseconds(timeout_us), ready))
+      throw timeout_error("the job has not finished yet");
+    auto f = S.failed.find(ticket);
+    if (f != S.failed.end()) {
+      const auto err = f->second;
+      S.failed.erase(f);
+      throw cuda_error(err.second);
+    }
+    auto it = S.finished.find(ticket);
+    *run = new sqsg_run{std::move(it->second)};
+    S.finished.erase(it);
+  });
+}
+
+sqsg_status sqsg_server_stats(sqsg_server* server, sqsg_server_counters* stats) {
+  return guarded([&] {
+    if (!server || !stats) throw std::invalid_argument("null pointer");
+    ServerState& S = server->s;
+    std::lock_guard<std::mutex> l(S.m);
+    *stats = S.stats;
+    stats->pending = S.pending.size();
+    uint64_t active = 0;
+    for (auto& x : S.slots) active += x ? 1 : 0;
+    stats->active = active;
+    size_t free_bytes = 0;
+    for (auto& [o, n] : S.free_list) free_bytes += n;
+    stats->arena_free_bytes = free_bytes;
+  });
+}
+
+sqsg_status sqsg_server_destroy(sqsg_server* server) {
+  if (!server) return SQSG_OK;
+  ServerState& S = server->s;
+  {
+    std::lock_guard<std::mutex> l(S.m);
+    S.stop = true;
+    S.cv_work.notify_all();
+  }
+  if (S.worker.joinable()) S.worker.join();
+  cudaSetDevice(S.device);
+  // every CTA leaves at its next claim: no tile is started after this
+  if (S.d_ctl && S.h_yield && S.copy) {
+    for (int b = 0; b < kBuckets; ++b) {
+      S.h_yield[b] = ~0u;
+      cudaMemcpyAsync(&S.q(b)->yield, &S.h_yield[b], sizeof(uint32_t), cudaMemcpyHostToDevice, S.copy);
+    }
+    cudaStreamSynchronize(S.copy);
+  }
+  for (auto& R : S.rings)
+    for (auto& L : R.ls)
+      if (L.stream) cudaStreamSynchronize(L.stream);
+  for (int b = 0; b < kBuckets; ++b) {
+    for (auto& L : S.rings[b].ls) {
+      if (L.stream) cudaStreamDestroy(L.stream);
+      if (L.done) cudaEventDestroy(L.done);
+    }
+    if (S.d_ring[b]) cudaFree(S.d_ring[b]);
+  }
+  if (S.copy) cudaStreamDestroy(S.copy);
+  if (S.arena) cudaFree(S.arena);
+  if (S.d_jobs) cudaFree(S.d_jobs);
+  if (S.d_counters) cudaFree(S.d_counters);
+  if (S.d_levels) cudaFree(S.d_levels);
+  if (S.d_ctl) cudaFree(S.d_ctl);
+  if (S.h_ctl) cudaFreeHost(S.h_ctl);
+  if (S.h_yield) cudaFreeHost(S.h_yield);
+  if (S.h_done) cudaFreeHost(S.h_done);
+  delete server;
+  return SQSG_OK;
 }
 
 }  // extern "C"

@@ -34,7 +34,8 @@ enum Counter : int {
   kTilesDone = 5,   // tiles completed
   kLevelOverflow = 6,  // the job's level table ran out of slots
   kRecordsFull = 7,    // set once the candidate buffer is full (appends stop)
-  kNumCounters = 8
+  kTilesLeft = 8,      // live queue: tiles of the job not yet finished
+  kNumCounters = 16
 };
 
 enum DeviceError : unsigned long long { kErrNone = 0, kErrStageTimeout = 1, kErrBadJob = 2 };
@@ -106,17 +107,27 @@ struct JobDesc {
 };
 
 struct Tile {
-  uint32_t job;
-  uint32_t reserved;
+  uint32_t job;         // index into the job table (a slot in live mode)
+  uint32_t gen;         // live mode: generation of the job occupying the slot
   uint64_t start;       // random: index of the tile's first configuration; systematic: its 1-based rank
   uint64_t count;       // configurations in the tile
   uint64_t reserved2;
 };
 
-// Queue control block for the persistent kernel (device memory, or host-mapped for serving).
+// Queue control block of the persistent kernel, in device memory.
+//  list mode (capacity == 0): tiles[0, n_tiles) are fixed; CTAs take them with atomicAdd on head.
+//  live mode (capacity > 0): tiles is a ring the host appends to; the host's copy stream raises tail
+//  after the tiles (and their jobs' descriptors) are in place, CTAs claim with atomicCAS on head and
+//  leave after idle_limit empty polls (the host relaunches when new work arrives). Between tiles a
+//  CTA that finds yield > 0 takes one unit of it and leaves: the host shrinks a ring's share of the
+//  GPU by writing yield, and counts resident-or-queued CTAs as (launched - exited).
 struct QueueCtl {
-  unsigned int head;    // next tile to take (atomicAdd)
-  unsigned int pad[3];
+  unsigned long long head;
+  unsigned long long tail;
+  unsigned int capacity;
+  unsigned int idle_limit;
+  unsigned int yield;
+  unsigned int exited;
 };
 
 }  // namespace sqsg

@@ -282,10 +282,17 @@ __device__ __forceinline__ uint32_t level_hash(unsigned long long key, uint32_t 
   return static_cast<uint32_t>(mix64(key)) & mask;
 }
 
+// Keys above the job's threshold can never be among the final keep+1 levels and are dropped. A probe
+// sequence is bounded; a key that finds no slot marks the table inexact (the host then rebuilds the
+// levels from the records), and from then on the table takes no more keys.
+constexpr int kLevelProbes = 64;
+
 __device__ __forceinline__ void global_level_add(const JobDesc& J, unsigned long long key, unsigned long long count,
                                                  unsigned int sa, unsigned int sb) {
+  if (key > *reinterpret_cast<volatile unsigned long long*>(&J.counters[kThreshold])) return;
+  if (*reinterpret_cast<volatile unsigned long long*>(&J.counters[kLevelOverflow]) != 0ull) return;
   uint32_t h = level_hash(key, kLevelSlots - 1);
-  for (int probe = 0; probe < kLevelSlots; ++probe, h = (h + 1) & (kLevelSlots - 1)) {
+  for (int probe = 0; probe < kLevelProbes; ++probe, h = (h + 1) & (kLevelSlots - 1)) {
     LevelSlot& slot = J.levels[h];
     const unsigned long long prev = atomicCAS(&slot.key, 0ull, key);
     if (prev == 0ull || prev == key) {
@@ -318,8 +325,7 @@ __device__ __forceinline__ void flush_levels(LevelSlot* tab, const JobDesc& J) {
   for (int i = threadIdx.x; i < kCtaLevelSlots; i += kBlock) {
     LevelSlot& slot = tab[i];
     if (slot.key) {
-      const unsigned long long thr = *reinterpret_cast<volatile unsigned long long*>(&J.counters[kThreshold]);
-      if (slot.key <= thr) global_level_add(J, slot.key, slot.count, slot.sum_a, slot.sum_b);
+      global_level_add(J, slot.key, slot.count, slot.sum_a, slot.sum_b);
       slot.key = 0;
       slot.count = 0;
       slot.sum_a = 0;
@@ -711,42 +717,83 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
 }
 
 // ------------------------------------------------------------------------------ persistent kernel
-// Tiles are taken from q->head with one atomicAdd per tile. A CTA stages a job's read-only data
-// (cubes, windows, pair stream, packed species) into shared memory with non-multicast bulk copies
-// whenever its next tile belongs to a different job.
-__global__ void __launch_bounds__(kBlock, kMinBlocks) sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
-                                                      uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
-                                                      unsigned long long* status) {
+constexpr unsigned long long kNoTile = ~0ull;
+
+// Live mode: claim the next published ring entry, waiting (bounded) for the host to publish more.
+__device__ __forceinline__ unsigned long long claim_live(QueueCtl* q, const volatile int32_t* cancel) {
+  uint32_t idle = 0;
+  for (;;) {
+    // a pending yield unit ends this CTA (each loop round takes one unit or sees another CTA take it)
+    uint32_t y = *reinterpret_cast<volatile unsigned int*>(&q->yield);
+    while (y != 0) {
+      const uint32_t o = atomicCAS(&q->yield, y, y - 1);
+      if (o == y) return kNoTile;
+      y = o;
+    }
+    const unsigned long long tl = *reinterpret_cast<volatile unsigned long long*>(&q->tail);
+    const unsigned long long hd = *reinterpret_cast<volatile unsigned long long*>(&q->head);
+    if (hd < tl) {
+      if (atomicCAS(&q->head, hd, hd + 1) == hd) {
+        __threadfence();  // the tile and its job's descriptor were written before tail was raised
+        return hd;
+      }
+      continue;  // another CTA took tile hd
+    }
+    if ((cancel && *cancel) || ++idle > q->idle_limit) return kNoTile;
+    __nanosleep(2000);
+  }
+}
+
+// Tiles are taken from q with one atomic per tile. A CTA stages a job's read-only data (cubes,
+// windows, pair stream, packed species, masks) into shared memory with non-multicast bulk copies
+// whenever its next tile belongs to another job. In live mode every tile ends with a level flush and
+// a decrement of the job's tile count; the CTA that finishes a job's last tile publishes the job's
+// generation in done[slot] (host-mapped memory).
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
+    sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ JobDesc sj;
   __shared__ LevelSlot ctab[kCtaLevelSlots];
-  __shared__ uint32_t s_tile, s_fail;
+  __shared__ unsigned long long s_tile;
+  __shared__ uint32_t s_fail;
   __shared__ __align__(8) uint64_t s_bar;
   if (threadIdx.x == 0) {
     mbar_init(&s_bar, 1);
     s_fail = 0;
   }
   for (int i = threadIdx.x; i < kCtaLevelSlots; i += kBlock) ctab[i] = LevelSlot{0ull, 0ull, 0u, 0u};
-  __syncthreads();
+  const bool live = q->capacity != 0;
   int cur = -1;
+  uint32_t cur_gen = 0;
   uint32_t phase = 0;
   WarpState ws;
   ws.reset();
-  if (threadIdx.x == 0) s_tile = (cancel && *cancel) ? n_tiles : atomicAdd(&q->head, 1u);
+  if (threadIdx.x == 0) {
+    if (live)
+      s_tile = claim_live(q, cancel);
+    else
+      s_tile = (cancel && *cancel) ? kNoTile : atomicAdd(&q->head, 1ull);
+  }
   for (;;) {
     __syncthreads();  // s_tile visible; every thread is done with the previous tile
-    const uint32_t ti = s_tile;
-    if (ti >= n_tiles) break;
-    // the next tile index is fetched now and only consumed after this tile: its latency hides
-    uint32_t next = n_tiles;
-    if (threadIdx.x == 0 && !(cancel && *cancel)) next = atomicAdd(&q->head, 1u);
-    const Tile tile = tiles[ti];
-    if (static_cast<int>(tile.job) != cur) {
-      if (cur >= 0) flush_levels(ctab, sj);  // the previous job's levels leave before its descriptor
+    const unsigned long long ti = s_tile;
+    if (ti == kNoTile || (!live && ti >= n_tiles)) break;
+    // list mode: the next tile index is fetched now and only consumed after this tile
+    unsigned long long next = kNoTile;
+    if (!live && threadIdx.x == 0 && !(cancel && *cancel)) next = atomicAdd(&q->head, 1ull);
+    Tile tile;
+    {
+      const uint4* src = reinterpret_cast<const uint4*>(&tiles[live ? ti % q->capacity : ti]);
+      uint4* dst = reinterpret_cast<uint4*>(&tile);
+      for (int k = 0; k < static_cast<int>(sizeof(Tile) / 16); ++k) dst[k] = __ldcg(src + k);
+    }
+    if (static_cast<int>(tile.job) != cur || tile.gen != cur_gen) {
+      if (cur >= 0 && !live) flush_levels(ctab, sj);  // the previous job's levels leave first
       __syncthreads();
       const uint32_t* src = reinterpret_cast<const uint32_t*>(&jobs[tile.job]);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&sj);
-      for (uint32_t i = threadIdx.x; i < sizeof(JobDesc) / 4; i += kBlock) dst[i] = src[i];
+      for (uint32_t i = threadIdx.x; i < sizeof(JobDesc) / 4; i += kBlock) dst[i] = __ldcg(src + i);
       __syncthreads();
       if (threadIdx.x == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -768,6 +815,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) sqsg_engine(const JobDesc*
         break;
       }
       cur = static_cast<int>(tile.job);
+      cur_gen = tile.gen;
       ws.reset();
     }
     if (sj.k2 == 1) {
@@ -792,13 +840,28 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) sqsg_engine(const JobDesc*
         run_tile<float, 2>(sj, smem, ctab, tile, ws);
     }
     __syncthreads();  // every thread is done with this tile before s_tile changes
+    if (live) {
+      flush_levels(ctab, sj);
+      __threadfence();
+      __syncthreads();
+    }
     if (threadIdx.x == 0) {
-      s_tile = next;
       atomicAdd(&sj.counters[kFinished], static_cast<unsigned long long>(tile.count));
       atomicAdd(&sj.counters[kTilesDone], 1ull);
+      if (live) {
+        __threadfence();  // this tile's counts land before the job's tile count drops
+        if (atomicAdd(&sj.counters[kTilesLeft], ~0ull) == 1ull && done) {
+          __threadfence_system();
+          done[tile.job] = tile.gen;
+        }
+        s_tile = claim_live(q, cancel);
+      } else {
+        s_tile = next;
+      }
     }
   }
-  if (cur >= 0) flush_levels(ctab, sj);
+  if (cur >= 0 && !live) flush_levels(ctab, sj);
+  if (live && threadIdx.x == 0) atomicAdd(&q->exited, 1u);
 }
 
 }  // namespace sqsg

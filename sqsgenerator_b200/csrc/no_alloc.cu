@@ -31,9 +31,9 @@
 
 namespace sqsg {
 
-__global__ void __launch_bounds__(kBlock, kMinBlocks) sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
-                                                      uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
-                                                      unsigned long long* status);
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
+    sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
 
 namespace noalloc {
 
@@ -337,7 +337,7 @@ static Err run(const sqsg_job& job, void* stream, uint32_t* n_levels, double* va
     sqsg_engine<<<static_cast<uint32_t>(grid), kBlock, d.smem_bytes, s>>>(
         reinterpret_cast<const JobDesc*>(dev + kDescOff), reinterpret_cast<const Tile*>(dev + kTilesOff),
         static_cast<uint32_t>(n_tiles), reinterpret_cast<QueueCtl*>(dev + kQueueOff), nullptr,
-        reinterpret_cast<unsigned long long*>(dev + kStatusOff));
+        reinterpret_cast<unsigned long long*>(dev + kStatusOff), nullptr);
     NA_CUDA(cudaGetLastError(), "engine launch failed");
   }
   static LevelSlot lv[kLevelSlots];  // static: guarded by g_mutex, keeps 96 KiB off the caller's stack
