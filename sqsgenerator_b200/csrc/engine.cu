@@ -507,27 +507,63 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
     sp_total += p.N;
     skk_total += static_cast<size_t>(p.S) * p.K * p.K;
   }
-  // Systematic ranks are unique, so only random runs can return one configuration twice.
+  size_t end = 0;
+  while (end < keys.size() && keys[end].obj <= tstar) ++end;
+  // Systematic ranks are unique, so only random runs can return one configuration twice. Equal
+  // configurations have equal objectives, so duplicates are removed inside each objective group:
+  // the group is ordered by (species hash, id) and, among records with equal species, the one with
+  // the smallest id stays (the first one met in (objective, id) order).
   const bool dedup = !pj.systematic;
-  std::unordered_set<std::string> seen;
-  std::string key;
-  run.objective.reserve(keys.size() * sizeof(T));
-  run.species.reserve(keys.size() * sp_total);
-  run.sro.reserve(keys.size() * skk_total * sizeof(T));
+  std::vector<uint8_t> keep_rec(end, 1);
+  if (dedup) {
+    auto species_eq = [&](uint64_t x, uint64_t y) {
+      for (uint32_t p = 0; p < d.n_parts; ++p) {
+        const size_t off = d.parts[p].rec_species_off;
+        if (std::memcmp(&recs[x * rb + off], &recs[y * rb + off], d.parts[p].n_sites) != 0) return false;
+      }
+      return true;
+    };
+    std::vector<std::pair<uint64_t, size_t>> grp;  // (species hash, position in keys)
+    for (size_t g0 = 0; g0 < end;) {
+      size_t g1 = g0 + 1;
+      while (g1 < end && keys[g1].obj == keys[g0].obj) ++g1;
+      if (g1 - g0 > 1) {
+        grp.clear();
+        for (size_t k = g0; k < g1; ++k) {
+          uint64_t h = 0xcbf29ce484222325ull;  // FNV-1a over the record's species bytes
+          const uint8_t* r = &recs[keys[k].idx * rb];
+          for (uint32_t p = 0; p < d.n_parts; ++p)
+            for (uint32_t x = 0; x < d.parts[p].n_sites; ++x) h = (h ^ r[d.parts[p].rec_species_off + x]) * 0x100000001b3ull;
+          grp.emplace_back(h, k);
+        }
+        std::sort(grp.begin(), grp.end());  // ties in hash keep (objective, id) order via the position
+        for (size_t u = 0; u < grp.size();) {
+          size_t v = u + 1;
+          while (v < grp.size() && grp[v].first == grp[u].first) ++v;
+          for (size_t x = u + 1; x < v; ++x)
+            for (size_t y = u; y < x; ++y)
+              if (keep_rec[grp[y].second] && species_eq(keys[grp[x].second].idx, keys[grp[y].second].idx)) {
+                keep_rec[grp[x].second] = 0;
+                break;
+              }
+          u = v;
+        }
+      }
+      g0 = g1;
+    }
+  }
+  run.objective.reserve(end * sizeof(T));
+  run.species.reserve(end * sp_total);
+  run.sro.reserve(end * skk_total * sizeof(T));
   T cur_obj = T(0);
   bool have_cur = false;
   uint64_t cur_count = 0;
-  for (const Key& k : keys) {
-    if (!(k.obj <= tstar)) break;
-    const uint8_t* r = &recs[k.idx * rb];
-    if (dedup) {
-      key.clear();
-      for (uint32_t p = 0; p < d.n_parts; ++p)
-        key.append(reinterpret_cast<const char*>(r + d.parts[p].rec_species_off), d.parts[p].n_sites);
-      if (!seen.insert(key).second) continue;
-    }
-    if (!have_cur || k.obj != cur_obj) {
-      cur_obj = k.obj;
+  for (size_t k = 0; k < end; ++k) {
+    if (!keep_rec[k]) continue;
+    const Key& key = keys[k];
+    const uint8_t* r = &recs[key.idx * rb];
+    if (!have_cur || key.obj != cur_obj) {
+      cur_obj = key.obj;
       have_cur = true;
       cur_count = 0;
     }
@@ -541,7 +577,7 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
       const size_t skk = static_cast<size_t>(P.n_shells) * P.n_species * P.n_species;
       run.sro.insert(run.sro.end(), r + P.rec_sro_off, r + P.rec_sro_off + skk * sizeof(T));
     }
-    run.id.push_back(k.id);
+    run.id.push_back(key.id);
     run.count++;
   }
 }
@@ -958,9 +994,17 @@ struct ServerState {
   std::map<uint64_t, Run> finished;
   std::map<uint64_t, std::pair<sqsg_status, std::string>> failed;
   std::string broken;  // set after a device error: the server fails every job from then on
+  struct Collected {    // a finished job's device state, downloaded; selected by a finalizer thread
+    std::unique_ptr<ServerJob> job;
+    std::vector<unsigned long long> cnt;
+    std::vector<LevelSlot> levels;
+    std::vector<uint8_t> records;
+  };
+  std::deque<Collected> collected;
   std::mutex m;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_work, cv_done, cv_fin;
   std::thread worker;
+  std::vector<std::thread> finalizers;
   bool stop = false;
   uint64_t next_ticket = 1;
   sqsg_server_counters stats{};
@@ -1077,75 +1121,97 @@ static bool try_admit(ServerState& S) {
   return true;
 }
 
-// Collects a finished job: counters, level table and records come back on the copy stream and the
-// result set is selected like sqsg_optimize selects it. A job whose record buffer overflowed is
-// re-admitted at the front of the queue with the threshold and buffer that assess() asks for (the
-// same tiles and Philox counters give the same evaluations), as sqsg_optimize re-runs it. Returns
-// true when the job's result is final.
-static bool finalize(ServerState& S, uint32_t slot) {
-  ServerJob& J = *S.slots[slot];
-  std::vector<unsigned long long> cnt(kNumCounters);
-  CUDA_CHECK(cudaMemcpyAsync(cnt.data(), S.d_counters + static_cast<size_t>(slot) * kNumCounters, cnt.size() * 8,
-                             cudaMemcpyDeviceToHost, S.copy));
-  std::vector<LevelSlot> lv(kLevelSlots);
-  CUDA_CHECK(cudaMemcpyAsync(lv.data(), S.d_levels + static_cast<size_t>(slot) * kLevelSlots,
+// Collects a finished job on the worker thread: counters, level table and records come back on the
+// copy stream, the job's slot and arena memory are released at once, and the selection of its
+// result set is left to a finalizer thread so that admission and launches go on meanwhile.
+static void collect(ServerState& S, uint32_t slot) {
+  ServerState::Collected c;
+  c.job = std::move(S.slots[slot]);
+  ServerJob& J = *c.job;
+  c.cnt.resize(kNumCounters);
+  CUDA_CHECK(cudaMemcpyAsync(c.cnt.data(), S.d_counters + static_cast<size_t>(slot) * kNumCounters,
+                             c.cnt.size() * 8, cudaMemcpyDeviceToHost, S.copy));
+  c.levels.resize(kLevelSlots);
+  CUDA_CHECK(cudaMemcpyAsync(c.levels.data(), S.d_levels + static_cast<size_t>(slot) * kLevelSlots,
                              kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost, S.copy));
   CUDA_CHECK(cudaStreamSynchronize(S.copy));
-  const uint64_t n = std::min<uint64_t>(cnt[kCandidates], J.capacity);
-  std::vector<uint8_t> recs(n * J.pj.record_bytes);
+  const uint64_t n = std::min<uint64_t>(c.cnt[kCandidates], J.capacity);
+  c.records.resize(n * J.pj.record_bytes);
   if (n) {
-    CUDA_CHECK(cudaMemcpyAsync(recs.data(), S.arena + J.arena_off + J.blob_bytes, recs.size(), cudaMemcpyDeviceToHost,
-                               S.copy));
+    CUDA_CHECK(cudaMemcpyAsync(c.records.data(), S.arena + J.arena_off + J.blob_bytes, c.records.size(),
+                               cudaMemcpyDeviceToHost, S.copy));
     CUDA_CHECK(cudaStreamSynchronize(S.copy));
   }
-  const uint64_t arena_records =
-      (S.opt.arena_bytes - std::min<uint64_t>(S.opt.arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) /
-      J.pj.record_bytes;
-  Outcome o = assess(J.pj, cnt.data(), lv, recs, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
-  if (o.rerun) {
-    arena_free(S, J.arena_off, J.arena_bytes);
-    J.capacity = o.rerun_capacity;
-    J.fixed_threshold = true;
-    J.start_threshold = o.rerun_threshold;
-    J.attempt++;
-    S.pending.push_front(std::move(S.slots[slot]));
-    return false;
-  }
-  Run r;
-  r.prec = J.pj.prec;
-  r.n_parts = J.pj.desc.n_parts;
-  r.parts = J.pj.parts;
-  r.tsz = J.pj.tsz;
-  r.levels_exact = o.levels_exact;
-  r.level_value = std::move(o.value);
-  r.level_count = std::move(o.count);
-  r.level_checksum = std::move(o.checksum);
-  r.candidates = cnt[kCandidates];
-  r.truncated = cnt[kRecordsFull] != 0 || r.candidates > J.capacity;
-  if (J.pj.prec == 1)
-    select_results<double>(J.pj, recs, n, r, o.levels_exact, o.tstar);
-  else
-    select_results<float>(J.pj, recs, n, r, o.levels_exact, o.tstar);
-  r.stats.finished = cnt[kFinished];
-  if (r.count) {
-    r.stats.best_objective =
-        J.pj.prec == 1 ? read_t<double>(r.objective.data()) : static_cast<double>(read_t<float>(r.objective.data()));
-    r.stats.best_rank = r.id[0];
-  } else {
-    r.stats.best_objective = std::numeric_limits<double>::infinity();
-  }
-  const uint64_t t_end = now_ns();
-  r.stats.timings_ns[SQSG_TIMING_TOTAL] = t_end - J.t_submit;  // latency: submission to result
-  r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = J.t_admit - J.t_submit;
-  r.stats.timings_ns[SQSG_TIMING_LOOP] = t_end - J.t_admit;
-  r.h2d_bytes = J.h2d_bytes;
-  r.d2h_bytes = kLevelSlots * sizeof(LevelSlot) + kNumCounters * 8 + recs.size();
-  S.stats.completed++;
-  S.stats.configurations += cnt[kFinished];
   arena_free(S, J.arena_off, J.arena_bytes);
-  S.finished.emplace(J.ticket, std::move(r));
-  S.slots[slot].reset();
-  return true;
+  S.collected.push_back(std::move(c));
+  S.cv_fin.notify_one();
+}
+
+// Finalizer thread: selects a collected job's result set like sqsg_optimize selects it, or, when
+// its record buffer overflowed, puts it back at the front of the queue with the threshold and
+// buffer that assess() asks for (the same tiles and Philox counters give the same evaluations).
+static void finalizer_loop(ServerState* Sp) {
+  ServerState& S = *Sp;
+  std::unique_lock<std::mutex> lock(S.m);
+  while (true) {
+    S.cv_fin.wait(lock, [&] { return S.stop || !S.collected.empty(); });
+    if (S.stop) return;
+    ServerState::Collected c = std::move(S.collected.front());
+    S.collected.pop_front();
+    const uint64_t arena_bytes = S.opt.arena_bytes;
+    lock.unlock();
+    ServerJob& J = *c.job;
+    const unsigned long long* cnt = c.cnt.data();
+    const uint64_t n = c.records.size() / J.pj.record_bytes;
+    const uint64_t arena_records =
+        (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) / J.pj.record_bytes;
+    Outcome o = assess(J.pj, cnt, c.levels, c.records, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
+    Run r;
+    if (!o.rerun) {
+      r.prec = J.pj.prec;
+      r.n_parts = J.pj.desc.n_parts;
+      r.parts = J.pj.parts;
+      r.tsz = J.pj.tsz;
+      r.levels_exact = o.levels_exact;
+      r.level_value = std::move(o.value);
+      r.level_count = std::move(o.count);
+      r.level_checksum = std::move(o.checksum);
+      r.candidates = cnt[kCandidates];
+      r.truncated = cnt[kRecordsFull] != 0 || r.candidates > J.capacity;
+      if (J.pj.prec == 1)
+        select_results<double>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
+      else
+        select_results<float>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
+      r.stats.finished = cnt[kFinished];
+      if (r.count) {
+        r.stats.best_objective = J.pj.prec == 1 ? read_t<double>(r.objective.data())
+                                                : static_cast<double>(read_t<float>(r.objective.data()));
+        r.stats.best_rank = r.id[0];
+      } else {
+        r.stats.best_objective = std::numeric_limits<double>::infinity();
+      }
+      const uint64_t t_end = now_ns();
+      r.stats.timings_ns[SQSG_TIMING_TOTAL] = t_end - J.t_submit;  // latency: submission to result
+      r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = J.t_admit - J.t_submit;
+      r.stats.timings_ns[SQSG_TIMING_LOOP] = t_end - J.t_admit;
+      r.h2d_bytes = J.h2d_bytes;
+      r.d2h_bytes = kLevelSlots * sizeof(LevelSlot) + kNumCounters * 8 + c.records.size();
+    }
+    lock.lock();
+    if (o.rerun) {
+      J.capacity = o.rerun_capacity;
+      J.fixed_threshold = true;
+      J.start_threshold = o.rerun_threshold;
+      J.attempt++;
+      S.pending.push_front(std::move(c.job));
+      S.cv_work.notify_one();
+    } else {
+      S.stats.completed++;
+      S.stats.configurations += cnt[kFinished];
+      S.finished.emplace(J.ticket, std::move(r));
+      S.cv_done.notify_all();
+    }
+  }
 }
 
 static void write_yield(ServerState& S, int b, uint32_t value) {
@@ -1228,7 +1294,7 @@ static void server_loop(ServerState* Sp) {
         for (uint32_t k = 0; k < S.slots.size(); ++k) {
           if (!S.slots[k]) continue;
           if (*reinterpret_cast<volatile uint32_t*>(&S.h_done[k]) == S.slots[k]->gen) {
-            if (finalize(S, k)) S.cv_done.notify_all();
+            collect(S, k);
             progress = true;
           }
         }
@@ -1513,6 +1579,7 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     S.slots.resize(nslot);
     S.slot_gen.assign(nslot, 0);
     S.worker = std::thread(server_loop, &S);
+    for (int k = 0; k < 4; ++k) S.finalizers.emplace_back(finalizer_loop, &S);
     *out = srv.release();
   });
 }
@@ -1608,8 +1675,11 @@ sqsg_status sqsg_server_destroy(sqsg_server* server) {
     std::lock_guard<std::mutex> l(S.m);
     S.stop = true;
     S.cv_work.notify_all();
+    S.cv_fin.notify_all();
   }
   if (S.worker.joinable()) S.worker.join();
+  for (auto& t : S.finalizers)
+    if (t.joinable()) t.join();
   cudaSetDevice(S.device);
   // every CTA leaves at its next claim: no tile is started after this
   if (S.d_ctl && S.h_yield && S.copy) {
