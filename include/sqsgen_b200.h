@@ -242,7 +242,7 @@ typedef struct sqsg_server sqsg_server;
 typedef struct {
   int32_t device;
   uint32_t max_jobs;              /* jobs admitted at once (0: 256) */
-  uint64_t arena_bytes;           /* device memory for admitted jobs' data and records (0: 4 GiB) */
+  uint64_t arena_bytes;           /* device memory for admitted jobs' data and records (0: 16 GiB, at most 1/4 of free memory) */
   uint64_t default_max_results;   /* record capacity of a job that leaves max_results at 0 (0: 65536) */
 } sqsg_server_options;
 

@@ -17,8 +17,9 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libsqsg_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["engine.cu", "geometry.cpp", "microbench.cu", "no_alloc.cu"]
-HEADERS = ["engine.cuh", "engine_device.cuh", "permutation.h", "philox.cuh", "sqsg_internal.h", "tiles.h"]
+SOURCES = ["engine.cu", "geometry.cpp", "microbench.cu", "no_alloc.cu", "select.cu"]
+HEADERS = ["engine.cuh", "engine_device.cuh", "permutation.h", "philox.cuh", "select.h", "sqsg_internal.h",
+           "tiles.h"]
 
 
 def nvcc() -> str:

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "engine_device.cuh"
+#include "select.h"
 #include "sqsg_internal.h"
 #include "tiles.h"
 
@@ -313,11 +314,15 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   return pj;
 }
 
-static void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles) {
-  for_each_tile(pj.range_first, pj.range_count, pj.systematic, [&](Tile t) {
-    t.job = job_index;
-    tiles.push_back(t);
-  });
+static void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles,
+                       uint64_t max_per_thread = 1u << 16) {
+  for_each_tile(
+      pj.range_first, pj.range_count, pj.systematic,
+      [&](Tile t) {
+        t.job = job_index;
+        tiles.push_back(t);
+      },
+      max_per_thread);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -343,6 +348,7 @@ struct Workspace {
   cudaStream_t stream = nullptr, monitor = nullptr;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   DevBuf blob, records, counters, levels, tiles, jobs, queue, status, trace_sp, trace_bd, trace_obj, trace_id;
+  SelectScratch select;
   int32_t* ctrl_host = nullptr;  // mapped pinned: [0] = cancel
   int32_t* ctrl_dev = nullptr;
   explicit Workspace(int dev) : device(dev) {
@@ -355,6 +361,7 @@ struct Workspace {
     std::memset(ctrl_host, 0, 64);
   }
   ~Workspace() {
+    select.release();
     if (stream) cudaStreamDestroy(stream);
     if (monitor) cudaStreamDestroy(monitor);
     if (ev_start) cudaEventDestroy(ev_start);
@@ -580,6 +587,47 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
     run.id.push_back(key.id);
     run.count++;
   }
+}
+
+// Candidate sets at least this large are selected on the device.
+constexpr uint64_t kDeviceSelectMin = 32768;
+// Device memory a re-run may give a job's records when the first pass overflowed (random runs over
+// small configuration spaces revisit configurations and store every visit at or below T*).
+constexpr uint64_t kRerunRecordBytes = 16ull << 30;
+
+static RecordLayout record_layout(const PreparedJob& pj) {
+  RecordLayout L;
+  L.record_bytes = static_cast<uint32_t>(pj.record_bytes);
+  L.tsz = static_cast<uint32_t>(pj.tsz);
+  L.n_parts = pj.desc.n_parts;
+  for (uint32_t p = 0; p < pj.desc.n_parts; ++p) {
+    const PartDesc& P = pj.desc.parts[p];
+    L.obj_off[p] = P.rec_obj_off;
+    L.species_off[p] = P.rec_species_off;
+    L.n_sites[p] = P.n_sites;
+    L.sro_off[p] = P.rec_sro_off;
+    L.sro_bytes[p] = static_cast<uint32_t>(static_cast<size_t>(P.n_shells) * P.n_species * P.n_species * pj.tsz);
+  }
+  return L;
+}
+
+// Selects the result set of device-resident records into run (exact levels required). Returns false
+// when the device path does not apply; the caller then downloads the records and selects on the host.
+static bool select_records_on_device(SelectScratch& scratch, cudaStream_t stream, const PreparedJob& pj,
+                                     const uint8_t* d_records, uint64_t n, const std::vector<double>& levels,
+                                     Run& run) {
+  if (n < kDeviceSelectMin) return false;  // small sets: the host is quicker than the launches
+  SelectedSet set;
+  if (!select_on_device(scratch, stream, record_layout(pj), d_records, n, levels, !pj.systematic, pj.max_rpo,
+                        pj.range_first + pj.range_count + 1, set))
+    return false;
+  run.count = set.count;
+  run.objective = std::move(set.objective);
+  run.sub_objective = std::move(set.sub_objective);
+  run.species = std::move(set.species);
+  run.sro = std::move(set.sro);
+  run.id = std::move(set.id);
+  return true;
 }
 
 // What one pass of a job left behind: its exact objective levels (keep+1 smallest distinct
@@ -836,8 +884,10 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     CUDA_CHECK(cudaMemcpy(&status, ws->status.p, sizeof(status), cudaMemcpyDeviceToHost));
     if (status == kErrStageTimeout) throw timeout_error("shared-memory staging wait timed out on the device");
     if (status != 0) throw cuda_error("device error code " + std::to_string(status));
-    // Every job's counters, level table and records come back; a job whose record buffer overflowed
-    // is re-run (see assess) when the caller left the capacity to the library.
+    // Every job's counters and level table come back; a job whose record buffer overflowed is re-run
+    // (see assess) when the caller left the capacity to the library. Records come back only when
+    // the level table overflowed (the levels are then rebuilt from them on the host) or the set is
+    // small; otherwise the result set is selected on the device and only it is copied out.
     bool rerun = false;
     std::vector<std::vector<uint8_t>> recs(nj);
     std::vector<Outcome> outc(nj);
@@ -847,14 +897,17 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       std::vector<LevelSlot> lv(kLevelSlots);
       CUDA_CHECK(cudaMemcpy(lv.data(), static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots,
                             kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost));
+      d2h_bytes += kLevelSlots * sizeof(LevelSlot);
       const uint64_t n = std::min<uint64_t>(cj[kCandidates], capacity[j]);
-      recs[j].resize(n * pjs[j].record_bytes);
-      if (n)
-        CUDA_CHECK(cudaMemcpy(recs[j].data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], recs[j].size(),
-                              cudaMemcpyDeviceToHost));
-      d2h_bytes += kLevelSlots * sizeof(LevelSlot) + recs[j].size();
+      if (cj[kLevelOverflow]) {
+        recs[j].resize(n * pjs[j].record_bytes);
+        if (n)
+          CUDA_CHECK(cudaMemcpy(recs[j].data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], recs[j].size(),
+                                cudaMemcpyDeviceToHost));
+        d2h_bytes += recs[j].size();
+      }
       const bool may_rerun = !pjs[j].max_results && attempt < 2;
-      outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, (4ull << 30) / pjs[j].record_bytes);
+      outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, kRerunRecordBytes / pjs[j].record_bytes);
       if (outc[j].rerun) {
         capacity[j] = outc[j].rerun_capacity;
         fixed_threshold[j] = true;
@@ -868,25 +921,36 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     runs.assign(nj, Run{});
     for (size_t j = 0; j < nj; ++j) {
       const unsigned long long* cj = &cnt[j * kNumCounters];
-      const uint64_t n = recs[j].size() / pjs[j].record_bytes;
+      const uint64_t n = std::min<uint64_t>(cj[kCandidates], capacity[j]);
       Run& r = runs[j];
-      r.h2d_bytes = h2d_bytes / nj;
-      r.d2h_bytes = d2h_bytes / nj;
       r.prec = pjs[j].prec;
       r.n_parts = pjs[j].desc.n_parts;
       r.parts = pjs[j].parts;
       r.tsz = pjs[j].tsz;
       Outcome& o = outc[j];
       r.levels_exact = o.levels_exact;
+      r.candidates = cj[kCandidates];
+      r.truncated = cj[kRecordsFull] != 0 || r.candidates > capacity[j];
+      const uint8_t* d_recs = static_cast<const uint8_t*>(ws->records.p) + rec_off[j];
+      bool done = false;
+      if (!cj[kLevelOverflow] && o.levels_exact)
+        done = select_records_on_device(ws->select, ws->stream, pjs[j], d_recs, n, o.value, r);
+      if (!done) {
+        if (recs[j].empty() && n) {
+          recs[j].resize(n * pjs[j].record_bytes);
+          CUDA_CHECK(cudaMemcpy(recs[j].data(), d_recs, recs[j].size(), cudaMemcpyDeviceToHost));
+          d2h_bytes += recs[j].size();
+        }
+        if (pjs[j].prec == 1)
+          select_results<double>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
+        else
+          select_results<float>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
+      } else {
+        d2h_bytes += r.objective.size() + r.sub_objective.size() + r.species.size() + r.sro.size() + r.id.size() * 8;
+      }
       r.level_value = std::move(o.value);
       r.level_count = std::move(o.count);
       r.level_checksum = std::move(o.checksum);
-      r.candidates = cj[kCandidates];
-      r.truncated = cj[kRecordsFull] != 0 || r.candidates > capacity[j];
-      if (pjs[j].prec == 1)
-        select_results<double>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
-      else
-        select_results<float>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
       r.stats.finished = cj[kFinished];
       r.stats.working = 0;
       if (r.count) {
@@ -896,6 +960,10 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       } else {
         r.stats.best_objective = std::numeric_limits<double>::infinity();
       }
+    }
+    for (size_t j = 0; j < nj; ++j) {
+      runs[j].h2d_bytes = h2d_bytes / nj;
+      runs[j].d2h_bytes = d2h_bytes / nj;
     }
     if (trace && trace->capacity) {
       const PreparedJob& pj = pjs[0];
@@ -932,12 +1000,18 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
 // that finishes a job's last tile marks the job's slot done in host-mapped memory; the worker then
 // downloads its records and levels, selects the result set and wakes the waiting caller. A job's
 // result does not depend on what else runs: its tiles and Philox counters depend only on the job.
-constexpr int kBuckets = 4;
-constexpr size_t kBucketSmem[kBuckets] = {24u << 10, 56u << 10, 112u << 10, 0};  // 0: device maximum
+// One ring per occupancy level of sqsg_engine (5, 4, 3, 2, 1 CTAs per SM): a job goes to the ring
+// with the largest shared-memory size it fits, i.e. the highest occupancy its data allow.
+constexpr int kBuckets = 5;
+constexpr int kMaxSm = 256;
 constexpr uint64_t kRingCap = 1u << 20;
-constexpr uint32_t kIdlePolls = 250;         // ~0.5 ms of empty polls before a CTA leaves its ring
-constexpr int kLaunchSlots = 8;              // concurrent launches per ring
-constexpr uint64_t kRebalanceNs = 1000000;   // at most one shrink per ring per millisecond
+constexpr uint32_t kIdlePolls = 250;          // ~0.5 ms of empty polls before a CTA leaves its ring
+constexpr int kLaunchSlots = 32;              // concurrent launches per ring
+constexpr uint64_t kRepartitionNs = 2000000;  // at most one SM repartition per 2 ms
+constexpr uint64_t kRelaunchNs = 1000000;     // at most one top-up launch per ring per ms
+constexpr uint8_t kNoOwner = 0xff;
+constexpr int kReservedSm = 2;                // SMs left to no ring: result selection runs there
+constexpr uint64_t kTilePairs = 1u << 19;     // pair evaluations per thread and tile, at most
 
 struct ServerJob {
   uint64_t ticket = 0;
@@ -945,6 +1019,8 @@ struct ServerJob {
   int bucket = 0;
   PreparedJob pj;
   std::vector<Tile> tiles;
+  std::vector<uint64_t> cum;  // cum[k] = configurations in tiles[0, k)
+  uint64_t pairs = 0;         // pair evaluations per configuration
   size_t arena_off = 0, arena_bytes = 0, blob_bytes = 0;
   uint64_t capacity = 0;
   bool user_capacity = false;
@@ -962,18 +1038,20 @@ struct LaunchSlot {
   bool busy = false;
 };
 
-// One ring of tiles per shared-memory class; several launches of sqsg_engine may serve a ring at once.
+// One ring of tiles per shared-memory class; launches of sqsg_engine serve a ring on the SMs that
+// the owner table gives it.
 struct Ring {
   size_t smem = 0;
-  uint32_t full_grid = 0;     // CTAs that fill the device at this shared-memory size
+  uint32_t per_sm = 1;        // resident CTAs per SM at this shared-memory size
   uint64_t published = 0;     // tiles appended so far (the ring's tail)
   uint32_t launched = 0;      // CTAs launched so far (wraps like QueueCtl::exited)
-  uint64_t last_shrink = 0;
+  uint64_t last_launch = 0;
   LaunchSlot ls[kLaunchSlots];
 };
 
 struct ServerState {
   int device = 0;
+  int n_sm = 0;
   sqsg_server_options opt{};
   cudaStream_t copy = nullptr;
   Ring rings[kBuckets];
@@ -983,9 +1061,14 @@ struct ServerState {
   unsigned long long* d_counters = nullptr;
   LevelSlot* d_levels = nullptr;
   Tile* d_ring[kBuckets] = {};
-  uint8_t* d_ctl = nullptr;   // kBuckets QueueCtl, then the device status word
-  uint8_t* h_ctl = nullptr;   // pinned mirror of d_ctl
+  // d_ctl: kBuckets QueueCtl, the device status word (64 B), kBuckets x kMaxSm alive counters
+  uint8_t* d_ctl = nullptr;
+  uint8_t* h_ctl = nullptr;     // pinned mirror of d_ctl
+  uint8_t* d_owner = nullptr;   // owner ring of each SM
+  uint8_t* h_owner = nullptr;   // pinned: the table as last written
+  uint64_t last_partition = 0;
   uint32_t* h_yield = nullptr;  // pinned sources of yield writes
+  uint8_t* h_zero = nullptr;    // pinned zeros: level tables are cleared by copy, not by a kernel
   uint32_t* h_done = nullptr;
   uint32_t* d_done = nullptr;
   std::vector<std::unique_ptr<ServerJob>> slots;
@@ -994,7 +1077,7 @@ struct ServerState {
   std::map<uint64_t, Run> finished;
   std::map<uint64_t, std::pair<sqsg_status, std::string>> failed;
   std::string broken;  // set after a device error: the server fails every job from then on
-  struct Collected {    // a finished job's device state, downloaded; selected by a finalizer thread
+  struct Collected {    // a finished job's counters and levels, downloaded; selected by a finalizer thread
     std::unique_ptr<ServerJob> job;
     std::vector<unsigned long long> cnt;
     std::vector<LevelSlot> levels;
@@ -1013,9 +1096,16 @@ struct ServerState {
   unsigned long long device_status() const {
     return *reinterpret_cast<const unsigned long long*>(h_ctl + kBuckets * sizeof(QueueCtl));
   }
+  unsigned int* d_alive(int b) const {
+    return reinterpret_cast<unsigned int*>(d_ctl + kBuckets * sizeof(QueueCtl) + 64) + static_cast<size_t>(b) * kMaxSm;
+  }
+  const unsigned int* h_alive(int b) const {
+    return reinterpret_cast<const unsigned int*>(h_ctl + kBuckets * sizeof(QueueCtl) + 64) +
+           static_cast<size_t>(b) * kMaxSm;
+  }
 };
 
-constexpr size_t kCtlBytes = kBuckets * sizeof(QueueCtl) + 64;
+constexpr size_t kCtlBytes = kBuckets * sizeof(QueueCtl) + 64 + kBuckets * kMaxSm * sizeof(unsigned int);
 
 static bool arena_alloc(ServerState& S, size_t bytes, size_t* off) {
   bytes = align_up(bytes, 256);
@@ -1097,7 +1187,8 @@ static bool try_admit(ServerState& S) {
   }
   CUDA_CHECK(cudaMemcpyAsync(S.arena + J.arena_off, J.pj.blob.data(), J.pj.blob.size(), cudaMemcpyHostToDevice, S.copy));
   CUDA_CHECK(cudaMemcpyAsync(d.counters, init.data(), init.size() * 8, cudaMemcpyHostToDevice, S.copy));
-  CUDA_CHECK(cudaMemsetAsync(d.levels, 0, kLevelSlots * sizeof(LevelSlot), S.copy));
+  // copies only: a memset kernel would wait for SMs held by the running persistent kernels
+  CUDA_CHECK(cudaMemcpyAsync(d.levels, S.h_zero, kLevelSlots * sizeof(LevelSlot), cudaMemcpyHostToDevice, S.copy));
   CUDA_CHECK(cudaMemcpyAsync(S.d_jobs + slot, &d, sizeof(d), cudaMemcpyHostToDevice, S.copy));
   const uint64_t n = J.tiles.size();
   const uint64_t pos = R.published % kRingCap;
@@ -1121,9 +1212,10 @@ static bool try_admit(ServerState& S) {
   return true;
 }
 
-// Collects a finished job on the worker thread: counters, level table and records come back on the
-// copy stream, the job's slot and arena memory are released at once, and the selection of its
-// result set is left to a finalizer thread so that admission and launches go on meanwhile.
+// Collects a finished job on the worker thread: counters and level table come back on the copy
+// stream (the records too when the level table overflowed) and the job's slot is released at once.
+// Its arena memory stays with it until a finalizer thread has selected the result set, so that
+// admission and launches go on meanwhile.
 static void collect(ServerState& S, uint32_t slot) {
   ServerState::Collected c;
   c.job = std::move(S.slots[slot]);
@@ -1136,69 +1228,100 @@ static void collect(ServerState& S, uint32_t slot) {
                              kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost, S.copy));
   CUDA_CHECK(cudaStreamSynchronize(S.copy));
   const uint64_t n = std::min<uint64_t>(c.cnt[kCandidates], J.capacity);
-  c.records.resize(n * J.pj.record_bytes);
-  if (n) {
+  if (c.cnt[kLevelOverflow] && n) {
+    c.records.resize(n * J.pj.record_bytes);
     CUDA_CHECK(cudaMemcpyAsync(c.records.data(), S.arena + J.arena_off + J.blob_bytes, c.records.size(),
                                cudaMemcpyDeviceToHost, S.copy));
     CUDA_CHECK(cudaStreamSynchronize(S.copy));
   }
-  arena_free(S, J.arena_off, J.arena_bytes);
   S.collected.push_back(std::move(c));
   S.cv_fin.notify_one();
 }
 
-// Finalizer thread: selects a collected job's result set like sqsg_optimize selects it, or, when
-// its record buffer overflowed, puts it back at the front of the queue with the threshold and
-// buffer that assess() asks for (the same tiles and Philox counters give the same evaluations).
+// Finalizer thread: selects a collected job's result set like sqsg_optimize selects it (on the
+// device from the job's arena records, on its own stream, for large sets), or, when its record
+// buffer overflowed, puts it back at the front of the queue with the threshold and buffer that
+// assess() asks for (the same configurations are evaluated again).
 static void finalizer_loop(ServerState* Sp) {
   ServerState& S = *Sp;
+  cudaSetDevice(S.device);
+  cudaStream_t stream = nullptr;
+  SelectScratch scratch;
   std::unique_lock<std::mutex> lock(S.m);
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    stream = nullptr;
+    if (S.broken.empty()) S.broken = "a finalizer could not create its stream";
+  }
   while (true) {
     S.cv_fin.wait(lock, [&] { return S.stop || !S.collected.empty(); });
-    if (S.stop) return;
+    if (S.stop) break;
     ServerState::Collected c = std::move(S.collected.front());
     S.collected.pop_front();
     const uint64_t arena_bytes = S.opt.arena_bytes;
     lock.unlock();
     ServerJob& J = *c.job;
     const unsigned long long* cnt = c.cnt.data();
-    const uint64_t n = c.records.size() / J.pj.record_bytes;
+    const uint64_t n = std::min<uint64_t>(cnt[kCandidates], J.capacity);
     const uint64_t arena_records =
         (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) / J.pj.record_bytes;
-    Outcome o = assess(J.pj, cnt, c.levels, c.records, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
     Run r;
-    if (!o.rerun) {
-      r.prec = J.pj.prec;
-      r.n_parts = J.pj.desc.n_parts;
-      r.parts = J.pj.parts;
-      r.tsz = J.pj.tsz;
-      r.levels_exact = o.levels_exact;
-      r.level_value = std::move(o.value);
-      r.level_count = std::move(o.count);
-      r.level_checksum = std::move(o.checksum);
-      r.candidates = cnt[kCandidates];
-      r.truncated = cnt[kRecordsFull] != 0 || r.candidates > J.capacity;
-      if (J.pj.prec == 1)
-        select_results<double>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
-      else
-        select_results<float>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
-      r.stats.finished = cnt[kFinished];
-      if (r.count) {
-        r.stats.best_objective = J.pj.prec == 1 ? read_t<double>(r.objective.data())
-                                                : static_cast<double>(read_t<float>(r.objective.data()));
-        r.stats.best_rank = r.id[0];
-      } else {
-        r.stats.best_objective = std::numeric_limits<double>::infinity();
+    std::string error;
+    Outcome o;
+    try {
+      o = assess(J.pj, cnt, c.levels, c.records, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
+      if (!o.rerun) {
+        r.prec = J.pj.prec;
+        r.n_parts = J.pj.desc.n_parts;
+        r.parts = J.pj.parts;
+        r.tsz = J.pj.tsz;
+        r.levels_exact = o.levels_exact;
+        r.candidates = cnt[kCandidates];
+        r.truncated = cnt[kRecordsFull] != 0 || r.candidates > J.capacity;
+        const uint8_t* d_recs = S.arena + J.arena_off + J.blob_bytes;
+        bool done = false;
+        if (!cnt[kLevelOverflow] && o.levels_exact && stream)
+          done = select_records_on_device(scratch, stream, J.pj, d_recs, n, o.value, r);
+        if (!done) {
+          if (c.records.empty() && n) {
+            if (!stream) throw cuda_error("no stream to download records on");
+            c.records.resize(n * J.pj.record_bytes);
+            CUDA_CHECK(cudaMemcpyAsync(c.records.data(), d_recs, c.records.size(), cudaMemcpyDeviceToHost, stream));
+            CUDA_CHECK(cudaStreamSynchronize(stream));
+          }
+          if (J.pj.prec == 1)
+            select_results<double>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
+          else
+            select_results<float>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
+        }
+        r.level_value = std::move(o.value);
+        r.level_count = std::move(o.count);
+        r.level_checksum = std::move(o.checksum);
+        r.stats.finished = cnt[kFinished];
+        if (r.count) {
+          r.stats.best_objective = J.pj.prec == 1 ? read_t<double>(r.objective.data())
+                                                  : static_cast<double>(read_t<float>(r.objective.data()));
+          r.stats.best_rank = r.id[0];
+        } else {
+          r.stats.best_objective = std::numeric_limits<double>::infinity();
+        }
+        const uint64_t t_end = now_ns();
+        r.stats.timings_ns[SQSG_TIMING_TOTAL] = t_end - J.t_submit;  // latency: submission to result
+        r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = J.t_admit - J.t_submit;
+        r.stats.timings_ns[SQSG_TIMING_LOOP] = t_end - J.t_admit;
+        r.h2d_bytes = J.h2d_bytes;
+        r.d2h_bytes = kLevelSlots * sizeof(LevelSlot) + kNumCounters * 8 + c.records.size() + r.objective.size() +
+                      r.sub_objective.size() + r.species.size() + r.sro.size() + r.id.size() * 8;
       }
-      const uint64_t t_end = now_ns();
-      r.stats.timings_ns[SQSG_TIMING_TOTAL] = t_end - J.t_submit;  // latency: submission to result
-      r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = J.t_admit - J.t_submit;
-      r.stats.timings_ns[SQSG_TIMING_LOOP] = t_end - J.t_admit;
-      r.h2d_bytes = J.h2d_bytes;
-      r.d2h_bytes = kLevelSlots * sizeof(LevelSlot) + kNumCounters * 8 + c.records.size();
+    } catch (std::exception const& ex) {
+      error = ex.what();
     }
     lock.lock();
-    if (o.rerun) {
+    arena_free(S, J.arena_off, J.arena_bytes);
+    if (!error.empty()) {
+      S.failed[J.ticket] = {SQSG_ERR_CUDA, error};
+      S.cv_done.notify_all();
+    } else if (o.rerun) {
       J.capacity = o.rerun_capacity;
       J.fixed_threshold = true;
       J.start_threshold = o.rerun_threshold;
@@ -1212,56 +1335,117 @@ static void finalizer_loop(ServerState* Sp) {
       S.cv_done.notify_all();
     }
   }
+  lock.unlock();
+  scratch.release();
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
 }
 
-static void write_yield(ServerState& S, int b, uint32_t value) {
-  S.h_yield[b] = value;
-  CUDA_CHECK(cudaMemcpyAsync(&S.q(b)->yield, &S.h_yield[b], sizeof(uint32_t), cudaMemcpyHostToDevice, S.copy));
-  CUDA_CHECK(cudaStreamSynchronize(S.copy));
-}
-
-// Shares the device between the rings that hold unclaimed tiles: each gets an equal part of the
-// CTAs that would fill the GPU at its shared-memory size. A ring below its share gets a launch of
-// the missing CTAs; a ring above it (after another ring gained work) is asked to give CTAs back
-// through its yield counter, which CTAs honour between tiles. Rings without unclaimed tiles are
-// left alone: their CTAs finish their tiles and leave after kIdlePolls empty polls.
+// Partitions the SMs (all but kReservedSm) between the rings that hold unclaimed tiles, in
+// proportion to their outstanding work in SM-time (pair evaluations of the unclaimed tiles over the
+// ring's CTAs per SM), so that every SM runs CTAs of one shared-memory size at that size's full
+// occupancy. A ring whose SMs hold fewer of its CTAs than they can take gets a launch of a full
+// grid; CTAs that land on another ring's SM leave at once, and CTAs leave between tiles when their
+// SM changes hands.
 static void schedule(ServerState& S) {
-  uint64_t unclaimed[kBuckets];
+  const uint64_t now = now_ns();
+  double work[kBuckets] = {};
+  double total = 0.0;
   int n_want = 0;
+  for (auto& x : S.slots) {
+    if (!x) continue;
+    const uint64_t head = S.hq(x->bucket).head;
+    if (head >= x->ring_end) continue;
+    const uint64_t k0 = head > x->ring_begin ? head - x->ring_begin : 0;
+    const double configs = static_cast<double>(x->cum.back() - x->cum[k0]);
+    work[x->bucket] += configs * static_cast<double>(x->pairs) / S.rings[x->bucket].per_sm;
+  }
   for (int b = 0; b < kBuckets; ++b) {
-    const uint64_t head = S.hq(b).head;
-    unclaimed[b] = S.rings[b].published > head ? S.rings[b].published - head : 0;
-    n_want += unclaimed[b] ? 1 : 0;
+    total += work[b];
+    n_want += work[b] > 0 ? 1 : 0;
   }
   if (!n_want) return;
-  const uint64_t now = now_ns();
+  const int n_sm = S.n_sm - kReservedSm;
+  int cur[kBuckets] = {};
+  for (int sm = 0; sm < n_sm; ++sm)
+    if (S.h_owner[sm] < kBuckets) cur[S.h_owner[sm]]++;
+  int want[kBuckets] = {};
+  double frac[kBuckets] = {};
+  int given = 0;
   for (int b = 0; b < kBuckets; ++b) {
-    if (!unclaimed[b]) continue;
-    Ring& R = S.rings[b];
-    const QueueCtl& q = S.hq(b);
-    const uint32_t live = R.launched - q.exited;
-    const uint32_t eff = live > q.yield ? live - q.yield : 0;
-    uint64_t target = std::max<uint32_t>(1, R.full_grid / n_want);
-    target = std::min<uint64_t>(target, eff + unclaimed[b]);
-    if (eff < target) {
-      for (auto& L : R.ls) {
-        if (L.busy) continue;
-        const uint32_t grid = static_cast<uint32_t>(target - eff);
-        if (q.yield) write_yield(S, b, 0);  // a pending yield would send the new CTAs away
-        sqsg_engine<<<grid, kBlock, R.smem, L.stream>>>(S.d_jobs, S.d_ring[b], 0, S.q(b), nullptr,
-                                                         reinterpret_cast<unsigned long long*>(
-                                                             S.d_ctl + kBuckets * sizeof(QueueCtl)),
-                                                         S.d_done);
-        CUDA_CHECK(cudaGetLastError());
-        CUDA_CHECK(cudaEventRecord(L.done, L.stream));
-        L.busy = true;
-        R.launched += grid;
-        S.stats.launches++;
-        break;
+    if (work[b] <= 0) continue;
+    const double share = n_sm * work[b] / total;
+    want[b] = std::max(1, static_cast<int>(share));
+    frac[b] = share - static_cast<int>(share);
+    given += want[b];
+  }
+  while (given < n_sm) {  // hand out the remainder by largest fractional share
+    int best = -1;
+    for (int b = 0; b < kBuckets; ++b)
+      if (work[b] > 0 && (best < 0 || frac[b] > frac[best])) best = b;
+    want[best]++;
+    frac[best] -= 1.0;
+    given++;
+  }
+  while (given > n_sm) {  // rings held at one SM each took too many: trim the largest
+    int big = 0;
+    for (int b = 1; b < kBuckets; ++b)
+      if (want[b] > want[big]) big = b;
+    want[big]--;
+    given--;
+  }
+  bool change = false;
+  for (int b = 0; b < kBuckets; ++b) {
+    if (work[b] > 0 && cur[b] == 0) change = true;
+    if (work[b] <= 0 && cur[b] > 0) change = true;
+    if (std::abs(want[b] - cur[b]) > std::max(2, cur[b] / 4)) change = true;
+  }
+  if (change && now - S.last_partition > kRepartitionNs) {
+    std::vector<int> pool;  // SMs to hand out: unowned, of rings without work, or a ring's excess
+    for (int sm = n_sm - 1; sm >= 0; --sm) {
+      const uint8_t o = S.h_owner[sm];
+      if (o >= kBuckets || work[o] <= 0 || cur[o] > want[o]) {
+        if (o < kBuckets && work[o] > 0) cur[o]--;
+        S.h_owner[sm] = kNoOwner;
+        pool.push_back(sm);
       }
-    } else if (n_want > 1 && eff > target + target / 8 && now - R.last_shrink > kRebalanceNs) {
-      write_yield(S, b, static_cast<uint32_t>(live - target));
-      R.last_shrink = now;
+    }
+    for (int b = 0; b < kBuckets; ++b) cur[b] = 0;
+    for (int sm = 0; sm < n_sm; ++sm)
+      if (S.h_owner[sm] < kBuckets) cur[S.h_owner[sm]]++;
+    for (int b = 0; b < kBuckets; ++b)
+      while (cur[b] < want[b] && !pool.empty()) {
+        S.h_owner[pool.back()] = static_cast<uint8_t>(b);
+        pool.pop_back();
+        cur[b]++;
+      }
+    CUDA_CHECK(cudaMemcpyAsync(S.d_owner, S.h_owner, kMaxSm, cudaMemcpyHostToDevice, S.copy));
+    CUDA_CHECK(cudaStreamSynchronize(S.copy));
+    S.last_partition = now;
+  }
+  for (int b = 0; b < kBuckets; ++b) {
+    if (work[b] <= 0) continue;
+    Ring& R = S.rings[b];
+    uint64_t room = 0;
+    const unsigned int* alive = S.h_alive(b);
+    for (int sm = 0; sm < n_sm; ++sm)
+      if (S.h_owner[sm] == b && alive[sm] < R.per_sm) room += R.per_sm - alive[sm];
+    if (room < R.per_sm || now - R.last_launch < kRelaunchNs) continue;  // top up by whole SMs
+    for (auto& L : R.ls) {
+      if (L.busy) continue;
+      const uint32_t grid = R.per_sm * static_cast<uint32_t>(S.n_sm);
+      sqsg_engine<<<grid, kBlock, R.smem, L.stream>>>(
+          S.d_jobs, S.d_ring[b], 0, S.q(b), nullptr,
+          reinterpret_cast<unsigned long long*>(S.d_ctl + kBuckets * sizeof(QueueCtl)), S.d_done);
+      CUDA_CHECK(cudaGetLastError());
+      CUDA_CHECK(cudaEventRecord(L.done, L.stream));
+      L.busy = true;
+      R.launched += grid;
+      R.last_launch = now;
+      S.stats.launches++;
+      break;
     }
   }
 }
@@ -1537,7 +1721,12 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     sqsg_server_options opt{};
     if (options) opt = *options;
     if (opt.device < 0 || opt.device >= ndev) throw std::invalid_argument("invalid device ordinal");
-    if (!opt.arena_bytes) opt.arena_bytes = 4ull << 30;
+    if (!opt.arena_bytes) {  // default: 16 GiB, at most a quarter of the free device memory
+      CUDA_CHECK(cudaSetDevice(opt.device));
+      size_t free_b = 0, total_b = 0;
+      CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+      opt.arena_bytes = std::min<uint64_t>(16ull << 30, free_b / 4);
+    }
     if (!opt.max_jobs) opt.max_jobs = 256;
     if (!opt.default_max_results) opt.default_max_results = 1u << 16;
     auto srv = std::unique_ptr<sqsg_server, sqsg_status (*)(sqsg_server*)>(new sqsg_server, sqsg_server_destroy);
@@ -1552,11 +1741,38 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_ctl), kCtlBytes, cudaHostAllocDefault));
     std::memset(S.h_ctl, 0, kCtlBytes);
     CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_yield), kBuckets * sizeof(uint32_t), cudaHostAllocDefault));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_zero), kLevelSlots * sizeof(LevelSlot), cudaHostAllocDefault));
+    std::memset(S.h_zero, 0, kLevelSlots * sizeof(LevelSlot));
+    CUDA_CHECK(cudaDeviceGetAttribute(&S.n_sm, cudaDevAttrMultiProcessorCount, S.device));
+    if (S.n_sm > kMaxSm || S.n_sm <= kReservedSm) throw unsupported_error("unsupported SM count for the server");
+    CUDA_CHECK(cudaMalloc(&S.d_owner, kMaxSm));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_owner), kMaxSm, cudaHostAllocDefault));
+    std::memset(S.h_owner, kNoOwner, kMaxSm);
+    CUDA_CHECK(cudaMemcpy(S.d_owner, S.h_owner, kMaxSm, cudaMemcpyHostToDevice));
+    // ring b: the largest dynamic shared memory at which 5 - b CTAs fit on an SM
+    configure_kernel(optin);
+    auto fits = [&](size_t smem) {
+      int nb = 0;
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqsg_engine, kBlock, smem));
+      return nb;
+    };
     for (int b = 0; b < kBuckets; ++b) {
       Ring& R = S.rings[b];
-      R.smem = kBucketSmem[b] ? std::min(kBucketSmem[b], optin) : optin;
-      configure_kernel(R.smem);
-      R.full_grid = launch_grid(S.device, R.smem, 1u << 30);
+      const int want = kBuckets - b;
+      size_t lo = 0, hi = optin;  // largest smem in [0, optin] with fits(smem) >= want
+      if (fits(hi) >= want) {
+        lo = hi;
+      } else {
+        while (hi - lo > 16) {
+          const size_t mid = (lo + hi) / 2 / 16 * 16;
+          if (fits(mid) >= want)
+            lo = mid;
+          else
+            hi = mid;
+        }
+      }
+      R.smem = lo;
+      R.per_sm = static_cast<uint32_t>(std::max(1, fits(lo)));
       for (auto& L : R.ls) {
         CUDA_CHECK(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
         CUDA_CHECK(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
@@ -1565,6 +1781,10 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
       QueueCtl q{};
       q.capacity = static_cast<unsigned int>(kRingCap);
       q.idle_limit = kIdlePolls;
+      q.ring = static_cast<unsigned int>(b);
+      q.n_owner = static_cast<unsigned int>(S.n_sm);
+      q.owner = S.d_owner;
+      q.alive = S.d_alive(b);
       CUDA_CHECK(cudaMemcpy(S.q(b), &q, sizeof(q), cudaMemcpyHostToDevice));
     }
     CUDA_CHECK(cudaMalloc(&S.arena, S.opt.arena_bytes));
@@ -1604,8 +1824,11 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
       }
     J->user_capacity = job->max_results != 0;
     J->capacity = job->max_results ? job->max_results : S.opt.default_max_results;
-    make_tiles(J->pj, 0, J->tiles);
+    for (uint32_t p = 0; p < job->n_sublattices; ++p) J->pairs += job->sublattices[p].n_pairs;
+    make_tiles(J->pj, 0, J->tiles, std::max<uint64_t>(1, kTilePairs / std::max<uint64_t>(1, J->pairs)));
     if (J->tiles.size() > kRingCap) throw unsupported_error("the job has more tiles than the ring holds");
+    J->cum.assign(J->tiles.size() + 1, 0);
+    for (size_t k = 0; k < J->tiles.size(); ++k) J->cum[k + 1] = J->cum[k] + J->tiles[k].count;
     if (job_footprint(*J) > S.opt.arena_bytes)
       throw std::length_error("the job's device footprint exceeds the server's arena; lower max_results");
     std::lock_guard<std::mutex> l(S.m);
@@ -1683,6 +1906,10 @@ sqsg_status sqsg_server_destroy(sqsg_server* server) {
   cudaSetDevice(S.device);
   // every CTA leaves at its next claim: no tile is started after this
   if (S.d_ctl && S.h_yield && S.copy) {
+    if (S.d_owner && S.h_owner) {
+      std::memset(S.h_owner, kNoOwner, kMaxSm);
+      cudaMemcpyAsync(S.d_owner, S.h_owner, kMaxSm, cudaMemcpyHostToDevice, S.copy);
+    }
     for (int b = 0; b < kBuckets; ++b) {
       S.h_yield[b] = ~0u;
       cudaMemcpyAsync(&S.q(b)->yield, &S.h_yield[b], sizeof(uint32_t), cudaMemcpyHostToDevice, S.copy);
@@ -1707,6 +1934,9 @@ sqsg_status sqsg_server_destroy(sqsg_server* server) {
   if (S.d_ctl) cudaFree(S.d_ctl);
   if (S.h_ctl) cudaFreeHost(S.h_ctl);
   if (S.h_yield) cudaFreeHost(S.h_yield);
+  if (S.h_zero) cudaFreeHost(S.h_zero);
+  if (S.d_owner) cudaFree(S.d_owner);
+  if (S.h_owner) cudaFreeHost(S.h_owner);
   if (S.h_done) cudaFreeHost(S.h_done);
   delete server;
   return SQSG_OK;

@@ -11,8 +11,32 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 
 namespace sqsg {
+
+// Order-preserving map of doubles onto unsigned 64-bit integers (for atomicMin).
+__host__ __device__ __forceinline__ unsigned long long ord_bits(double x) {
+#ifdef __CUDA_ARCH__
+  unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+#else
+  unsigned long long b;
+  std::memcpy(&b, &x, 8);
+#endif
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
+  unsigned long long b = (u >> 63) ? (u & 0x7fffffffffffffffull) : ~u;
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(static_cast<long long>(b));
+#else
+  double x;
+  std::memcpy(&x, &b, 8);
+  return x;
+#endif
+}
+
 
 constexpr int kBlock = 128;       // threads per CTA (each owns one configuration)
 constexpr int kMinBlocks = 5;     // CTAs per SM the register budget must allow (<= 102 registers)
@@ -118,9 +142,12 @@ struct Tile {
 //  list mode (capacity == 0): tiles[0, n_tiles) are fixed; CTAs take them with atomicAdd on head.
 //  live mode (capacity > 0): tiles is a ring the host appends to; the host's copy stream raises tail
 //  after the tiles (and their jobs' descriptors) are in place, CTAs claim with atomicCAS on head and
-//  leave after idle_limit empty polls (the host relaunches when new work arrives). Between tiles a
-//  CTA that finds yield > 0 takes one unit of it and leaves: the host shrinks a ring's share of the
-//  GPU by writing yield, and counts resident-or-queued CTAs as (launched - exited).
+//  leave after idle_limit empty polls (the host relaunches when new work arrives). With an owner
+//  table, a CTA works only on an SM that the table gives to its ring and leaves (at start or
+//  between tiles) once the SM belongs to another ring: the host partitions the SMs between rings
+//  of different shared-memory sizes instead of letting their CTAs fragment every SM. alive[sm]
+//  counts this ring's working CTAs per SM. A CTA that finds yield > 0 between tiles takes one
+//  unit of it and leaves. launched - exited counts a ring's CTAs not yet gone.
 struct QueueCtl {
   unsigned long long head;
   unsigned long long tail;
@@ -128,6 +155,11 @@ struct QueueCtl {
   unsigned int idle_limit;
   unsigned int yield;
   unsigned int exited;
+  unsigned int ring;
+  unsigned int n_owner;                  // entries in owner[] (0: no owner table)
+  const volatile unsigned char* owner;   // owner ring of each SM
+  unsigned int* alive;                   // working CTAs of this ring per SM
+  unsigned long long reserved;
 };
 
 }  // namespace sqsg

@@ -1,8 +1,9 @@
 // Device side of the SQS engine (included once, by engine.cu).
 //
 // Per configuration a thread
-//   1. (random mode) Fisher-Yates-shuffles every window of every part with Philox4x32-10 draws and
-//      the reference's bounded draw p = (x * i) >> 32 (include/sqsgen/core/shuffle.h:28-50);
+//   1. (random mode) Fisher-Yates-shuffles every window of every part of the packed initial
+//      arrangement with Philox4x32-10 draws (key = seed, counter = (draw block, 0, configuration id,
+//      part)) and the reference's bounded draw p = (x * i) >> 32 (include/sqsgen/core/shuffle.h:28-50);
 //   2. counts ordered bonds (s, species[i], species[j]) over the part's pairs (optimization.h:74-77);
 //   3. evaluates the objective in T with the reference's loop order and no FMA contraction
 //      (optimization.h:79-103), summing parts left to right from T(0) (sqs.h:417-418, fold.h:51-53);
@@ -37,27 +38,6 @@ template <> struct FP<float> {
   static __device__ __forceinline__ float maxv() { return FLT_MAX; }
 };
 
-// Order-preserving map of doubles onto unsigned 64-bit integers (for atomicMin).
-__host__ __device__ __forceinline__ unsigned long long ord_bits(double x) {
-#ifdef __CUDA_ARCH__
-  unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
-#else
-  unsigned long long b;
-  std::memcpy(&b, &x, 8);
-#endif
-  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
-}
-
-__host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
-  unsigned long long b = (u >> 63) ? (u & 0x7fffffffffffffffull) : ~u;
-#ifdef __CUDA_ARCH__
-  return __longlong_as_double(static_cast<long long>(b));
-#else
-  double x;
-  std::memcpy(&x, &b, 8);
-  return x;
-#endif
-}
 
 // Byte offset of site x inside a lane's species column: words of four sites are interleaved across
 // the kBlock lanes, so both a uniform site (bond counting) and per-lane random sites (shuffling) hit
@@ -490,9 +470,9 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
   const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
   const uint64_t max_count = base + (rem ? 1 : 0);
   const bool systematic = J.mode == 1;
-  // random mode: a chain is named by the index of its first configuration, so ids are unique for
-  // any split of the job into tiles or devices
-  const unsigned long long chain = tile.start + my_off;
+  // random mode: configuration id is the Philox Fisher-Yates shuffle, with counter id, of the
+  // packed initial arrangement; it depends on nothing but (seed, id), so any split of the job into
+  // tiles, launches or devices evaluates the same configurations
   const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
 
   for (uint32_t p = 0; p < J.n_parts; ++p) init_column(smem, J.parts[p], t);
@@ -512,7 +492,10 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
     if (active) {
       for (uint32_t p = 0; p < J.n_parts; ++p) {
         const PartDesc& P = J.parts[p];
-        if (!systematic) shuffle_part(smem, P, t, static_cast<uint32_t>(it), chain, p, k0, k1);
+        if (!systematic) {
+          if (it > 0) init_column(smem, P, t);
+          shuffle_part(smem, P, t, 0u, tile.start + my_off + it, p, k0, k1);
+        }
         count_part<KW>(smem, P, t);
         const T o = objective_part<T>(smem, P, t);
         total = p == 0 ? o : F::add(total, o);
@@ -619,7 +602,6 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
   const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
   const uint64_t max_count = base + (rem ? 1 : 0);
   const bool systematic = J.mode == 1;
-  const unsigned long long chain = tile.start + my_off;
   const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
   const uint8_t* part = part_base(smem, P);
   const uint32_t N = P.n_sites, S = P.n_shells;
@@ -629,9 +611,10 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
   const T* w = f + 4 * S;
   const T* tg = w + 4 * S;
   const uint32_t* win = reinterpret_cast<const uint32_t*>(part + P.win_off);
-  V v = 0;
+  V v0 = 0;  // the packed initial arrangement
   for (uint32_t x = 0; x < N; ++x)
-    if (part[P.species_off + x]) v |= V(1) << (N - 1 - x);
+    if (part[P.species_off + x]) v0 |= V(1) << (N - 1 - x);
+  V v = v0;
   uint32_t wn = 0, wshift = 0;
   V wmask = 0;
   if (systematic) {
@@ -664,14 +647,16 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
     T total = T(0);
     if (active) {
       if (!systematic) {  // core/shuffle.h:39-50 on bits, same Philox words as the general path
-        const uint32_t c_lo = static_cast<uint32_t>(chain), c_hi = static_cast<uint32_t>(chain >> 32) << 8;
+        const uint64_t cid = tile.start + my_off + it;
+        const uint32_t c_lo = static_cast<uint32_t>(cid), c_hi = static_cast<uint32_t>(cid >> 32) << 8;
         uint32_t blk = 0;
+        v = v0;
         for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
           const uint32_t lo = win[2 * wi];
           uint32_t i = win[2 * wi + 1] - lo;
           const uint32_t top = N - 1 - lo;  // bit of the window's first site
           while (i > 1) {
-            const philox_ctr r = philox4x32_10(philox_ctr{blk++, static_cast<uint32_t>(it), c_lo, c_hi}, k0, k1);
+            const philox_ctr r = philox4x32_10(philox_ctr{blk++, 0u, c_lo, c_hi}, k0, k1);
             const uint32_t xs[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -720,9 +705,22 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
 constexpr unsigned long long kNoTile = ~0ull;
 
 // Live mode: claim the next published ring entry, waiting (bounded) for the host to publish more.
-__device__ __forceinline__ unsigned long long claim_live(QueueCtl* q, const volatile int32_t* cancel) {
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t id;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(id));
+  return id;
+}
+
+// Live mode: may this CTA work on its SM for its ring?
+__device__ __forceinline__ bool owns_sm(const QueueCtl* q, uint32_t smid) {
+  if (q->n_owner == 0) return true;
+  return smid < q->n_owner && q->owner[smid] == q->ring;
+}
+
+__device__ __forceinline__ unsigned long long claim_live(QueueCtl* q, const volatile int32_t* cancel, uint32_t smid) {
   uint32_t idle = 0;
   for (;;) {
+    if (!owns_sm(q, smid)) return kNoTile;  // the SM went to another ring
     // a pending yield unit ends this CTA (each loop round takes one unit or sees another CTA take it)
     uint32_t y = *reinterpret_cast<volatile unsigned int*>(&q->yield);
     while (y != 0) {
@@ -769,11 +767,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   uint32_t phase = 0;
   WarpState ws;
   ws.reset();
+  const uint32_t smid = sm_id();
+  bool counted = false;  // thread 0: this CTA is in alive[smid]
   if (threadIdx.x == 0) {
-    if (live)
-      s_tile = claim_live(q, cancel);
-    else
+    if (live) {
+      s_tile = kNoTile;
+      if (owns_sm(q, smid)) {  // resident on one of its ring's SMs: counted while it stays
+        if (q->alive && smid < q->n_owner) {
+          atomicAdd(&q->alive[smid], 1u);
+          counted = true;
+        }
+        s_tile = claim_live(q, cancel, smid);
+      }
+    } else {
       s_tile = (cancel && *cancel) ? kNoTile : atomicAdd(&q->head, 1ull);
+    }
   }
   for (;;) {
     __syncthreads();  // s_tile visible; every thread is done with the previous tile
@@ -854,14 +862,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
           __threadfence_system();
           done[tile.job] = tile.gen;
         }
-        s_tile = claim_live(q, cancel);
+        s_tile = claim_live(q, cancel, smid);
       } else {
         s_tile = next;
       }
     }
   }
   if (cur >= 0 && !live) flush_levels(ctab, sj);
-  if (live && threadIdx.x == 0) atomicAdd(&q->exited, 1u);
+  if (live && threadIdx.x == 0) {
+    if (counted) atomicAdd(&q->alive[smid], ~0u);
+    atomicAdd(&q->exited, 1u);
+  }
 }
 
 }  // namespace sqsg

@@ -1,0 +1,53 @@
+// Result-set selection on the device: from a job's candidate records to the reference's result
+// set (every distinct configuration whose objective is one of the keep+1 best distinct objectives,
+// ordered by objective then id, at most max_results_per_objective+1 per objective).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace sqsg {
+
+// Where the fields of one candidate record live (offsets in bytes inside a record).
+struct RecordLayout {
+  uint32_t record_bytes = 0;
+  uint32_t tsz = 8;  // sizeof(T)
+  uint32_t n_parts = 1;
+  uint32_t obj_off[kMaxParts] = {};
+  uint32_t species_off[kMaxParts] = {};
+  uint32_t n_sites[kMaxParts] = {};
+  uint32_t sro_off[kMaxParts] = {};
+  uint32_t sro_bytes[kMaxParts] = {};
+};
+
+struct SelectedSet {
+  uint64_t count = 0;
+  std::vector<uint8_t> objective, sub_objective, species, sro;  // raw T bytes / species bytes
+  std::vector<uint64_t> id;
+};
+
+// Grow-only device scratch for select_on_device, bound to the stream it was last used on.
+struct SelectScratch {
+  void* buf[16] = {};
+  size_t size[16] = {};
+  cudaStream_t stream = nullptr;
+  ~SelectScratch() { release(); }
+  void* get(int slot, size_t bytes);
+  // Frees every buffer on its stream and waits for it; call before that stream is destroyed.
+  void release();
+};
+
+// Selects the records whose objective equals one of `levels` (the keep+1 smallest distinct
+// objectives, exact) from n device-resident records. Random runs (dedup) keep, among equal species,
+// the record with the smallest id. Returns false without doing anything when the ids do not leave
+// room for the level index in a 64-bit sort key (id_limit >= 2^58); the caller then selects on
+// the host.
+bool select_on_device(SelectScratch& scratch, cudaStream_t stream, const RecordLayout& layout,
+                      const uint8_t* d_records, uint64_t n, const std::vector<double>& levels, bool dedup,
+                      int64_t max_per_objective, uint64_t id_limit, SelectedSet& out);
+
+}  // namespace sqsg

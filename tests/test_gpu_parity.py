@@ -259,6 +259,37 @@ def test_random_records_bit_exact_and_deduplicated():
     assert len(distinct) == 11
 
 
+@pytest.mark.parametrize("prec,keep,cap", [("double", 3, None), ("double", 10, 7), ("single", 5, 2)])
+def test_random_result_set_from_full_trace(prec, keep, cap):
+    """Every evaluation of a degenerate random run is traced; the result set must equal the rule
+    restated here on the trace: the keep+1 smallest distinct objectives, one record per distinct
+    configuration (the smallest id), ordered by objective then id, at most cap+1 per objective."""
+    cfg = cases.fcc32(prec, iterations=120000, seed=11, keep=keep)
+    if cap is not None:
+        cfg["max_results_per_objective"] = cap
+    _, d, _, sp, _, ob, ids = cases.trace(cfg, 120000)
+    assert len(ob) == 120000
+    levels = sorted(set(ob.tolist()))[: keep + 1]
+    lset = set(levels)
+    order = sorted((float(ob[k]), int(ids[k]), k) for k in range(len(ob)) if float(ob[k]) in lset)
+    seen, per, expect = set(), collections.Counter(), []
+    for o, i, k in order:
+        key = sp[k].tobytes()
+        if key in seen:
+            continue
+        seen.add(key)
+        if cap is not None and per[o] > cap:
+            continue
+        per[o] += 1
+        expect.append((o, i, key))
+    _, _, recs, lv, info = native_run(cfg)
+    got = [(float(recs["objective"][k]), int(recs["id"][k]), recs["species"][k].tobytes())
+           for k in range(len(recs["objective"]))]
+    assert not info["truncated"] and info["levels_exact"]
+    assert [v for v, _, _ in lv] == levels
+    assert got == expect
+
+
 def test_split_records_bit_exact():
     c, d, recs, levels, info = native_run(cases.rocksalt_split("double", iterations=50000, seed=9))
     n = len(recs["objective"])
@@ -325,45 +356,39 @@ def test_fcc32_systematic_full_space_levels(prec):
 
 
 # --------------------------------------------------------------------------- RNG stream and fast path
-def _chain_starts(total):
-    """Chain start indices of the guided tile decomposition (csrc/tiles.h): each tile takes about
-    1/2048 of what is left, at least `floor` configurations per thread, 128 threads per tile."""
-    floor = max(1, min(16, total // (128 * 8192)))
-    starts = []
-    done = 0
-    while done < total:
-        left = total - done
-        cpt = min(max(-(-left // (128 * 2048)), floor), 1 << 16)
-        c = min(cpt * 128, left)
-        base, rem = divmod(c, 128)
-        for t in range(128):
-            n = base + (1 if t < rem else 0)
-            if n:
-                starts.append((done + t * base + min(t, rem), n))
-        done += c
-    return starts
-
-
 @pytest.mark.parametrize("composition", [{"Ti": 16, "Al": 16}, {"Ti": 11, "Al": 11, "Nb": 10}],
                          ids=["binary_fast_path", "ternary_general_path"])
 def test_random_stream_is_philox_fisher_yates(composition):
-    """Configuration g is the (g - c)-th Philox Fisher-Yates shuffle of the chain starting at c."""
+    """Configuration g is the Philox Fisher-Yates shuffle, with counter g, of the packed initial
+    arrangement: it depends on (seed, g) alone, not on tiles, launches or devices."""
     import philox_ref
 
     total = 2_097_153
     cfg = cases.fcc32("double", composition=composition, iterations=total, seed=0x1234_5678_9ABC)
     c, d, pack, sp, bd, ob, ids = cases.trace(cfg, total)
     assert np.array_equal(ids, np.arange(total, dtype=np.uint64))
-    starts = _chain_starts(total)
     windows = [tuple(w) for w in d[0].windows.tolist()]
     rng = np.random.default_rng(0)
-    for k in rng.choice(len(starts), size=48, replace=False):
-        start, n = starts[k]
+    for g in sorted(set(rng.choice(total, size=400, replace=False).tolist()) | {0, 1, total - 1}):
         conf = d[0].species_packed.tolist()
-        for it in range(n):
-            philox_ref.shuffle(conf, windows, cfg["seed"], start, it)
-            assert conf == sp[start + it].tolist(), (start, it)
+        philox_ref.shuffle(conf, windows, cfg["seed"], g, 0)
+        assert conf == sp[g].tolist(), g
     assert cases.trace_mismatches(d, sp[:1500], bd[:1500], ob[:1500], "double") == []
+
+
+def test_random_results_do_not_depend_on_the_split():
+    """Three contiguous shares of a seeded random job (as on three GPUs) evaluate exactly the
+    configurations of the whole job: merged levels equal the whole job's levels."""
+    from sqsgenerator_b200.shard import merge_levels, shard_range
+
+    cfg = cases.fcc32("double", iterations=3_000_001, seed=77, pair_weights=None)
+    _, _, _, whole, _ = native_run(cfg)
+    parts = []
+    for r in range(3):
+        first, count = shard_range(3_000_001, 3, r)
+        _, _, _, lv, _ = native_run(cfg, range_first=first, range_count=count)
+        parts.append(lv)
+    assert merge_levels(parts, 10) == whole
 
 
 def test_fast_path_64_sites():
