@@ -71,6 +71,12 @@ template <class T> static void copy_cube(std::vector<uint8_t>& blob, size_t off,
 
 // Pair stream of a part: for each shell s and site i (ascending) a header word (s | cnt << 8), the
 // byte offset of i in a species column, and cnt byte offsets of its neighbours j > i in shell s.
+// The grouped pair stream of one part: for each (shell s, site i) the sites j > i of its pairs, in
+// groups of at most kMaxGroup. Narrow form (every column offset below 2^16, i.e. N <= 512): one
+// header word  ioff | s << 16 | cnt << 24  and the cnt column offsets as 16-bit halves, two per
+// word. Wide form: header words  s | cnt << 8  and  ioff, then one word per offset.
+static bool narrow_stream(uint32_t n_sites) { return host_site_off(n_sites ? n_sites - 1 : 0) < 0x10000u; }
+
 static std::vector<uint32_t> build_stream(const sqsg_sublattice& sl) {
   const uint32_t N = sl.n_sites, S = sl.n_shells, P = sl.n_pairs;
   std::vector<std::vector<uint32_t>> by(static_cast<size_t>(S) * N);
@@ -87,6 +93,7 @@ static std::vector<uint32_t> build_stream(const sqsg_sublattice& sl) {
   for (uint32_t s = 0; s < S; ++s)
     if (per_shell[s] > 0xffffu)
       throw unsupported_error("a shell holds more than 65535 pairs; the 16-bit bond counters cannot hold it");
+  const bool narrow = narrow_stream(N);
   std::vector<uint32_t> st;
   st.reserve(P + 2 * static_cast<size_t>(S) * N);
   for (uint32_t s = 0; s < S; ++s)
@@ -95,9 +102,18 @@ static std::vector<uint32_t> build_stream(const sqsg_sublattice& sl) {
       std::sort(js.begin(), js.end());
       for (size_t b = 0; b < js.size(); b += kMaxGroup) {
         uint32_t cnt = static_cast<uint32_t>(std::min<size_t>(kMaxGroup, js.size() - b));
-        st.push_back(s | (cnt << 8));
-        st.push_back(host_site_off(i));
-        for (uint32_t e = 0; e < cnt; ++e) st.push_back(host_site_off(js[b + e]));
+        if (narrow) {
+          st.push_back(host_site_off(i) | (s << 16) | (cnt << 24));
+          for (uint32_t e = 0; e < cnt; e += 2) {
+            const uint32_t lo = host_site_off(js[b + e]);
+            const uint32_t hi = e + 1 < cnt ? host_site_off(js[b + e + 1]) : 0u;
+            st.push_back(lo | (hi << 16));
+          }
+        } else {
+          st.push_back(s | (cnt << 8));
+          st.push_back(host_site_off(i));
+          for (uint32_t e = 0; e < cnt; ++e) st.push_back(host_site_off(js[b + e]));
+        }
       }
     }
   return st;
@@ -187,6 +203,7 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     if (sl.n_species > 4) d.kw = 2;
     streams[p] = build_stream(sl);
     P.stream_words = static_cast<uint32_t>(streams[p].size());
+    P.stream_narrow = narrow_stream(sl.n_sites) ? 1u : 0u;
     const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
     // binary fast path data: per (shell, site) mask of the neighbours j > i (bit N-1-j)
     const bool k2 = job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64;
@@ -414,6 +431,13 @@ static int device_sm_count(int dev) {
   return n;
 }
 
+using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, const volatile int32_t*,
+                              unsigned long long*, volatile uint32_t*);
+
+// The general path runs in sqsg_engine_wide (128 registers); a launch whose jobs all take the binary
+// bit-mask path runs in sqsg_engine (96 registers, 5 CTAs per SM).
+static EngineKernel engine_for(bool all_bitmask) { return all_bitmask ? sqsg_engine : sqsg_engine_wide; }
+
 static void configure_kernel(size_t smem) {
   static std::mutex m;
   static size_t configured = 0;
@@ -421,14 +445,16 @@ static void configure_kernel(size_t smem) {
   if (smem > configured) {
     CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
+    CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
     configured = smem;
   }
 }
 
-static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles) {
+static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel kernel = sqsg_engine) {
   configure_kernel(smem);
   int per_sm = 0;
-  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sqsg_engine, kBlock, smem));
+  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem));
   if (per_sm <= 0) throw unsupported_error("the job needs more shared memory than one SM offers");
   size_t grid = static_cast<size_t>(per_sm) * device_sm_count(dev);
   return static_cast<uint32_t>(std::max<size_t>(1, std::min(grid, n_tiles)));
@@ -437,9 +463,10 @@ static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles) {
 static size_t max_dynamic_smem(int dev) {
   int v = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes attr{};
-  CUDA_CHECK(cudaFuncGetAttributes(&attr, sqsg_engine));
-  return static_cast<size_t>(v) - attr.sharedSizeBytes;
+  cudaFuncAttributes a{}, b{};
+  CUDA_CHECK(cudaFuncGetAttributes(&a, sqsg_engine));
+  CUDA_CHECK(cudaFuncGetAttributes(&b, sqsg_engine_wide));
+  return static_cast<size_t>(v) - std::max(a.sharedSizeBytes, b.sharedSizeBytes);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -819,10 +846,13 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     CUDA_CHECK(cudaMemsetAsync(ws->status.p, 0, sizeof(unsigned long long), ws->stream));
     ws->ctrl_host[0] = 0;
 
-    const uint32_t grid = launch_grid(device, smem, tiles.size());
+    bool all_bitmask = true;
+    for (size_t j = 0; j < nj; ++j) all_bitmask = all_bitmask && pjs[j].desc.k2 != 0;
+    const EngineKernel kernel = engine_for(all_bitmask);
+    const uint32_t grid = launch_grid(device, smem, tiles.size(), kernel);
     CUDA_CHECK(cudaEventRecord(ws->ev_start, ws->stream));
     if (!tiles.empty()) {
-      sqsg_engine<<<grid, kBlock, smem, ws->stream>>>(
+      kernel<<<grid, kBlock, smem, ws->stream>>>(
           static_cast<const JobDesc*>(ws->jobs.p), static_cast<const Tile*>(ws->tiles.p),
           static_cast<uint32_t>(tiles.size()), static_cast<QueueCtl*>(ws->queue.p), ws->ctrl_dev,
           static_cast<unsigned long long*>(ws->status.p), nullptr);
@@ -1000,8 +1030,9 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
 // that finishes a job's last tile marks the job's slot done in host-mapped memory; the worker then
 // downloads its records and levels, selects the result set and wakes the waiting caller. A job's
 // result does not depend on what else runs: its tiles and Philox counters depend only on the job.
-// One ring per occupancy level of sqsg_engine (5, 4, 3, 2, 1 CTAs per SM): a job goes to the ring
-// with the largest shared-memory size it fits, i.e. the highest occupancy its data allow.
+// One ring per occupancy level: ring 0 runs sqsg_engine at 5 CTAs per SM and takes binary bit-mask
+// jobs; rings 1-4 run sqsg_engine_wide at 4, 3, 2, 1 CTAs per SM. A job goes to the ring with the
+// largest shared-memory size it fits, i.e. the highest occupancy its data allow.
 constexpr int kBuckets = 5;
 constexpr int kMaxSm = 256;
 constexpr uint64_t kRingCap = 1u << 20;
@@ -1041,6 +1072,7 @@ struct LaunchSlot {
 // One ring of tiles per shared-memory class; launches of sqsg_engine serve a ring on the SMs that
 // the owner table gives it.
 struct Ring {
+  EngineKernel kernel = nullptr;  // ring 0: sqsg_engine (bit-mask jobs); others: sqsg_engine_wide
   size_t smem = 0;
   uint32_t per_sm = 1;        // resident CTAs per SM at this shared-memory size
   uint64_t published = 0;     // tiles appended so far (the ring's tail)
@@ -1436,7 +1468,7 @@ static void schedule(ServerState& S) {
     for (auto& L : R.ls) {
       if (L.busy) continue;
       const uint32_t grid = R.per_sm * static_cast<uint32_t>(S.n_sm);
-      sqsg_engine<<<grid, kBlock, R.smem, L.stream>>>(
+      R.kernel<<<grid, kBlock, R.smem, L.stream>>>(
           S.d_jobs, S.d_ring[b], 0, S.q(b), nullptr,
           reinterpret_cast<unsigned long long*>(S.d_ctl + kBuckets * sizeof(QueueCtl)), S.d_done);
       CUDA_CHECK(cudaGetLastError());
@@ -1749,15 +1781,16 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_owner), kMaxSm, cudaHostAllocDefault));
     std::memset(S.h_owner, kNoOwner, kMaxSm);
     CUDA_CHECK(cudaMemcpy(S.d_owner, S.h_owner, kMaxSm, cudaMemcpyHostToDevice));
-    // ring b: the largest dynamic shared memory at which 5 - b CTAs fit on an SM
+    // ring b: the largest dynamic shared memory at which 5 - b CTAs of its kernel fit on an SM
     configure_kernel(optin);
-    auto fits = [&](size_t smem) {
-      int nb = 0;
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqsg_engine, kBlock, smem));
-      return nb;
-    };
     for (int b = 0; b < kBuckets; ++b) {
       Ring& R = S.rings[b];
+      R.kernel = b == 0 ? sqsg_engine : sqsg_engine_wide;
+      auto fits = [&](size_t smem) {
+        int nb = 0;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, R.kernel, kBlock, smem));
+        return nb;
+      };
       const int want = kBuckets - b;
       size_t lo = 0, hi = optin;  // largest smem in [0, optin] with fits(smem) >= want
       if (fits(hi) >= want) {
@@ -1817,7 +1850,7 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
     if (need > S.rings[kBuckets - 1].smem)
       throw unsupported_error("the job needs more shared memory per CTA than this device offers");
     J->bucket = kBuckets - 1;
-    for (int b = 0; b < kBuckets; ++b)
+    for (int b = J->pj.desc.k2 ? 0 : 1; b < kBuckets; ++b)  // general-path jobs use the wide kernel
       if (need <= S.rings[b].smem) {
         J->bucket = b;
         break;

@@ -39,7 +39,8 @@ __host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
 
 
 constexpr int kBlock = 128;       // threads per CTA (each owns one configuration)
-constexpr int kMinBlocks = 5;     // CTAs per SM the register budget must allow (<= 102 registers)
+constexpr int kMinBlocks = 5;     // sqsg_engine: CTAs per SM the register budget must allow (<= 102 registers)
+constexpr int kMinBlocksWide = 4; // sqsg_engine_wide (general path): 128 registers, no spills in the pair loop
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
 constexpr int kMaxSpecies = 8;    // K per part handled by the packed-row counter
@@ -77,6 +78,7 @@ struct PartDesc {
   uint32_t n_sites, n_species, n_shells, n_windows;
   uint32_t hw;            // histogram words per (shell, species) row: ceil(K/2) 16-bit fields pairs
   uint32_t stream_words;  // words of the grouped pair stream
+  uint32_t stream_narrow; // 1: 16-bit j offsets, two per word, one header word per group (N <= 512)
   uint32_t blob_off;      // staged section: offset in the job blob (16-byte aligned)
   uint32_t static_bytes;  // staged section size (multiple of 16)
   uint32_t smem_off;      // part base in dynamic shared memory

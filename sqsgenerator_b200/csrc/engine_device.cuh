@@ -103,6 +103,43 @@ template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, cons
   const uint32_t nh = P.n_shells * K * hw;
   for (uint32_t w = 0; w < nh; ++w) hist[w * kBlock] = 0;
   uint32_t pos = 0;
+  if (P.stream_narrow) {
+    // one header word per group, then two 16-bit column offsets per word
+    while (pos < words) {
+      const uint32_t hdr = st[pos];
+      const uint32_t s = (hdr >> 16) & 0xffu, cnt = hdr >> 24;
+      const uint32_t ci = col[hdr & 0xffffu] >> 3;
+      const uint32_t* js = st + pos + 1;
+      const uint32_t pairs = cnt >> 1;
+      uint32_t* h = hist + ((s * K + ci) * hw) * kBlock;
+      if (KW == 1) {
+        uint32_t row = 0;
+#pragma unroll 4
+        for (uint32_t e = 0; e < pairs; ++e) {
+          const uint32_t w2 = js[e];
+          row += (1u << col[w2 & 0xffffu]) + (1u << col[w2 >> 16]);
+        }
+        if (cnt & 1u) row += 1u << col[js[pairs] & 0xffffu];
+        h[0] += __byte_perm(row, 0, 0x4140);
+        if (hw > 1) h[kBlock] += __byte_perm(row, 0, 0x4342);
+      } else {
+        unsigned long long row = 0;
+#pragma unroll 4
+        for (uint32_t e = 0; e < pairs; ++e) {
+          const uint32_t w2 = js[e];
+          row += (1ull << col[w2 & 0xffffu]) + (1ull << col[w2 >> 16]);
+        }
+        if (cnt & 1u) row += 1ull << col[js[pairs] & 0xffffu];
+        const uint32_t lo = static_cast<uint32_t>(row), hi = static_cast<uint32_t>(row >> 32);
+        h[0] += __byte_perm(lo, 0, 0x4140);
+        if (hw > 1) h[kBlock] += __byte_perm(lo, 0, 0x4342);
+        if (hw > 2) h[2 * kBlock] += __byte_perm(hi, 0, 0x4140);
+        if (hw > 3) h[3 * kBlock] += __byte_perm(hi, 0, 0x4342);
+      }
+      pos += 1 + ((cnt + 1) >> 1);
+    }
+    return;
+  }
   while (pos < words) {
     const uint32_t hdr = st[pos];
     const uint32_t ioff = st[pos + 1];
@@ -460,7 +497,7 @@ template <class T> __device__ __forceinline__ T load_threshold(const JobDesc& J)
 }
 
 // ------------------------------------------------------------------------------ one tile
-template <class T, int KW>
+template <class T, int KW, bool SYS>
 __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                       WarpState& ws) {
   using F = FP<T>;
@@ -469,7 +506,7 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
   const uint64_t my_count = base + (static_cast<uint64_t>(t) < rem ? 1 : 0);
   const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
   const uint64_t max_count = base + (rem ? 1 : 0);
-  const bool systematic = J.mode == 1;
+  constexpr bool systematic = SYS;  // J.mode == 1
   // random mode: configuration id is the Philox Fisher-Yates shuffle, with counter id, of the
   // packed initial arrangement; it depends on nothing but (seed, id), so any split of the job into
   // tiles, launches or devices evaluates the same configurations
@@ -591,7 +628,7 @@ __device__ __forceinline__ void k2_materialize(uint8_t* smem, const PartDesc& P,
   }
 }
 
-template <class T, int W>
+template <class T, int W, bool SYS>
 __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                          WarpState& ws) {
   using V = typename Word<W>::type;
@@ -601,7 +638,7 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
   const uint64_t my_count = base + (static_cast<uint64_t>(t) < rem ? 1 : 0);
   const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
   const uint64_t max_count = base + (rem ? 1 : 0);
-  const bool systematic = J.mode == 1;
+  constexpr bool systematic = SYS;  // J.mode == 1
   const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
   const uint8_t* part = part_base(smem, P);
   const uint32_t N = P.n_sites, S = P.n_shells;
@@ -742,19 +779,48 @@ __device__ __forceinline__ unsigned long long claim_live(QueueCtl* q, const vola
   }
 }
 
+// One instantiation per (path, precision, row width, mode): random and systematic loops keep only
+// their own state live.
+template <bool SYS>
+__device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                              WarpState& ws) {
+  if (sj.k2 == 1) {
+    if (sj.prec == 1)
+      run_tile_k2<double, 1, SYS>(sj, smem, ctab, tile, ws);
+    else
+      run_tile_k2<float, 1, SYS>(sj, smem, ctab, tile, ws);
+  } else if (sj.k2 == 2) {
+    if (sj.prec == 1)
+      run_tile_k2<double, 2, SYS>(sj, smem, ctab, tile, ws);
+    else
+      run_tile_k2<float, 2, SYS>(sj, smem, ctab, tile, ws);
+  } else if (sj.prec == 1) {
+    if (sj.kw == 1)
+      run_tile<double, 1, SYS>(sj, smem, ctab, tile, ws);
+    else
+      run_tile<double, 2, SYS>(sj, smem, ctab, tile, ws);
+  } else {
+    if (sj.kw == 1)
+      run_tile<float, 1, SYS>(sj, smem, ctab, tile, ws);
+    else
+      run_tile<float, 2, SYS>(sj, smem, ctab, tile, ws);
+  }
+}
+
 // Tiles are taken from q with one atomic per tile. A CTA stages a job's read-only data (cubes,
 // windows, pair stream, packed species, masks) into shared memory with non-multicast bulk copies
 // whenever its next tile belongs to another job. In live mode every tile ends with a level flush and
 // a decrement of the job's tile count; the CTA that finishes a job's last tile publishes the job's
 // generation in done[slot] (host-mapped memory).
-__global__ void __launch_bounds__(kBlock, kMinBlocks)
-    sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
-                const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
+__device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
+                                            uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
+                                            unsigned long long* status, volatile uint32_t* done) {
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ JobDesc sj;
   __shared__ LevelSlot ctab[kCtaLevelSlots];
   __shared__ unsigned long long s_tile;
   __shared__ uint32_t s_fail;
+  __shared__ uint32_t s_counted;  // live mode: this CTA is counted in alive[its SM]
   __shared__ __align__(8) uint64_t s_bar;
   if (threadIdx.x == 0) {
     mbar_init(&s_bar, 1);
@@ -767,15 +833,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   uint32_t phase = 0;
   WarpState ws;
   ws.reset();
-  const uint32_t smid = sm_id();
-  bool counted = false;  // thread 0: this CTA is in alive[smid]
   if (threadIdx.x == 0) {
+    s_counted = 0;
     if (live) {
+      const uint32_t smid = sm_id();
       s_tile = kNoTile;
       if (owns_sm(q, smid)) {  // resident on one of its ring's SMs: counted while it stays
         if (q->alive && smid < q->n_owner) {
           atomicAdd(&q->alive[smid], 1u);
-          counted = true;
+          s_counted = 1;
         }
         s_tile = claim_live(q, cancel, smid);
       }
@@ -826,27 +892,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
       cur_gen = tile.gen;
       ws.reset();
     }
-    if (sj.k2 == 1) {
-      if (sj.prec == 1)
-        run_tile_k2<double, 1>(sj, smem, ctab, tile, ws);
-      else
-        run_tile_k2<float, 1>(sj, smem, ctab, tile, ws);
-    } else if (sj.k2 == 2) {
-      if (sj.prec == 1)
-        run_tile_k2<double, 2>(sj, smem, ctab, tile, ws);
-      else
-        run_tile_k2<float, 2>(sj, smem, ctab, tile, ws);
-    } else if (sj.prec == 1) {
-      if (sj.kw == 1)
-        run_tile<double, 1>(sj, smem, ctab, tile, ws);
-      else
-        run_tile<double, 2>(sj, smem, ctab, tile, ws);
-    } else {
-      if (sj.kw == 1)
-        run_tile<float, 1>(sj, smem, ctab, tile, ws);
-      else
-        run_tile<float, 2>(sj, smem, ctab, tile, ws);
-    }
+    if (sj.mode == 1)
+      dispatch_tile<true>(sj, smem, ctab, tile, ws);
+    else
+      dispatch_tile<false>(sj, smem, ctab, tile, ws);
     __syncthreads();  // every thread is done with this tile before s_tile changes
     if (live) {
       flush_levels(ctab, sj);
@@ -862,7 +911,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
           __threadfence_system();
           done[tile.job] = tile.gen;
         }
-        s_tile = claim_live(q, cancel, smid);
+        s_tile = claim_live(q, cancel, sm_id());
       } else {
         s_tile = next;
       }
@@ -870,9 +919,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   }
   if (cur >= 0 && !live) flush_levels(ctab, sj);
   if (live && threadIdx.x == 0) {
-    if (counted) atomicAdd(&q->alive[smid], ~0u);
+    if (s_counted) atomicAdd(&q->alive[sm_id()], ~0u);
     atomicAdd(&q->exited, 1u);
   }
+}
+
+// Two register budgets of the same engine: 96 registers (5 CTAs per SM) for the binary bit-mask
+// path, whose state is small and whose shared-memory footprint allows 5 CTAs; 128 registers for the
+// general path, whose pair loop spills at 96 and whose shared memory allows at most 4 CTAs anyway.
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
+    sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
+  engine_body(jobs, tiles, n_tiles, q, cancel, status, done);
+}
+
+__global__ void __launch_bounds__(kBlock, kMinBlocksWide)
+    sqsg_engine_wide(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
+  engine_body(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
 }  // namespace sqsg

@@ -173,6 +173,8 @@ static Err prepare(const sqsg_job& job, JobDesc& d, size_t& blob_size, size_t& n
       if (i == j) NA_FAIL(SQSG_ERR_INVALID_ARGUMENT, "pair with i == j");
     }
     // count the stream words: groups of <= kMaxGroup neighbours per (shell, site)
+    const bool narrow = site_off(N ? N - 1 : 0) < 0x10000u;
+    P.stream_narrow = narrow ? 1u : 0u;
     size_t words = 0;
     for (uint32_t s = 0; s < S; ++s) {
       uint64_t in_shell = 0;
@@ -181,7 +183,11 @@ static Err prepare(const sqsg_job& job, JobDesc& d, size_t& blob_size, size_t& n
         for (uint32_t e = 0; e < sl.n_pairs; ++e)
           if (sl.pairs[3 * e + 2] == s && std::min(sl.pairs[3 * e], sl.pairs[3 * e + 1]) == i) ++cnt;
         in_shell += cnt;
-        words += cnt + 2ull * ((cnt + kMaxGroup - 1) / kMaxGroup);
+        for (uint32_t left = cnt; left > 0;) {  // the same groups as the regular entry point
+          const uint32_t g = std::min<uint32_t>(left, kMaxGroup);
+          words += narrow ? 1ull + (g + 1) / 2 : 2ull + g;
+          left -= g;
+        }
       }
       if (in_shell > 0xffffu) NA_FAIL(SQSG_ERR_UNSUPPORTED, "a shell holds more than 65535 pairs");
     }
@@ -217,13 +223,19 @@ static Err prepare(const sqsg_job& job, JobDesc& d, size_t& blob_size, size_t& n
           if (sl.pairs[3 * e + 2] != s || std::min(a, b) != i) continue;
           if (in_group == 0 || in_group == static_cast<uint32_t>(kMaxGroup)) {
             hdr = w;
-            st[w++] = s;
-            st[w++] = site_off(i);
+            st[w++] = 0;
+            if (!narrow) st[w++] = site_off(i);
             in_group = 0;
           }
-          st[w++] = site_off(std::max(a, b));
+          const uint32_t jo = site_off(std::max(a, b));
+          if (!narrow)
+            st[w++] = jo;
+          else if (in_group % 2 == 0)
+            st[w++] = jo;
+          else
+            st[w - 1] |= jo << 16;
           ++in_group;
-          st[hdr] = s | (in_group << 8);
+          st[hdr] = narrow ? (site_off(i) | (s << 16) | (in_group << 24)) : (s | (in_group << 8));
         }
       }
     for (uint32_t x = 0; x < N; ++x) base[P.species_off + x] = static_cast<unsigned char>(sl.species[x] << 3);
