@@ -1639,9 +1639,38 @@ static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, co
       pjs.push_back(prepare(jobs[j], trace ? trace->capacity : 0));
       srcs.push_back(&jobs[j]);
     }
-    std::vector<Run> runs;
-    execute(pjs, srcs, device, runs, trace);
-    for (uint32_t j = 0; j < n; ++j) out[j] = new sqsg_run{std::move(runs[j])};
+    if (n == 1 || trace) {
+      std::vector<Run> runs;
+      execute(pjs, srcs, device, runs, trace);
+      for (uint32_t j = 0; j < n; ++j) out[j] = new sqsg_run{std::move(runs[j])};
+      return;
+    }
+    // A batch runs as one persistent launch per occupancy class (kernel, CTAs per SM): a launch
+    // takes the largest shared-memory size of its jobs, so mixing small and large jobs in one launch
+    // would run the small ones at the large ones' occupancy.
+    CUDA_CHECK(cudaSetDevice(device));
+    configure_kernel(max_dynamic_smem(device));
+    std::map<std::pair<int, int>, std::vector<uint32_t>> classes;
+    for (uint32_t j = 0; j < n; ++j) {
+      const bool bitmask = pjs[j].desc.k2 != 0;
+      int per_sm = 0;
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_for(bitmask), kBlock,
+                                                               pjs[j].desc.smem_bytes));
+      classes[{bitmask ? 0 : 1, -per_sm}].push_back(j);
+    }
+    std::vector<std::unique_ptr<sqsg_run>> done(n);
+    for (auto& [key, idx] : classes) {
+      std::vector<PreparedJob> g;
+      std::vector<const sqsg_job*> gs;
+      for (uint32_t j : idx) {
+        g.push_back(std::move(pjs[j]));
+        gs.push_back(srcs[j]);
+      }
+      std::vector<Run> runs;
+      execute(g, gs, device, runs, nullptr);
+      for (size_t k = 0; k < idx.size(); ++k) done[idx[k]].reset(new sqsg_run{std::move(runs[k])});
+    }
+    for (uint32_t j = 0; j < n; ++j) out[j] = done[j].release();
   });
 }
 
