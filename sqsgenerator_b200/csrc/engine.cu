@@ -331,15 +331,24 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   return pj;
 }
 
+// A job may have at most this many tiles (about 1.4e14 configurations at full-size tiles).
+constexpr size_t kMaxJobTiles = 1u << 24;
+
 static void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles,
                        uint64_t max_per_thread = 1u << 16) {
+  size_t added = 0;
   for_each_tile(
       pj.range_first, pj.range_count, pj.systematic,
-      [&](Tile t) {
+      [&](Tile t) -> bool {
+        if (++added > kMaxJobTiles) return false;
         t.job = job_index;
         tiles.push_back(t);
+        return true;
       },
       max_per_thread);
+  if (added > kMaxJobTiles)
+    throw unsupported_error("the job has more than " + std::to_string(kMaxJobTiles) +
+                            " tiles; split it with range_first/range_count");
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -420,13 +420,24 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
   unsigned m = __ballot_sync(0xffffffffu, pass);
   if (!m) return;
   const double v_mine = static_cast<double>(total);
-  unsigned mm = m;
-  while (mm) {
-    const int src = __ffs(mm) - 1;
-    mm &= mm - 1;
-    const double v = __shfl_sync(0xffffffffu, v_mine, src);
-    if (v < ws.list_thr) {
-      if (!__any_sync(0xffffffffu, ws.list == v)) {
+  // Only values below the warp's (keep+1)-th entry that are not in its list yet change the list.
+  // Membership: the lower bound of each lane's value in the ascending list (one entry per lane),
+  // found by a five-step shuffle search; then one insertion per distinct new value, lane order.
+  bool fresh = pass && v_mine < ws.list_thr;
+  if (__any_sync(0xffffffffu, fresh)) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const double e = __shfl_sync(0xffffffffu, ws.list, lo + step - 1);
+      if (e < v_mine) lo += step;
+    }
+    const double at = __shfl_sync(0xffffffffu, ws.list, lo);  // every lane takes part in the shuffle
+    fresh = fresh && at != v_mine;
+    unsigned fm = __ballot_sync(0xffffffffu, fresh);
+    while (fm) {
+      const double v = __shfl_sync(0xffffffffu, v_mine, __ffs(fm) - 1);
+      fm &= ~__ballot_sync(0xffffffffu, v_mine == v);  // lanes with the same value: one insertion
+      if (v < ws.list_thr) {
         const int pos = __popc(__ballot_sync(0xffffffffu, ws.list < v));
         const double up = __shfl_up_sync(0xffffffffu, ws.list, 1);
         if (lane == pos)
@@ -454,7 +465,9 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
   const bool keep_it = pass && v_mine <= bound;
   const unsigned km = __ballot_sync(0xffffffffu, keep_it);
   if (!km) return;
-  // objective levels: one shared-memory update per distinct value per warp
+  // objective levels: one shared-memory update per distinct value per warp. The reductions run with
+  // the full warp mask, one distinct value per round (a reduction whose mask differs between the
+  // threads executing it is not allowed).
   {
     const unsigned long long mykey = ord_bits(v_mine);
     const unsigned long long h = mix64(id);

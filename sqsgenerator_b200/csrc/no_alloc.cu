@@ -281,12 +281,13 @@ static Err prepare(const sqsg_job& job, JobDesc& d, size_t& blob_size, size_t& n
   // tiles: the same decomposition as sqsg_optimize (tiles.h)
   n_tiles = 0;
   bool too_many = false;
-  for_each_tile(job.range_first, count, systematic, [&](const Tile& t) {
-    if (n_tiles < kMaxTiles)
-      g_stage_tiles[n_tiles] = t;
-    else
+  for_each_tile(job.range_first, count, systematic, [&](const Tile& t) -> bool {
+    if (n_tiles >= kMaxTiles) {
       too_many = true;
-    ++n_tiles;
+      return false;  // stop at once: a job of 1e18 configurations has ~1e11 tiles
+    }
+    g_stage_tiles[n_tiles++] = t;
+    return true;
   });
   if (too_many) NA_FAIL(SQSG_ERR_CAPACITY, "the job needs more tiles than the static tile list holds");
   return kOk;

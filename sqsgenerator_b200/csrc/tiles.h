@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 #include "engine.cuh"
 
@@ -28,7 +29,11 @@ inline void for_each_tile(uint64_t first, uint64_t count, bool systematic, Emit&
     Tile t{};
     t.count = std::min<uint64_t>(cpt * kBlock, left);
     t.start = first + done + (systematic ? 1 : 0);
-    emit(t);
+    if constexpr (std::is_same_v<decltype(emit(t)), bool>) {
+      if (!emit(t)) return;  // the caller has seen enough tiles
+    } else {
+      emit(t);
+    }
     done += t.count;
   }
 }
