@@ -174,6 +174,7 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   size_t rec = 16, tsp = 0, tbd = 0;
   std::vector<std::vector<uint32_t>> streams(job.n_sublattices);
   std::vector<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>> k2_data;
+  std::vector<std::vector<uint32_t>> k2_nbp_data;
   for (uint32_t p = 0; p < job.n_sublattices; ++p) {
     const sqsg_sublattice& sl = job.sublattices[p];
     PartDesc& P = d.parts[p];
@@ -206,8 +207,8 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     P.stream_narrow = narrow_stream(sl.n_sites) ? 1u : 0u;
     const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
     // binary fast path data: per (shell, site) mask of the neighbours j > i (bit N-1-j)
-    const bool k2 = job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64;
-    std::vector<uint32_t> k2_entries, k2_shells;
+    const bool k2 = job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64 && sl.n_shells <= kK2MaxShells;
+    std::vector<uint32_t> k2_entries, k2_shells, k2_nbp;
     if (k2) {
       const uint32_t N = sl.n_sites;
       std::vector<unsigned long long> nb(static_cast<size_t>(sl.n_shells) * N, 0ull);
@@ -219,6 +220,7 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
         nb[static_cast<size_t>(sh) * N + i] |= 1ull << (N - 1 - j);
         ps[sh]++;
       }
+      std::vector<uint32_t> shell_end(sl.n_shells);
       for (uint32_t sh = 0; sh < sl.n_shells; ++sh) {
         for (uint32_t i = 0; i < N; ++i) {
           const unsigned long long m = nb[static_cast<size_t>(sh) * N + i];
@@ -228,9 +230,45 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
           k2_entries.push_back(N - 1 - i);
           k2_entries.push_back(static_cast<uint32_t>(__builtin_popcountll(m)));
         }
+        shell_end[sh] = static_cast<uint32_t>(k2_entries.size() / 4);
+      }
+      // degree classes: sites grouped by their number of shell-s pairs (either end), so that
+      // n01 + n10 = sum_x b_x deg_s(x) - 2 n11 costs one popcount per class
+      for (uint32_t sh = 0; sh < sl.n_shells; ++sh) {
+        std::vector<uint32_t> deg(N, 0);
+        for (uint32_t i = 0; i < N; ++i) {
+          const unsigned long long m = nb[static_cast<size_t>(sh) * N + i];
+          deg[i] += static_cast<uint32_t>(__builtin_popcountll(m));
+          for (uint32_t j = 0; j < N; ++j)
+            if ((m >> (N - 1 - j)) & 1ull) deg[j]++;
+        }
+        std::map<uint32_t, unsigned long long> classes;
+        for (uint32_t x = 0; x < N; ++x)
+          if (deg[x]) classes[deg[x]] |= 1ull << (N - 1 - x);
+        const uint32_t d0 = static_cast<uint32_t>(k2_entries.size() / 4);
+        for (auto& [dv, m] : classes) {
+          k2_entries.push_back(static_cast<uint32_t>(m));
+          k2_entries.push_back(static_cast<uint32_t>(m >> 32));
+          k2_entries.push_back(dv);
+          k2_entries.push_back(0);
+        }
         k2_shells.push_back(ps[sh]);
+        k2_shells.push_back(shell_end[sh]);
+        k2_shells.push_back(d0);
         k2_shells.push_back(static_cast<uint32_t>(k2_entries.size() / 4));
       }
+      // neighbour masks indexed by the bit position p = N-1-i of site i, for the per-configuration
+      // loop over the set bits of the minority species
+      const uint32_t slots = N <= 32 ? 32 : 64;
+      for (uint32_t sh = 0; sh < sl.n_shells; ++sh)
+        for (uint32_t bp = 0; bp < slots; ++bp) {
+          const unsigned long long m = bp < N ? nb[static_cast<size_t>(sh) * N + (N - 1 - bp)] : 0ull;
+          k2_nbp.push_back(static_cast<uint32_t>(m));
+          if (slots == 64) k2_nbp.push_back(static_cast<uint32_t>(m >> 32));
+        }
+      uint32_t ones = 0;
+      for (uint32_t x = 0; x < N; ++x) ones += sl.species[x] != 0 ? 1u : 0u;
+      P.k2_zeros = 2 * ones > N ? 1u : 0u;
     }
     // staged section layout: cubes | windows | stream | species codes | binary-path masks
     size_t off = 0;
@@ -248,9 +286,13 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
       off = align_up(off + 4 * k2_entries.size(), 16);
       P.k2_shell_off = static_cast<uint32_t>(off);
       off = align_up(off + 4 * k2_shells.size(), 16);
+      P.k2_nbp_off = static_cast<uint32_t>(off);
+      off = align_up(off + 4 * k2_nbp.size(), 16);
       k2_data.emplace_back(std::move(k2_entries), std::move(k2_shells));
+      k2_nbp_data.emplace_back(std::move(k2_nbp));
     } else {
       k2_data.emplace_back();
+      k2_nbp_data.emplace_back();
     }
     P.static_bytes = static_cast<uint32_t>(off);
     P.blob_off = static_cast<uint32_t>(blob_size);
@@ -313,6 +355,8 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     const auto& k2d = k2_data[p];
     if (!k2d.first.empty()) std::memcpy(base + P.k2_off, k2d.first.data(), 4 * k2d.first.size());
     if (!k2d.second.empty()) std::memcpy(base + P.k2_shell_off, k2d.second.data(), 4 * k2d.second.size());
+    if (!k2_nbp_data[p].empty())
+      std::memcpy(base + P.k2_nbp_off, k2_nbp_data[p].data(), 4 * k2_nbp_data[p].size());
   }
   // binary systematic path: binomials C(m, j) for m <= window size, j <= ones in the window, kept in
   // global memory after the staged sections (read through the L1 by the per-thread unrank)

@@ -40,6 +40,7 @@ __host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
 
 constexpr int kBlock = 128;       // threads per CTA (each owns one configuration)
 constexpr int kMinBlocks = 5;     // sqsg_engine: CTAs per SM the register budget must allow (<= 102 registers)
+constexpr int kK2MaxShells = 4;   // shells of the binary bit-mask path (per-shell counters in registers)
 constexpr int kMinBlocksWide = 4; // sqsg_engine_wide (general path): 128 registers, no spills in the pair loop
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
@@ -101,8 +102,10 @@ struct PartDesc {
   // binary fast path (K == 2, N <= 64): per (shell, site) neighbour masks, see run_tile_k2
   uint32_t k2_off;        // entries: uint4 {mask lo, mask hi, site | shell << 8, popcount}
   uint32_t k2_entries;
-  uint32_t k2_shell_off;  // S x (pairs in shell, end of its entries)
+  uint32_t k2_shell_off;  // S x (pairs in shell, end of its entries, degree classes [begin, end))
   uint32_t k2_binom_off;  // blob offset (global, not staged) of C(m, j), m <= window, j <= ones
+  uint32_t k2_nbp_off;    // neighbour masks by bit position: u32 [S][32] (N <= 32) or uint2 [S][64]
+  uint32_t k2_zeros;      // 1: count over the zeros (species 0 is the minority), else over the ones
 };
 
 struct JobDesc {

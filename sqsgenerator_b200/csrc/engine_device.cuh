@@ -611,6 +611,24 @@ __device__ __forceinline__ void k2_counts(const uint4* ent, uint32_t e0, uint32_
   n00 = ps - n11 - n01 - n10;
 }
 
+// popc(NB_s[site of bit bp] & u) from the bit-position table (u32 entries for N <= 32: the lanes'
+// different positions fall in different banks; uint2 entries otherwise).
+template <class V, int W>
+__device__ __forceinline__ uint32_t k2_nbp_count(const uint8_t* tab, int s, int bp, V u) {
+  if (W == 1) {
+    const uint32_t m = reinterpret_cast<const uint32_t*>(tab)[s * 32 + bp];
+    return __popc(static_cast<uint32_t>(u) & m);
+  } else {
+    const uint2 m = reinterpret_cast<const uint2*>(tab)[s * 64 + bp];
+    return Word<W>::pc(u, m.x, m.y);
+  }
+}
+
+// What the objective needs per shell: n11, n01 + n10 and n00. With deg_s(x) the number of shell-s
+// pairs at site x, sum_x b_x deg_s(x) = 2 n11 + n01 + n10 (the degree classes, sites of equal degree
+// as one mask, give it in one popcount per class) and sum_x deg_s(x) = 2 P_s, so one count of the
+// pairs inside the minority species fixes all three.
+
 template <class T>
 __device__ __forceinline__ T k2_term(T obj, uint32_t n, const T* f, const T* w, const T* tg, uint32_t d) {
   using F = FP<T>;
@@ -634,8 +652,8 @@ __device__ __forceinline__ void k2_materialize(uint8_t* smem, const PartDesc& P,
   uint32_t e0 = 0;
   for (uint32_t s = 0; s < P.n_shells; ++s) {
     uint32_t n00, n01, n10, n11;
-    k2_counts<V, W>(ent, e0, sh[2 * s + 1], sh[2 * s], v, n00, n01, n10, n11);
-    e0 = sh[2 * s + 1];
+    k2_counts<V, W>(ent, e0, sh[4 * s + 1], sh[4 * s], v, n00, n01, n10, n11);
+    e0 = sh[4 * s + 1];
     hist[(s * 2 + 0) * kBlock] = n00 | (n01 << 16);
     hist[(s * 2 + 1) * kBlock] = n10 | (n11 << 16);
   }
@@ -720,14 +738,39 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
           }
         }
       }
-      uint32_t e0 = 0;
-      for (uint32_t s = 0; s < S; ++s) {
-        uint32_t n00, n01, n10, n11;
-        const uint32_t e1 = sh[2 * s + 1];
-        k2_counts<V, W>(ent, e0, e1, sh[2 * s], v, n00, n01, n10, n11);
-        e0 = e1;
+      // pairs within the minority species, for up to kK2MaxShells shells in one pass over its set
+      // bits (every lane has the same number of them: no divergence)
+      const V vv = P.k2_zeros ? ~v : v;
+      V x = vv & low_mask<V>(N);
+      uint32_t a[kK2MaxShells] = {};
+      while (x) {
+        const int bp = Word<W>::ctz(x);
+        x &= x - 1;
+#pragma unroll
+        for (int s = 0; s < kK2MaxShells; ++s)
+          if (s < static_cast<int>(S)) a[s] += k2_nbp_count<V, W>(part + P.k2_nbp_off, s, bp, vv);
+      }
+#pragma unroll
+      for (int s = 0; s < kK2MaxShells; ++s) {
+        if (s >= static_cast<int>(S)) break;
+        uint32_t DE = 0;  // sum over the ones of their shell-s degree: 2 n11 + n01 + n10
+        for (uint32_t e = sh[4 * s + 2]; e < sh[4 * s + 3]; ++e) {
+          const uint4 q = ent[e];
+          DE += q.z * Word<W>::pc(v, q.x, q.y);
+        }
+        const uint32_t ps = sh[4 * s];
+        uint32_t n00, nx, n11;
+        if (P.k2_zeros) {
+          n00 = a[s];
+          nx = (2u * ps - DE) - 2u * n00;
+          n11 = ps - n00 - nx;
+        } else {
+          n11 = a[s];
+          nx = DE - 2u * n11;
+          n00 = ps - n11 - nx;
+        }
         total = k2_term<T>(total, n00, f, w, tg, s * 4 + 0);
-        total = k2_term<T>(total, n01 + n10, f, w, tg, s * 4 + 1);
+        total = k2_term<T>(total, nx, f, w, tg, s * 4 + 1);
         total = k2_term<T>(total, n11, f, w, tg, s * 4 + 3);
       }
     }
