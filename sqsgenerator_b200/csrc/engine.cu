@@ -77,6 +77,33 @@ template <class T> static void copy_cube(std::vector<uint8_t>& blob, size_t off,
 // word. Wide form: header words  s | cnt << 8  and  ioff, then one word per offset.
 static bool narrow_stream(uint32_t n_sites) { return host_site_off(n_sites ? n_sites - 1 : 0) < 0x10000u; }
 
+// CTAs of the general-path kernel (sqsg_engine_wide, at most kMinBlocksWide) that fit on one SM of
+// `device` with `dynamic_smem` bytes each, from the device's shared memory per SM and per-block
+// reservation and the kernel's static shared memory (an estimate that needs no CUDA context).
+static int ctas_per_sm(int device, size_t dynamic_smem) {
+  static std::mutex m;
+  static std::map<int, std::pair<size_t, size_t>> cache;  // device -> (smem per SM, reserved per block)
+  std::pair<size_t, size_t> dev{233472, 1024};
+  {
+    std::lock_guard<std::mutex> l(m);
+    auto it = cache.find(device);
+    if (it != cache.end()) {
+      dev = it->second;
+    } else {
+      int per_sm = 0, reserved = 0;
+      if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) == cudaSuccess &&
+          cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) == cudaSuccess)
+        dev = {static_cast<size_t>(per_sm), static_cast<size_t>(reserved)};
+      else
+        cudaGetLastError();
+      cache[device] = dev;
+    }
+  }
+  const size_t static_smem = sizeof(JobDesc) + kCtaLevelSlots * sizeof(LevelSlot) + 128;
+  const size_t per_cta = align_up(dynamic_smem + static_smem, 128) + dev.second;
+  return static_cast<int>(std::min<size_t>(kMinBlocksWide, dev.first / per_cta));
+}
+
 static std::vector<uint32_t> build_stream(const sqsg_sublattice& sl) {
   const uint32_t N = sl.n_sites, S = sl.n_shells, P = sl.n_pairs;
   std::vector<std::vector<uint32_t>> by(static_cast<size_t>(S) * N);
@@ -270,14 +297,15 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
       for (uint32_t x = 0; x < N; ++x) ones += sl.species[x] != 0 ? 1u : 0u;
       P.k2_zeros = 2 * ones > N ? 1u : 0u;
     }
-    // staged section layout: cubes | windows | stream | species codes | binary-path masks
+    // blob section layout: cubes | windows | species codes | binary-path masks | pair stream. The
+    // stream is staged into shared memory with the rest when that costs no CTA per SM; otherwise
+    // (large cells, split jobs, the binary path that does not read it) it is read from the blob
+    // through L1: one copy per SM for all its CTAs, leaving the shared memory to more CTAs.
     size_t off = 0;
     P.cube_off = 0;
     off = align_up(3 * skk * pj.tsz, 16);
     P.win_off = static_cast<uint32_t>(off);
     off = align_up(off + 8ull * sl.n_windows, 16);
-    P.stream_off = static_cast<uint32_t>(off);
-    off = align_up(off + 4ull * streams[p].size(), 16);
     P.species_off = static_cast<uint32_t>(off);
     off = align_up(off + sl.n_sites, 16);
     if (k2) {
@@ -294,9 +322,17 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
       k2_data.emplace_back();
       k2_nbp_data.emplace_back();
     }
-    P.static_bytes = static_cast<uint32_t>(off);
+    P.stream_off = static_cast<uint32_t>(off);
+    const size_t with_stream = align_up(off + 4ull * streams[p].size(), 16);
+    const size_t lanes = (static_cast<size_t>((sl.n_sites + 3) / 4) +
+                          static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw) * kBlock * 4;
+    const bool staged = !k2 && job.n_sublattices == 1 &&
+                        ctas_per_sm(job.device, with_stream + lanes) >= ctas_per_sm(job.device, off + lanes);
+    P.stream_global = staged ? 0u : 1u;
+    P.static_bytes = static_cast<uint32_t>(staged ? with_stream : off);
     P.blob_off = static_cast<uint32_t>(blob_size);
-    blob_size += off;
+    blob_size += with_stream;
+    off = P.static_bytes;
     // shared memory: staged section, species columns, histogram
     P.smem_off = static_cast<uint32_t>(smem);
     P.col_off = static_cast<uint32_t>(off);

@@ -80,6 +80,7 @@ struct PartDesc {
   uint32_t hw;            // histogram words per (shell, species) row: ceil(K/2) 16-bit fields pairs
   uint32_t stream_words;  // words of the grouped pair stream
   uint32_t stream_narrow; // 1: 16-bit j offsets, two per word, one header word per group (N <= 512)
+  uint32_t stream_global; // 1: the stream is read from the job blob (through L1), 0: staged in shared memory
   uint32_t blob_off;      // staged section: offset in the job blob (16-byte aligned)
   uint32_t static_bytes;  // staged section size (multiple of 16)
   uint32_t smem_off;      // part base in dynamic shared memory

@@ -94,11 +94,20 @@ __device__ __forceinline__ void init_column(uint8_t* smem, const PartDesc& P, in
 }
 
 // Ordered bond counts of the lane's configuration into its histogram (16-bit fields).
-template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, const PartDesc& P, int t) {
+// Stream word k: from the job blob through the read-only L1 path (GLOBAL; every lane of a warp reads
+// the same address, one request, and the stream stays L1-resident for all CTAs of the SM) or from
+// the staged copy in shared memory.
+template <bool GLOBAL> __device__ __forceinline__ uint32_t stream_word(const uint32_t* st, uint32_t k) {
+  if (GLOBAL) return __ldg(st + k);
+  return st[k];
+}
+
+template <int KW, bool GLOBAL>
+__device__ __forceinline__ void count_part_from(uint8_t* smem, const uint32_t* __restrict__ st, const PartDesc& P,
+                                                int t) {
   uint8_t* part = part_base(smem, P);
   const uint8_t* col = part + P.col_off + 4 * t;
   uint32_t* hist = reinterpret_cast<uint32_t*>(part + P.hist_off) + t;
-  const uint32_t* st = reinterpret_cast<const uint32_t*>(part + P.stream_off);
   const uint32_t K = P.n_species, hw = P.hw, words = P.stream_words;
   const uint32_t nh = P.n_shells * K * hw;
   for (uint32_t w = 0; w < nh; ++w) hist[w * kBlock] = 0;
@@ -106,7 +115,7 @@ template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, cons
   if (P.stream_narrow) {
     // one header word per group, then two 16-bit column offsets per word
     while (pos < words) {
-      const uint32_t hdr = st[pos];
+      const uint32_t hdr = stream_word<GLOBAL>(st, pos);
       const uint32_t s = (hdr >> 16) & 0xffu, cnt = hdr >> 24;
       const uint32_t ci = col[hdr & 0xffffu] >> 3;
       const uint32_t* js = st + pos + 1;
@@ -116,20 +125,20 @@ template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, cons
         uint32_t row = 0;
 #pragma unroll 4
         for (uint32_t e = 0; e < pairs; ++e) {
-          const uint32_t w2 = js[e];
+          const uint32_t w2 = stream_word<GLOBAL>(js, e);
           row += (1u << col[w2 & 0xffffu]) + (1u << col[w2 >> 16]);
         }
-        if (cnt & 1u) row += 1u << col[js[pairs] & 0xffffu];
+        if (cnt & 1u) row += 1u << col[stream_word<GLOBAL>(js, pairs) & 0xffffu];
         h[0] += __byte_perm(row, 0, 0x4140);
         if (hw > 1) h[kBlock] += __byte_perm(row, 0, 0x4342);
       } else {
         unsigned long long row = 0;
 #pragma unroll 4
         for (uint32_t e = 0; e < pairs; ++e) {
-          const uint32_t w2 = js[e];
+          const uint32_t w2 = stream_word<GLOBAL>(js, e);
           row += (1ull << col[w2 & 0xffffu]) + (1ull << col[w2 >> 16]);
         }
-        if (cnt & 1u) row += 1ull << col[js[pairs] & 0xffffu];
+        if (cnt & 1u) row += 1ull << col[stream_word<GLOBAL>(js, pairs) & 0xffffu];
         const uint32_t lo = static_cast<uint32_t>(row), hi = static_cast<uint32_t>(row >> 32);
         h[0] += __byte_perm(lo, 0, 0x4140);
         if (hw > 1) h[kBlock] += __byte_perm(lo, 0, 0x4342);
@@ -141,8 +150,8 @@ template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, cons
     return;
   }
   while (pos < words) {
-    const uint32_t hdr = st[pos];
-    const uint32_t ioff = st[pos + 1];
+    const uint32_t hdr = stream_word<GLOBAL>(st, pos);
+    const uint32_t ioff = stream_word<GLOBAL>(st, pos + 1);
     const uint32_t s = hdr & 0xffu, cnt = (hdr >> 8) & 0xffu;
     const uint32_t ci = col[ioff] >> 3;
     const uint32_t* js = st + pos + 2;
@@ -150,13 +159,13 @@ template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, cons
     if (KW == 1) {
       uint32_t row = 0;
 #pragma unroll 4
-      for (uint32_t e = 0; e < cnt; ++e) row += 1u << col[js[e]];
+      for (uint32_t e = 0; e < cnt; ++e) row += 1u << col[stream_word<GLOBAL>(js, e)];
       h[0] += __byte_perm(row, 0, 0x4140);
       if (hw > 1) h[kBlock] += __byte_perm(row, 0, 0x4342);
     } else {
       unsigned long long row = 0;
 #pragma unroll 4
-      for (uint32_t e = 0; e < cnt; ++e) row += 1ull << col[js[e]];
+      for (uint32_t e = 0; e < cnt; ++e) row += 1ull << col[stream_word<GLOBAL>(js, e)];
       const uint32_t lo = static_cast<uint32_t>(row), hi = static_cast<uint32_t>(row >> 32);
       h[0] += __byte_perm(lo, 0, 0x4140);
       if (hw > 1) h[kBlock] += __byte_perm(lo, 0, 0x4342);
@@ -165,6 +174,14 @@ template <int KW> __device__ __forceinline__ void count_part(uint8_t* smem, cons
     }
     pos += 2 + cnt;
   }
+}
+
+template <int KW>
+__device__ __forceinline__ void count_part(uint8_t* smem, const uint8_t* blob, const PartDesc& P, int t) {
+  if (P.stream_global)
+    count_part_from<KW, true>(smem, reinterpret_cast<const uint32_t*>(blob + P.blob_off + P.stream_off), P, t);
+  else
+    count_part_from<KW, false>(smem, reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.stream_off), P, t);
 }
 
 __device__ __forceinline__ uint32_t bond(const uint32_t* hist, uint32_t K, uint32_t hw, uint32_t s, uint32_t a,
@@ -546,7 +563,7 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
           if (it > 0) init_column(smem, P, t);
           shuffle_part(smem, P, t, 0u, tile.start + my_off + it, p, k0, k1);
         }
-        count_part<KW>(smem, P, t);
+        count_part<KW>(smem, J.blob, P, t);
         const T o = objective_part<T>(smem, P, t);
         total = p == 0 ? o : F::add(total, o);
       }

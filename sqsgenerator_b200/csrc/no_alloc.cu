@@ -197,17 +197,18 @@ static Err prepare(const sqsg_job& job, JobDesc& d, size_t& blob_size, size_t& n
     off = align_up(3 * skk * tsz, 16);
     P.win_off = static_cast<uint32_t>(off);
     off = align_up(off + 8ull * sl.n_windows, 16);
-    P.stream_off = static_cast<uint32_t>(off);
-    off = align_up(off + 4ull * words, 16);
     P.species_off = static_cast<uint32_t>(off);
     off = align_up(off + N, 16);
-    P.static_bytes = static_cast<uint32_t>(off);
+    P.static_bytes = static_cast<uint32_t>(off);  // staged; the stream after it is read from the blob
+    P.stream_off = static_cast<uint32_t>(off);
+    P.stream_global = 1;
+    const size_t section = align_up(off + 4ull * words, 16);
     P.blob_off = static_cast<uint32_t>(blob_size);
-    if (blob_size + off > kBlobBytes) NA_FAIL(SQSG_ERR_CAPACITY, "job data exceeds the 3 MiB static staging area");
+    if (blob_size + section > kBlobBytes) NA_FAIL(SQSG_ERR_CAPACITY, "job data exceeds the 3 MiB static staging area");
     P.stream_words = static_cast<uint32_t>(words);
     // fill the staged section
     unsigned char* base = g_stage_blob + blob_size;
-    std::memset(base, 0, off);
+    std::memset(base, 0, section);
     std::memcpy(base + P.cube_off, sl.prefactors, skk * tsz);
     std::memcpy(base + P.cube_off + skk * tsz, sl.pair_weights, skk * tsz);
     std::memcpy(base + P.cube_off + 2 * skk * tsz, sl.target, skk * tsz);
@@ -239,7 +240,7 @@ static Err prepare(const sqsg_job& job, JobDesc& d, size_t& blob_size, size_t& n
         }
       }
     for (uint32_t x = 0; x < N; ++x) base[P.species_off + x] = static_cast<unsigned char>(sl.species[x] << 3);
-    blob_size += off;
+    blob_size += section;
     P.smem_off = static_cast<uint32_t>(smem);
     P.col_off = static_cast<uint32_t>(off);
     off += static_cast<size_t>((N + 3) / 4) * kBlock * 4;
