@@ -63,6 +63,10 @@ struct PreparedJob {
   uint32_t configs_per_thread = 1;
   uint64_t max_results = 0;     // caller's record capacity (0 = default)
   uint64_t range_first = 0, range_count = 0;  // share of the configuration space to evaluate
+  // a re-run of an overflowed job: record capacity, starting threshold, passes already made
+  uint64_t rerun_capacity = 0;
+  double rerun_threshold = 0.0;
+  int passes = 0;
 };
 
 template <class T> static void copy_cube(std::vector<uint8_t>& blob, size_t off, const void* src, size_t n) {
@@ -572,9 +576,9 @@ struct Run {
   std::vector<PartMeta> parts;
   size_t tsz = 8;
   uint64_t count = 0;
-  std::vector<uint8_t> objective, sub_objective, sro;  // raw T bytes
-  std::vector<uint8_t> species;
-  std::vector<uint64_t> id;
+  ByteVec objective, sub_objective, sro;  // raw T bytes
+  ByteVec species;
+  IdVec id;
   sqsg_statistics stats{};
   // keep+1 best distinct objectives with evaluation counts and id checksums (exact unless
   // levels_exact is false), and whether the record set was cut at the capacity.
@@ -873,6 +877,11 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     blob_total = align_up(blob_total + pjs[j].blob.size(), 256);
     const uint64_t budget = (512ull << 20) / pjs[j].record_bytes;
     capacity[j] = pjs[j].max_results ? pjs[j].max_results : std::max<uint64_t>(1024, std::min<uint64_t>(1u << 20, budget));
+    if (pjs[j].rerun_capacity) {
+      capacity[j] = pjs[j].rerun_capacity;
+      fixed_threshold[j] = true;
+      start_threshold[j] = pjs[j].rerun_threshold;
+    }
   }
   std::vector<Tile> tiles;
   for (size_t j = 0; j < nj; ++j) make_tiles(pjs[j], static_cast<uint32_t>(j), tiles);
@@ -1025,7 +1034,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
                                 cudaMemcpyDeviceToHost));
         d2h_bytes += recs[j].size();
       }
-      const bool may_rerun = !pjs[j].max_results && attempt < 2;
+      const bool may_rerun = !pjs[j].max_results && pjs[j].passes + attempt < 2;
       outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, kRerunRecordBytes / pjs[j].record_bytes);
       if (outc[j].rerun) {
         capacity[j] = outc[j].rerun_capacity;
@@ -1034,11 +1043,16 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
         rerun = true;
       }
     }
-    if (rerun) continue;
+    if (rerun && trace) continue;  // a traced job is one job: run it again whole
 
     const uint64_t t_loop = now_ns();
     runs.assign(nj, Run{});
+    std::vector<size_t> again;  // overflowed jobs of a batch run again alone, the rest finish now
     for (size_t j = 0; j < nj; ++j) {
+      if (outc[j].rerun) {
+        again.push_back(j);
+        continue;
+      }
       const unsigned long long* cj = &cnt[j * kNumCounters];
       const uint64_t n = std::min<uint64_t>(cj[kCandidates], capacity[j]);
       Run& r = runs[j];
@@ -1084,6 +1098,25 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       runs[j].h2d_bytes = h2d_bytes / nj;
       runs[j].d2h_bytes = d2h_bytes / nj;
     }
+    if (!again.empty()) {
+      std::vector<PreparedJob> sub;
+      std::vector<const sqsg_job*> subsrc;
+      for (size_t j : again) {
+        PreparedJob pj = pjs[j];
+        pj.rerun_capacity = capacity[j];
+        pj.rerun_threshold = start_threshold[j];
+        pj.passes += attempt + 1;
+        sub.push_back(std::move(pj));
+        subsrc.push_back(srcs[j]);
+      }
+      std::vector<Run> subruns;
+      execute(sub, subsrc, device, subruns, nullptr);
+      for (size_t k = 0; k < again.size(); ++k) {
+        const uint64_t total = subruns[k].stats.timings_ns[SQSG_TIMING_LOOP];
+        runs[again[k]] = std::move(subruns[k]);
+        runs[again[k]].stats.timings_ns[SQSG_TIMING_LOOP] = total + static_cast<uint64_t>(loop_ms_total * 1e6);
+      }
+    }
     if (trace && trace->capacity) {
       const PreparedJob& pj = pjs[0];
       const uint64_t n = std::min<uint64_t>(pj.range_count, trace->capacity);
@@ -1098,10 +1131,13 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       if (trace->id) CUDA_CHECK(cudaMemcpy(trace->id, ws->trace_id.p, n * 8, cudaMemcpyDeviceToHost));
     }
     const uint64_t t_end = now_ns();
-    for (auto& r : runs) {
+    std::vector<bool> rerun_job(nj, false);
+    for (size_t j : again) rerun_job[j] = true;
+    for (size_t j = 0; j < nj; ++j) {
+      Run& r = runs[j];
       r.stats.timings_ns[SQSG_TIMING_TOTAL] = t_end - t0;
       r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = t_setup - t0;
-      r.stats.timings_ns[SQSG_TIMING_LOOP] = static_cast<uint64_t>(loop_ms_total * 1e6);
+      if (!rerun_job[j]) r.stats.timings_ns[SQSG_TIMING_LOOP] = static_cast<uint64_t>(loop_ms_total * 1e6);
       r.stats.timings_ns[SQSG_TIMING_COMM] = t_end - t_loop;
     }
     return;

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 #include <string>
 
 #include "select.h"
@@ -40,7 +41,51 @@ void SelectScratch::release() {
   }
   if (stream) cudaStreamSynchronize(stream);
   stream = nullptr;
+  for (int k = 0; k < 2; ++k) {
+    if (bounce[k]) cudaFreeHost(bounce[k]);
+    if (bounce_done[k]) cudaEventDestroy(bounce_done[k]);
+    bounce[k] = nullptr;
+    bounce_done[k] = nullptr;
+  }
 }
+
+namespace {
+
+constexpr size_t kBounceBytes = 32u << 20;
+
+// Device-to-host copy into pageable memory. Large copies go through two pinned buffers: the copy
+// engine fills one while the host drains the other (several times the driver's pageable rate).
+void copy_out(SelectScratch& S, cudaStream_t st, void* dst, const void* src, size_t bytes) {
+  if (bytes < (4u << 20)) {
+    SEL_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    return;
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (!S.bounce[k]) SEL_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.bounce[k]), kBounceBytes, cudaHostAllocDefault));
+    if (!S.bounce_done[k]) SEL_CHECK(cudaEventCreateWithFlags(&S.bounce_done[k], cudaEventDisableTiming));
+  }
+  size_t pend_off[2] = {}, pend_len[2] = {};
+  bool pend[2] = {false, false};
+  int b = 0;
+  auto drain = [&](int k) {
+    SEL_CHECK(cudaEventSynchronize(S.bounce_done[k]));
+    std::memcpy(static_cast<uint8_t*>(dst) + pend_off[k], S.bounce[k], pend_len[k]);
+    pend[k] = false;
+  };
+  for (size_t off = 0; off < bytes; off += kBounceBytes, b ^= 1) {
+    const size_t len = std::min(kBounceBytes, bytes - off);
+    if (pend[b]) drain(b);
+    SEL_CHECK(cudaMemcpyAsync(S.bounce[b], static_cast<const uint8_t*>(src) + off, len, cudaMemcpyDeviceToHost, st));
+    SEL_CHECK(cudaEventRecord(S.bounce_done[b], st));
+    pend[b] = true;
+    pend_off[b] = off;
+    pend_len[b] = len;
+  }
+  for (int k = 0; k < 2; ++k)
+    if (pend[(b + k) % 2]) drain((b + k) % 2);
+}
+
+}  // namespace
 
 // The device's default pool keeps what select_on_device frees, so later calls reuse it.
 static void keep_pool_memory() {
@@ -352,11 +397,11 @@ bool select_on_device(SelectScratch& S, cudaStream_t st, const RecordLayout& lay
   out.species.resize(b_sp);
   out.sro.resize(b_sro);
   out.id.resize(m2);
-  SEL_CHECK(cudaMemcpyAsync(out.objective.data(), o.objective, b_obj, cudaMemcpyDeviceToHost, st));
-  SEL_CHECK(cudaMemcpyAsync(out.sub_objective.data(), o.sub_objective, b_sub, cudaMemcpyDeviceToHost, st));
-  SEL_CHECK(cudaMemcpyAsync(out.species.data(), o.species, b_sp, cudaMemcpyDeviceToHost, st));
-  SEL_CHECK(cudaMemcpyAsync(out.sro.data(), o.sro, b_sro, cudaMemcpyDeviceToHost, st));
-  SEL_CHECK(cudaMemcpyAsync(out.id.data(), o.id, b_id, cudaMemcpyDeviceToHost, st));
+  copy_out(S, st, out.objective.data(), o.objective, b_obj);
+  copy_out(S, st, out.sub_objective.data(), o.sub_objective, b_sub);
+  copy_out(S, st, out.species.data(), o.species, b_sp);
+  copy_out(S, st, out.sro.data(), o.sro, b_sro);
+  copy_out(S, st, out.id.data(), o.id, b_id);
   SEL_CHECK(cudaStreamSynchronize(st));
   return true;
 }

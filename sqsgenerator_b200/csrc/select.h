@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "engine.cuh"
@@ -24,10 +26,22 @@ struct RecordLayout {
   uint32_t sro_bytes[kMaxParts] = {};
 };
 
+// Allocator whose resize() leaves new elements uninitialised: result arrays of millions of
+// configurations are overwritten right away, and zero-filling them first doubled their cost.
+template <class T> struct NoInitAlloc : std::allocator<T> {
+  template <class U> struct rebind { using other = NoInitAlloc<U>; };
+  NoInitAlloc() = default;
+  template <class U> NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  template <class U> void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
+  template <class U, class... A> void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+using ByteVec = std::vector<uint8_t, NoInitAlloc<uint8_t>>;
+using IdVec = std::vector<uint64_t, NoInitAlloc<uint64_t>>;
+
 struct SelectedSet {
   uint64_t count = 0;
-  std::vector<uint8_t> objective, sub_objective, species, sro;  // raw T bytes / species bytes
-  std::vector<uint64_t> id;
+  ByteVec objective, sub_objective, species, sro;  // raw T bytes / species bytes
+  IdVec id;
 };
 
 // Grow-only device scratch for select_on_device, bound to the stream it was last used on.
@@ -35,6 +49,8 @@ struct SelectScratch {
   void* buf[16] = {};
   size_t size[16] = {};
   cudaStream_t stream = nullptr;
+  uint8_t* bounce[2] = {};        // pinned host buffers for large device-to-host copies
+  cudaEvent_t bounce_done[2] = {};
   ~SelectScratch() { release(); }
   void* get(int slot, size_t bytes);
   // Frees every buffer on its stream and waits for it; call before that stream is destroyed.
