@@ -5,8 +5,12 @@
 
 #include <cuda_runtime.h>
 
+#include <sys/mman.h>
+
 #include <cstdint>
+#include <cstdlib>
 #include <memory>
+#include <new>
 #include <utility>
 #include <vector>
 
@@ -26,12 +30,30 @@ struct RecordLayout {
   uint32_t sro_bytes[kMaxParts] = {};
 };
 
-// Allocator whose resize() leaves new elements uninitialised: result arrays of millions of
-// configurations are overwritten right away, and zero-filling them first doubled their cost.
+// Allocator for result arrays of up to millions of configurations: resize() leaves new elements
+// uninitialised (they are overwritten right away; zero-filling first doubled the cost), and blocks
+// of 64 MiB and more are 2 MiB-aligned and advised for transparent huge pages, so that filling
+// them takes a few thousand page faults instead of a million.
 template <class T> struct NoInitAlloc : std::allocator<T> {
+  static constexpr size_t kHuge = 2u << 20, kLarge = 64u << 20;
   template <class U> struct rebind { using other = NoInitAlloc<U>; };
   NoInitAlloc() = default;
   template <class U> NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  T* allocate(size_t n) {
+    const size_t bytes = n * sizeof(T);
+    if (bytes < kLarge) return std::allocator<T>::allocate(n);
+    const size_t rounded = (bytes + kHuge - 1) / kHuge * kHuge;
+    void* p = std::aligned_alloc(kHuge, rounded);
+    if (!p) throw std::bad_alloc();
+    madvise(p, rounded, MADV_HUGEPAGE);
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t n) noexcept {
+    if (n * sizeof(T) < kLarge)
+      std::allocator<T>::deallocate(p, n);
+    else
+      std::free(p);
+  }
   template <class U> void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
   template <class U, class... A> void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
 };
