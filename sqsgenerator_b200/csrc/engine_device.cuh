@@ -379,11 +379,13 @@ struct WarpState {
   double list;          // lane's entry of the warp list (+inf = empty)
   double list_thr;      // warp-uniform (keep+1)-th entry
   unsigned long long published_thr, published_best;
+  bool records_full;    // lane 0: the job's record buffer is known to be full (it never empties)
   __device__ void reset() {
     list = __longlong_as_double(0x7ff0000000000000ll);
     list_thr = list;
     published_thr = ~0ull;
     published_best = ~0ull;
+    records_full = false;
   }
 };
 
@@ -504,11 +506,16 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
   // candidate counter is left alone.
   unsigned long long base = 0;
   if (lane == 0) {
-    if (*reinterpret_cast<volatile unsigned long long*>(&J.counters[kRecordsFull]) != 0ull) {
+    if (ws.records_full ||
+        *reinterpret_cast<volatile unsigned long long*>(&J.counters[kRecordsFull]) != 0ull) {
+      ws.records_full = true;  // no more loads of the flag from this warp
       base = ~0ull;
     } else {
       base = atomicAdd(&J.counters[kCandidates], static_cast<unsigned long long>(__popc(km)));
-      if (base + __popc(km) > J.capacity) J.counters[kRecordsFull] = 1ull;
+      if (base + __popc(km) > J.capacity) {
+        J.counters[kRecordsFull] = 1ull;
+        ws.records_full = true;
+      }
     }
   }
   base = __shfl_sync(0xffffffffu, base, 0);
