@@ -20,7 +20,6 @@
 #include <random>
 #include <string>
 #include <thread>
-#include <tuple>
 #include <unordered_set>
 #include <vector>
 
@@ -207,7 +206,6 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   std::vector<std::vector<uint32_t>> streams(job.n_sublattices);
   std::vector<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>> k2_data;
   std::vector<std::vector<uint32_t>> k2_nbp_data;
-  std::vector<std::tuple<std::vector<uint32_t>, std::vector<uint32_t>, std::vector<uint32_t>>> bits_data;
   for (uint32_t p = 0; p < job.n_sublattices; ++p) {
     const sqsg_sublattice& sl = job.sublattices[p];
     PartDesc& P = d.parts[p];
@@ -241,65 +239,6 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
     // binary fast path data: per (shell, site) mask of the neighbours j > i (bit N-1-j)
     const bool k2 = job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64 && sl.n_shells <= kK2MaxShells;
-    // binary bit-set path for larger random-mode cells: per site and shell the masks of the
-    // neighbours j > i grouped by 32-bit word, per shell the degree classes
-    const bool bitset = !k2 && !pj.systematic && job.n_sublattices == 1 && sl.n_species == 2 &&
-                        sl.n_shells <= kK2MaxShells && sl.n_sites <= kBitsMaxSites;
-    std::vector<uint32_t> site_stream, deg_stream, bits0;
-    if (bitset) {
-      const uint32_t N = sl.n_sites, S = sl.n_shells, Wd = (N + 31) / 32;
-      std::vector<std::map<uint32_t, uint32_t>> fw(static_cast<size_t>(S) * N);  // (s, i) -> word -> mask
-      std::vector<uint32_t> deg(static_cast<size_t>(S) * N, 0), fwd(static_cast<size_t>(S) * N, 0);
-      for (uint32_t e = 0; e < sl.n_pairs; ++e) {
-        uint32_t i = sl.pairs[3 * e], j = sl.pairs[3 * e + 1];
-        const uint32_t sh = sl.pairs[3 * e + 2];
-        if (i > j) std::swap(i, j);
-        fw[static_cast<size_t>(sh) * N + i][j >> 5] |= 1u << (j & 31);
-        deg[static_cast<size_t>(sh) * N + i]++;
-        deg[static_cast<size_t>(sh) * N + j]++;
-        fwd[static_cast<size_t>(sh) * N + i]++;
-      }
-      bool fits = true;
-      for (uint32_t x = 0; x < S * N; ++x) fits = fits && fwd[x] <= 0xffu && fw[x].size() <= 0xffu;
-      if (fits) {
-        for (uint32_t i = 0; i < N; ++i) {
-          uint32_t w0 = 0, w1 = 0;
-          for (uint32_t sh = 0; sh < S; ++sh) {
-            w0 |= static_cast<uint32_t>(fw[static_cast<size_t>(sh) * N + i].size()) << (8 * sh);
-            w1 |= fwd[static_cast<size_t>(sh) * N + i] << (8 * sh);
-          }
-          site_stream.push_back(w0);
-          site_stream.push_back(w1);
-          for (uint32_t sh = 0; sh < S; ++sh)
-            for (auto& [word, mask] : fw[static_cast<size_t>(sh) * N + i]) {
-              site_stream.push_back(mask);
-              site_stream.push_back(word);
-            }
-        }
-        for (uint32_t sh = 0; sh < S; ++sh) {
-          std::map<uint32_t, std::vector<uint32_t>> classes;
-          for (uint32_t x = 0; x < N; ++x) {
-            const uint32_t dv = deg[static_cast<size_t>(sh) * N + x];
-            if (!dv) continue;
-            auto& m = classes[dv];
-            if (m.empty()) m.assign(Wd, 0u);
-            m[x >> 5] |= 1u << (x & 31);
-          }
-          deg_stream.push_back(static_cast<uint32_t>(classes.size()));
-          for (auto& [dv, m] : classes) {
-            deg_stream.push_back(dv);
-            deg_stream.insert(deg_stream.end(), m.begin(), m.end());
-          }
-        }
-        bits0.assign(Wd, 0u);
-        for (uint32_t x = 0; x < N; ++x)
-          if (sl.species[x]) bits0[x >> 5] |= 1u << (x & 31);
-        std::vector<uint32_t> per_shell(S, 0);  // after the words: the pairs of each shell
-        for (uint32_t e = 0; e < sl.n_pairs; ++e) per_shell[sl.pairs[3 * e + 2]]++;
-        bits0.insert(bits0.end(), per_shell.begin(), per_shell.end());
-        P.bits_words = Wd;
-      }
-    }
     std::vector<uint32_t> k2_entries, k2_shells, k2_nbp;
     if (k2) {
       const uint32_t N = sl.n_sites;
@@ -373,10 +312,6 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     off = align_up(off + 8ull * sl.n_windows, 16);
     P.species_off = static_cast<uint32_t>(off);
     off = align_up(off + sl.n_sites, 16);
-    if (P.bits_words) {
-      P.bits0_off = static_cast<uint32_t>(off);
-      off = align_up(off + 4ull * bits0.size(), 16);
-    }
     if (k2) {
       P.k2_off = static_cast<uint32_t>(off);
       P.k2_entries = static_cast<uint32_t>(k2_entries.size() / 4);
@@ -395,32 +330,17 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     const size_t with_stream = align_up(off + 4ull * streams[p].size(), 16);
     const size_t lanes = (static_cast<size_t>((sl.n_sites + 3) / 4) +
                           static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw) * kBlock * 4;
-    const bool staged = !k2 && !P.bits_words && job.n_sublattices == 1 &&
+    const bool staged = !k2 && job.n_sublattices == 1 &&
                         ctas_per_sm(job.device, with_stream + lanes) >= ctas_per_sm(job.device, off + lanes);
     P.stream_global = staged ? 0u : 1u;
     P.static_bytes = static_cast<uint32_t>(staged ? with_stream : off);
     P.blob_off = static_cast<uint32_t>(blob_size);
-    size_t section = with_stream;
-    if (P.bits_words) {  // global-only tables of the bit-set path after the pair stream
-      P.site_stream_off = static_cast<uint32_t>(section);
-      section = align_up(section + 4ull * site_stream.size(), 16);
-      P.deg_stream_off = static_cast<uint32_t>(section);
-      section = align_up(section + 4ull * deg_stream.size(), 16);
-      bits_data.emplace_back(std::move(bits0), std::move(site_stream), std::move(deg_stream));
-    } else {
-      bits_data.emplace_back();
-    }
-    blob_size += section;
+    blob_size += with_stream;
     off = P.static_bytes;
-    // shared memory: staged section, species columns (bit sets on the bit-set path), histogram
+    // shared memory: staged section, species columns, histogram
     P.smem_off = static_cast<uint32_t>(smem);
     P.col_off = static_cast<uint32_t>(off);
-    if (P.bits_words) {
-      P.bits_off = static_cast<uint32_t>(off);
-      off += static_cast<size_t>(P.bits_words) * kBlock * 4;
-    } else {
-      off += static_cast<size_t>((sl.n_sites + 3) / 4) * kBlock * 4;
-    }
+    off += static_cast<size_t>((sl.n_sites + 3) / 4) * kBlock * 4;
     P.hist_off = static_cast<uint32_t>(off);
     off += static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw * kBlock * 4;
     smem += align_up(off, 16);
@@ -439,7 +359,6 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     if (pj.systematic) pj.total = window_permutations(sl, P);
     if (k2 && (!pj.systematic || (P.unrank_k == 2 && P.unrank_rev[0] == 0 && P.unrank_rev[1] == 1)))
       d.k2 = sl.n_sites <= 32 ? 1 : 2;
-    if (P.bits_words) d.k2 = 3;
   }
   if (!pj.systematic) pj.total = job.iterations;
   d.total = pj.total;
@@ -478,12 +397,6 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     if (!k2d.second.empty()) std::memcpy(base + P.k2_shell_off, k2d.second.data(), 4 * k2d.second.size());
     if (!k2_nbp_data[p].empty())
       std::memcpy(base + P.k2_nbp_off, k2_nbp_data[p].data(), 4 * k2_nbp_data[p].size());
-    if (P.bits_words) {
-      const auto& [b0, ss, ds] = bits_data[p];
-      std::memcpy(base + P.bits0_off, b0.data(), 4 * b0.size());
-      std::memcpy(base + P.site_stream_off, ss.data(), 4 * ss.size());
-      std::memcpy(base + P.deg_stream_off, ds.data(), 4 * ds.size());
-    }
   }
   // binary systematic path: binomials C(m, j) for m <= window size, j <= ones in the window, kept in
   // global memory after the staged sections (read through the L1 by the per-thread unrank)
@@ -1032,7 +945,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     ws->ctrl_host[0] = 0;
 
     bool all_bitmask = true;
-    for (size_t j = 0; j < nj; ++j) all_bitmask = all_bitmask && (pjs[j].desc.k2 == 1 || pjs[j].desc.k2 == 2);
+    for (size_t j = 0; j < nj; ++j) all_bitmask = all_bitmask && pjs[j].desc.k2 != 0;
     const EngineKernel kernel = engine_for(all_bitmask);
     const uint32_t grid = launch_grid(device, smem, tiles.size(), kernel);
     CUDA_CHECK(cudaEventRecord(ws->ev_start, ws->stream));
@@ -1864,7 +1777,7 @@ static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, co
     configure_kernel(max_dynamic_smem(device));
     std::map<std::pair<int, int>, std::vector<uint32_t>> classes;
     for (uint32_t j = 0; j < n; ++j) {
-      const bool bitmask = pjs[j].desc.k2 == 1 || pjs[j].desc.k2 == 2;
+      const bool bitmask = pjs[j].desc.k2 != 0;
       int per_sm = 0;
       CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_for(bitmask), kBlock,
                                                                pjs[j].desc.smem_bytes));
@@ -2091,8 +2004,7 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
     if (need > S.rings[kBuckets - 1].smem)
       throw unsupported_error("the job needs more shared memory per CTA than this device offers");
     J->bucket = kBuckets - 1;
-    const bool bitmask = J->pj.desc.k2 == 1 || J->pj.desc.k2 == 2;
-    for (int b = bitmask ? 0 : 1; b < kBuckets; ++b)  // other jobs use the wide kernel
+    for (int b = J->pj.desc.k2 ? 0 : 1; b < kBuckets; ++b)  // general-path jobs use the wide kernel
       if (need <= S.rings[b].smem) {
         J->bucket = b;
         break;

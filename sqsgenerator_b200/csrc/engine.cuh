@@ -40,8 +40,7 @@ __host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
 
 constexpr int kBlock = 128;       // threads per CTA (each owns one configuration)
 constexpr int kMinBlocks = 5;     // sqsg_engine: CTAs per SM the register budget must allow (<= 102 registers)
-constexpr int kK2MaxShells = 4;
-constexpr uint32_t kBitsMaxSites = 1024;  // sites of the binary bit-set path (32 words per lane)   // shells of the binary bit-mask path (per-shell counters in registers)
+constexpr int kK2MaxShells = 4;   // shells of the binary bit-mask path (per-shell counters in registers)
 constexpr int kMinBlocksWide = 4; // sqsg_engine_wide (general path): 128 registers, no spills in the pair loop
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
@@ -108,12 +107,6 @@ struct PartDesc {
   uint32_t k2_binom_off;  // blob offset (global, not staged) of C(m, j), m <= window, j <= ones
   uint32_t k2_nbp_off;    // neighbour masks by bit position: u32 [S][32] (N <= 32) or uint2 [S][64]
   uint32_t k2_zeros;      // 1: count over the zeros (species 0 is the minority), else over the ones
-  // binary bit-set path (K == 2, N > 64, random mode): a lane's configuration is a bit set
-  uint32_t bits_words;      // words of a lane's bit set (0: another path)
-  uint32_t bits_off;        // shared-memory offset of the lane bit sets, bits_words x kBlock words
-  uint32_t bits0_off;       // staged: the packed initial arrangement as bits_words words, then S pair counts
-  uint32_t site_stream_off; // blob (read through L1): per site, per shell the j > i masks by word
-  uint32_t deg_stream_off;  // blob: per shell the degree classes (degree, bits_words mask words)
 };
 
 struct JobDesc {
@@ -121,7 +114,7 @@ struct JobDesc {
   uint32_t mode;          // 0 random, 1 systematic
   uint32_t n_parts;
   uint32_t kw;            // 1: every part has K <= 4 (32-bit row), 2: K <= 8 (64-bit row)
-  uint32_t k2;            // 0: general path; 1, 2: binary bitmask path with N <= 32, 64; 3: binary bit-set path
+  uint32_t k2;            // 0: general path; 1: binary bitmask path with N <= 32; 2: with N <= 64
   uint32_t keep;
   uint32_t record_bytes;
   uint32_t smem_bytes;

@@ -389,15 +389,6 @@ struct WarpState {
   }
 };
 
-// Species index of site x in the lane's configuration (byte column, or bit set on the bit-set path).
-__device__ __forceinline__ uint32_t lane_species(const uint8_t* part, const PartDesc& P, int t, uint32_t x) {
-  if (P.bits_words) {
-    const uint32_t* b = reinterpret_cast<const uint32_t*>(part + P.bits_off) + t;
-    return (b[(x >> 5) * kBlock] >> (x & 31u)) & 1u;
-  }
-  return part[P.col_off + 4 * t + site_off(x)] >> 3;
-}
-
 template <class T>
 __device__ __forceinline__ void write_record(const JobDesc& J, uint8_t* smem, uint64_t idx, T total, uint64_t id,
                                              int t) {
@@ -406,8 +397,8 @@ __device__ __forceinline__ void write_record(const JobDesc& J, uint8_t* smem, ui
   *reinterpret_cast<uint64_t*>(rec + 8) = id;
   for (uint32_t p = 0; p < J.n_parts; ++p) {
     const PartDesc& P = J.parts[p];
-    const uint8_t* part = part_base(smem, P);
-    for (uint32_t x = 0; x < P.n_sites; ++x) rec[P.rec_species_off + x] = static_cast<uint8_t>(lane_species(part, P, t, x));
+    const uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
+    for (uint32_t x = 0; x < P.n_sites; ++x) rec[P.rec_species_off + x] = col[site_off(x)] >> 3;
     T* sro = reinterpret_cast<T*>(rec + P.rec_sro_off);
     *reinterpret_cast<T*>(rec + P.rec_obj_off) = objective_part<T>(smem, P, t, sro);
   }
@@ -422,8 +413,9 @@ __device__ __forceinline__ void write_trace(const JobDesc& J, uint8_t* smem, uin
   for (uint32_t p = 0; p < J.n_parts; ++p) {
     const PartDesc& P = J.parts[p];
     const uint8_t* part = part_base(smem, P);
+    const uint8_t* col = part + P.col_off + 4 * t;
     const uint32_t* hist = reinterpret_cast<const uint32_t*>(part + P.hist_off) + t;
-    for (uint32_t x = 0; x < P.n_sites; ++x) sp[P.trace_species_off + x] = static_cast<uint8_t>(lane_species(part, P, t, x));
+    for (uint32_t x = 0; x < P.n_sites; ++x) sp[P.trace_species_off + x] = col[site_off(x)] >> 3;
     const uint32_t S = P.n_shells, K = P.n_species;
     for (uint32_t s = 0; s < S; ++s)
       for (uint32_t a = 0; a < K; ++a)
@@ -867,167 +859,11 @@ __device__ __forceinline__ unsigned long long claim_live(QueueCtl* q, const vola
   }
 }
 
-// ------------------------------------------------------------------------------ binary bit-set path
-// Random mode, K == 2, 64 < N <= kBitsMaxSites: the lane's configuration is a bit set (site x at bit
-// x & 31 of word x >> 5; words interleaved across lanes like the byte columns, so a uniform word
-// index is conflict-free). Fisher-Yates swaps two sites by flipping both bits when they differ,
-// with the general path's Philox words, so both paths evaluate the same configurations. Counting
-// walks the sites in order (every lane at the same site): per shell the site's neighbours j > i
-// come as (mask, word) pairs, and n11 = sum_i b_i popc(mask & bits[word]); degree classes give
-// 2 n11 + n01 + n10 and P_s closes the system (as on the bit-mask path). Tables are read from the
-// job blob through L1 with warp-uniform addresses.
-__device__ __forceinline__ void bits_swap(uint32_t* b, uint32_t a, uint32_t c) {
-  const uint32_t ia = (a >> 5) * kBlock, ic = (c >> 5) * kBlock, sa = a & 31u, sc = c & 31u;
-  const uint32_t wa = b[ia];
-  const uint32_t d = ((wa >> sa) ^ (b[ic] >> sc)) & 1u;
-  b[ia] = wa ^ (d << sa);
-  b[ic] ^= d << sc;  // re-read: a and c may share the word
-}
-
-__device__ __forceinline__ void bits_shuffle(uint32_t* b, const uint32_t* win, uint32_t n_windows, uint64_t cid,
-                                             uint32_t k0, uint32_t k1) {
-  const uint32_t c_lo = static_cast<uint32_t>(cid), c_hi = static_cast<uint32_t>(cid >> 32) << 8;
-  uint32_t blk = 0;
-  for (uint32_t wi = 0; wi < n_windows; ++wi) {
-    const uint32_t lo = win[2 * wi];
-    uint32_t i = win[2 * wi + 1] - lo;
-    while (i > 1) {
-      const philox_ctr r = philox4x32_10(philox_ctr{blk++, 0u, c_lo, c_hi}, k0, k1);
-      const uint32_t xs[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (i <= 1) break;
-        bits_swap(b, lo + i - 1, lo + __umulhi(xs[q], i));
-        --i;
-      }
-    }
-  }
-}
-
-// Per shell: n11 (pairs inside species 1) and, with `ordered`, E = sum_i b_i fwd_s(i) (pairs i < j
-// with b_i = 1), from which n10 = E - n11.
-__device__ __forceinline__ void bits_count(const uint32_t* b, const uint32_t* __restrict__ st, uint32_t N, uint32_t S,
-                                           uint32_t* a, uint32_t* e, bool ordered) {
-  uint32_t pos = 0;
-  for (uint32_t i = 0; i < N; ++i) {
-    const uint32_t cnt = __ldg(st + pos), fwd = __ldg(st + pos + 1);
-    pos += 2;
-    const uint32_t nb = 0u - ((b[(i >> 5) * kBlock] >> (i & 31u)) & 1u);
-#pragma unroll
-    for (int s = 0; s < kK2MaxShells; ++s) {
-      if (s >= static_cast<int>(S)) break;
-      const uint32_t c = (cnt >> (8 * s)) & 0xffu;
-      uint32_t acc = 0;
-      for (uint32_t k = 0; k < c; ++k) {
-        const uint32_t m = __ldg(st + pos), w = __ldg(st + pos + 1);
-        pos += 2;
-        acc += __popc(m & b[w * kBlock]);
-      }
-      a[s] += acc & nb;
-      if (ordered) e[s] += ((fwd >> (8 * s)) & 0xffu) & nb;
-    }
-  }
-}
-
-// sum_x b_x deg_s(x) for shell s from its degree classes; returns the position after them.
-__device__ __forceinline__ uint32_t bits_degree(const uint32_t* b, const uint32_t* __restrict__ ds, uint32_t pos,
-                                                uint32_t W, uint32_t& de) {
-  const uint32_t nc = __ldg(ds + pos++);
-  de = 0;
-  for (uint32_t c = 0; c < nc; ++c) {
-    const uint32_t dv = __ldg(ds + pos++);
-    uint32_t ones = 0;
-    for (uint32_t w = 0; w < W; ++w) ones += __popc(b[w * kBlock] & __ldg(ds + pos + w));
-    pos += W;
-    de += dv * ones;
-  }
-  return pos;
-}
-
-template <class T>
-__device__ __forceinline__ void run_tile_bits(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
-                                           WarpState& ws) {
-  const int t = threadIdx.x;
-  const PartDesc& P = J.parts[0];
-  const uint64_t base = tile.count / kBlock, rem = tile.count % kBlock;
-  const uint64_t my_count = base + (static_cast<uint64_t>(t) < rem ? 1 : 0);
-  const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
-  const uint64_t max_count = base + (rem ? 1 : 0);
-  const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
-  uint8_t* part = part_base(smem, P);
-  const uint32_t N = P.n_sites, S = P.n_shells, W = P.bits_words;
-  uint32_t* bits = reinterpret_cast<uint32_t*>(part + P.bits_off) + t;
-  const uint32_t* bits0 = reinterpret_cast<const uint32_t*>(part + P.bits0_off);
-  const uint32_t* win = reinterpret_cast<const uint32_t*>(part + P.win_off);
-  const uint32_t* st = reinterpret_cast<const uint32_t*>(J.blob + P.blob_off + P.site_stream_off);
-  const uint32_t* ds = reinterpret_cast<const uint32_t*>(J.blob + P.blob_off + P.deg_stream_off);
-  const T* f = reinterpret_cast<const T*>(part + P.cube_off);
-  const T* w = f + 4 * S;
-  const T* tg = w + 4 * S;
-  T thr_g = load_threshold<T>(J);
-  for (uint64_t it = 0; it < max_count; ++it) {
-    const bool active = it < my_count;
-    const uint64_t id = tile.start + my_off + it;
-    T total = T(0);
-    uint32_t a[kK2MaxShells] = {}, de[kK2MaxShells] = {};
-    if (active) {
-      for (uint32_t k = 0; k < W; ++k) bits[k * kBlock] = bits0[k];
-      bits_shuffle(bits, win, P.n_windows, id, k0, k1);
-      bits_count(bits, st, N, S, a, nullptr, false);
-      uint32_t dpos = 0;
-#pragma unroll
-      for (int s = 0; s < kK2MaxShells; ++s) {
-        if (s >= static_cast<int>(S)) break;
-        dpos = bits_degree(bits, ds, dpos, W, de[s]);
-      }
-      const uint32_t* sh_ps = bits0 + W;  // pairs per shell
-#pragma unroll
-      for (int s = 0; s < kK2MaxShells; ++s) {
-        if (s >= static_cast<int>(S)) break;
-        const uint32_t n11 = a[s], nx = de[s] - 2u * a[s], n00 = sh_ps[s] - n11 - nx;
-        total = k2_term<T>(total, n00, f, w, tg, s * 4 + 0);
-        total = k2_term<T>(total, nx, f, w, tg, s * 4 + 1);
-        total = k2_term<T>(total, n11, f, w, tg, s * 4 + 3);
-      }
-    }
-    if ((it & 15) == 0) thr_g = load_threshold<T>(J);
-    const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
-    const bool pass = active && static_cast<double>(total) <= bound;
-    // the ordered counts (n01, n10 apart) are needed only for a record or a trace: one more pass
-    auto materialize = [&]() {
-      uint32_t a2[kK2MaxShells] = {}, e2[kK2MaxShells] = {};
-      bits_count(bits, st, N, S, a2, e2, true);
-      uint32_t* hist = reinterpret_cast<uint32_t*>(part + P.hist_off) + t;
-      const uint32_t* sh_ps = bits0 + W;  // pairs per shell
-      for (uint32_t s = 0; s < S; ++s) {
-        const uint32_t n11 = a2[s], nx = de[s] - 2u * n11, n10 = e2[s] - n11, n01 = nx - n10;
-        const uint32_t n00 = sh_ps[s] - n11 - nx;
-        hist[(s * 2 + 0) * kBlock] = n00 | (n01 << 16);
-        hist[(s * 2 + 1) * kBlock] = n10 | (n11 << 16);
-      }
-    };
-    handle_candidates<T>(J, smem, ctab, ws, pass, total, thr_g, id, t, materialize);
-    if (J.trace && active) {
-      materialize();
-      write_trace<T>(J, smem, id - J.trace_base, total, id, t);
-    }
-  }
-}
-
 // One instantiation per (path, precision, row width, mode): random and systematic loops keep only
 // their own state live.
 template <bool SYS>
 __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                               WarpState& ws) {
-  if constexpr (!SYS) {
-    if (sj.k2 == 3) {  // random mode only
-      if (sj.prec == 1)
-        run_tile_bits<double>(sj, smem, ctab, tile, ws);
-      else
-        run_tile_bits<float>(sj, smem, ctab, tile, ws);
-      return;
-    }
-  }
   if (sj.k2 == 1) {
     if (sj.prec == 1)
       run_tile_k2<double, 1, SYS>(sj, smem, ctab, tile, ws);

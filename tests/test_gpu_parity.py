@@ -391,43 +391,6 @@ def test_random_results_do_not_depend_on_the_split():
     assert merge_levels(parts, 10) == whole
 
 
-@pytest.mark.parametrize("prec", ["double", "single"])
-def test_bitset_path_binary_108_sites(prec):
-    """Binary cells above 64 sites in random mode take the bit-set path: every traced configuration
-    has the oracle's ordered bonds and objective, and configuration g is the Philox Fisher-Yates
-    shuffle of the packed initial arrangement with counter g."""
-    import philox_ref
-
-    cfg = cases.fcc32(prec, iterations=20000, seed=5, pair_weights=None, keep=4)
-    cfg["structure"]["supercell"] = [3, 3, 3]
-    cfg["composition"] = {"Ti": 40, "Al": 68}
-    cfg["shell_weights"] = {"1": 1.0, "2": 0.5, "3": 0.25}
-    c, d, pack, sp, bd, ob, ids = cases.trace(cfg, 20000)
-    assert len(d[0].species_packed) == 108 and len(ob) == 20000
-    assert cases.trace_mismatches(d, sp, bd, ob, prec) == []
-    windows = [tuple(w) for w in d[0].windows.tolist()]
-    for g in (0, 1, 777, 19999):
-        conf = d[0].species_packed.tolist()
-        philox_ref.shuffle(conf, windows, cfg["seed"], g, 0)
-        assert conf == sp[g].tolist(), g
-    _, _, recs, lv, info = native_run(cfg)
-    assert info["levels_exact"] and not info["truncated"]
-    for k in range(len(recs["objective"])):
-        o, sro = oracle.evaluate(d[0], recs["species"][k], prec)
-        assert o.tobytes() == recs["objective"][k].tobytes()
-        assert sro.tobytes() == recs["sro"][k].reshape(sro.shape).tobytes()
-
-
-def test_bitset_path_partial_window():
-    """A 60-site window inside a 108-site cell of the same background species (two species overall)."""
-    cfg = cases.fcc32("double", iterations=30000, seed=9, keep=6, pair_weights=None)
-    cfg["structure"]["supercell"] = [3, 3, 3]
-    cfg["composition"] = {"sites": list(range(60)), "Ti": 25, "H": 35}
-    c, d, pack, sp, bd, ob, ids = cases.trace(cfg, 30000)
-    assert len(d[0].species_packed) == 108 and d[0].windows.tolist() != [[0, 108]]
-    assert cases.trace_mismatches(d, sp, bd, ob, "double") == []
-
-
 def test_fast_path_64_sites():
     cfg = cases.fcc32("double", iterations=20000, pair_weights=None)
     cfg["structure"]["supercell"] = [2, 2, 4]
