@@ -529,7 +529,7 @@ using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, 
 
 // The general path runs in sqsg_engine_wide (128 registers); a launch whose jobs all take the binary
 // bit-mask path runs in sqsg_engine (96 registers, 5 CTAs per SM).
-static EngineKernel engine_for(bool all_bitmask) { return all_bitmask ? sqsg_engine : sqsg_engine_wide; }
+static EngineKernel engine_for(bool all_bitmask) { return all_bitmask ? sqsg_engine_mask : sqsg_engine_wide; }
 
 static void configure_kernel(size_t smem) {
   static std::mutex m;
@@ -539,6 +539,8 @@ static void configure_kernel(size_t smem) {
     CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
     CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine_mask, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
     configured = smem;
   }
@@ -556,10 +558,11 @@ static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel k
 static size_t max_dynamic_smem(int dev) {
   int v = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes a{}, b{};
+  cudaFuncAttributes a{}, b{}, c{};
   CUDA_CHECK(cudaFuncGetAttributes(&a, sqsg_engine));
   CUDA_CHECK(cudaFuncGetAttributes(&b, sqsg_engine_wide));
-  return static_cast<size_t>(v) - std::max(a.sharedSizeBytes, b.sharedSizeBytes);
+  CUDA_CHECK(cudaFuncGetAttributes(&c, sqsg_engine_mask));
+  return static_cast<size_t>(v) - std::max({a.sharedSizeBytes, b.sharedSizeBytes, c.sharedSizeBytes});
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1155,7 +1158,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
 // that finishes a job's last tile marks the job's slot done in host-mapped memory; the worker then
 // downloads its records and levels, selects the result set and wakes the waiting caller. A job's
 // result does not depend on what else runs: its tiles and Philox counters depend only on the job.
-// One ring per occupancy level: ring 0 runs sqsg_engine at 5 CTAs per SM and takes binary bit-mask
+// One ring per occupancy level: ring 0 runs sqsg_engine_mask at 5 CTAs per SM and takes binary bit-mask
 // jobs; rings 1-4 run sqsg_engine_wide at 4, 3, 2, 1 CTAs per SM. A job goes to the ring with the
 // largest shared-memory size it fits, i.e. the highest occupancy its data allow.
 constexpr int kBuckets = 5;
@@ -1197,7 +1200,7 @@ struct LaunchSlot {
 // One ring of tiles per shared-memory class; launches of sqsg_engine serve a ring on the SMs that
 // the owner table gives it.
 struct Ring {
-  EngineKernel kernel = nullptr;  // ring 0: sqsg_engine (bit-mask jobs); others: sqsg_engine_wide
+  EngineKernel kernel = nullptr;  // ring 0: sqsg_engine_mask (bit-mask jobs); others: sqsg_engine_wide
   size_t smem = 0;
   uint32_t per_sm = 1;        // resident CTAs per SM at this shared-memory size
   uint64_t published = 0;     // tiles appended so far (the ring's tail)
@@ -1939,7 +1942,7 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     configure_kernel(optin);
     for (int b = 0; b < kBuckets; ++b) {
       Ring& R = S.rings[b];
-      R.kernel = b == 0 ? sqsg_engine : sqsg_engine_wide;
+      R.kernel = b == 0 ? sqsg_engine_mask : sqsg_engine_wide;
       auto fits = [&](size_t smem) {
         int nb = 0;
         CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, R.kernel, kBlock, smem));

@@ -861,7 +861,7 @@ __device__ __forceinline__ unsigned long long claim_live(QueueCtl* q, const vola
 
 // One instantiation per (path, precision, row width, mode): random and systematic loops keep only
 // their own state live.
-template <bool SYS>
+template <bool SYS, bool GENERAL>
 __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                               WarpState& ws) {
   if (sj.k2 == 1) {
@@ -874,6 +874,8 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
       run_tile_k2<double, 2, SYS>(sj, smem, ctab, tile, ws);
     else
       run_tile_k2<float, 2, SYS>(sj, smem, ctab, tile, ws);
+  } else if constexpr (!GENERAL) {
+    return;  // a launch of bit-mask jobs only (the host never gives it others)
   } else if (sj.prec == 1) {
     if (sj.kw == 1)
       run_tile<double, 1, SYS>(sj, smem, ctab, tile, ws);
@@ -892,6 +894,7 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
 // whenever its next tile belongs to another job. In live mode every tile ends with a level flush and
 // a decrement of the job's tile count; the CTA that finishes a job's last tile publishes the job's
 // generation in done[slot] (host-mapped memory).
+template <bool GENERAL>
 __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
                                             uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
                                             unsigned long long* status, volatile uint32_t* done) {
@@ -973,9 +976,9 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
       ws.reset();
     }
     if (sj.mode == 1)
-      dispatch_tile<true>(sj, smem, ctab, tile, ws);
+      dispatch_tile<true, GENERAL>(sj, smem, ctab, tile, ws);
     else
-      dispatch_tile<false>(sj, smem, ctab, tile, ws);
+      dispatch_tile<false, GENERAL>(sj, smem, ctab, tile, ws);
     __syncthreads();  // every thread is done with this tile before s_tile changes
     if (live) {
       flush_levels(ctab, sj);
@@ -1010,13 +1013,20 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
 __global__ void __launch_bounds__(kBlock, kMinBlocks)
     sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                 const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body(jobs, tiles, n_tiles, q, cancel, status, done);
+  engine_body<true>(jobs, tiles, n_tiles, q, cancel, status, done);
+}
+
+// The bit-mask path alone, so that the general path's code does not weigh on its 96 registers.
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
+    sqsg_engine_mask(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
+  engine_body<false>(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
 __global__ void __launch_bounds__(kBlock, kMinBlocksWide)
     sqsg_engine_wide(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                      const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body(jobs, tiles, n_tiles, q, cancel, status, done);
+  engine_body<true>(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
 }  // namespace sqsg
