@@ -861,8 +861,8 @@ __device__ __forceinline__ unsigned long long claim_live(QueueCtl* q, const vola
 
 // One instantiation per (path, precision, row width, mode): random and systematic loops keep only
 // their own state live.
-template <bool SYS, bool GENERAL>
-__device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+template <bool SYS>
+__device__ __forceinline__ void dispatch_mask(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                               WarpState& ws) {
   if (sj.k2 == 1) {
     if (sj.prec == 1)
@@ -874,9 +874,13 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
       run_tile_k2<double, 2, SYS>(sj, smem, ctab, tile, ws);
     else
       run_tile_k2<float, 2, SYS>(sj, smem, ctab, tile, ws);
-  } else if constexpr (!GENERAL) {
-    return;  // a launch of bit-mask jobs only (the host never gives it others)
-  } else if (sj.prec == 1) {
+  }
+}
+
+template <bool SYS>
+__device__ __forceinline__ void dispatch_general(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                                 WarpState& ws) {
+  if (sj.prec == 1) {
     if (sj.kw == 1)
       run_tile<double, 1, SYS>(sj, smem, ctab, tile, ws);
     else
@@ -889,12 +893,26 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
   }
 }
 
+template <bool SYS, bool GENERAL, bool MASK>
+__device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                              WarpState& ws) {
+  if constexpr (MASK) {
+    if (sj.k2 == 1 || sj.k2 == 2) {
+      dispatch_mask<SYS>(sj, smem, ctab, tile, ws);
+      return;
+    }
+  }
+  if constexpr (GENERAL) {  // also correct for bit-mask jobs: their columns and stream exist too
+    dispatch_general<SYS>(sj, smem, ctab, tile, ws);
+  }
+}
+
 // Tiles are taken from q with one atomic per tile. A CTA stages a job's read-only data (cubes,
 // windows, pair stream, packed species, masks) into shared memory with non-multicast bulk copies
 // whenever its next tile belongs to another job. In live mode every tile ends with a level flush and
 // a decrement of the job's tile count; the CTA that finishes a job's last tile publishes the job's
 // generation in done[slot] (host-mapped memory).
-template <bool GENERAL>
+template <bool GENERAL, bool MASK>
 __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
                                             uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
                                             unsigned long long* status, volatile uint32_t* done) {
@@ -976,9 +994,9 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
       ws.reset();
     }
     if (sj.mode == 1)
-      dispatch_tile<true, GENERAL>(sj, smem, ctab, tile, ws);
+      dispatch_tile<true, GENERAL, MASK>(sj, smem, ctab, tile, ws);
     else
-      dispatch_tile<false, GENERAL>(sj, smem, ctab, tile, ws);
+      dispatch_tile<false, GENERAL, MASK>(sj, smem, ctab, tile, ws);
     __syncthreads();  // every thread is done with this tile before s_tile changes
     if (live) {
       flush_levels(ctab, sj);
@@ -1007,26 +1025,28 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
   }
 }
 
-// Two register budgets of the same engine: 96 registers (5 CTAs per SM) for the binary bit-mask
-// path, whose state is small and whose shared-memory footprint allows 5 CTAs; 128 registers for the
-// general path, whose pair loop spills at 96 and whose shared memory allows at most 4 CTAs anyway.
+// The same engine compiled three ways. sqsg_engine_mask: the binary bit-mask path alone at 96
+// registers (5 CTAs per SM; without the general path's code nothing forces spills).
+// sqsg_engine_wide: the general path alone at 128 registers (its pair loop spills at 96 and its
+// shared memory allows at most 4 CTAs anyway); a bit-mask job given to it runs the general path,
+// which holds all its data too and gives the same result. sqsg_engine: both paths at 96 registers,
+// for callers that launch one kernel for any job.
 __global__ void __launch_bounds__(kBlock, kMinBlocks)
     sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                 const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body<true>(jobs, tiles, n_tiles, q, cancel, status, done);
+  engine_body<true, true>(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
-// The bit-mask path alone, so that the general path's code does not weigh on its 96 registers.
 __global__ void __launch_bounds__(kBlock, kMinBlocks)
     sqsg_engine_mask(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                      const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body<false>(jobs, tiles, n_tiles, q, cancel, status, done);
+  engine_body<false, true>(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
 __global__ void __launch_bounds__(kBlock, kMinBlocksWide)
     sqsg_engine_wide(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                      const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body<true>(jobs, tiles, n_tiles, q, cancel, status, done);
+  engine_body<true, false>(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
 }  // namespace sqsg
