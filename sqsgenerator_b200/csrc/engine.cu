@@ -459,16 +459,19 @@ struct Workspace {
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   DevBuf blob, records, counters, levels, tiles, jobs, queue, status, trace_sp, trace_bd, trace_obj, trace_id;
   SelectScratch select;
-  int32_t* ctrl_host = nullptr;  // mapped pinned: [0] = cancel
-  int32_t* ctrl_dev = nullptr;
+  // Cancellation flag in device memory (CTAs read it once per tile from L2; a flag in mapped host
+  // memory cost a PCIe round trip per tile, queued across hundreds of CTAs), raised by a copy on
+  // the monitor stream from a pinned word holding 1.
+  int32_t* cancel_dev = nullptr;
+  int32_t* one_host = nullptr;
   explicit Workspace(int dev) : device(dev) {
     CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CUDA_CHECK(cudaStreamCreateWithFlags(&monitor, cudaStreamNonBlocking));
     CUDA_CHECK(cudaEventCreate(&ev_start));
     CUDA_CHECK(cudaEventCreate(&ev_stop));
-    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&ctrl_host), 64, cudaHostAllocMapped));
-    CUDA_CHECK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctrl_dev), ctrl_host, 0));
-    std::memset(ctrl_host, 0, 64);
+    CUDA_CHECK(cudaMalloc(reinterpret_cast<void**>(&cancel_dev), 256));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&one_host), 64, cudaHostAllocDefault));
+    one_host[0] = 1;
   }
   ~Workspace() {
     select.release();
@@ -476,7 +479,8 @@ struct Workspace {
     if (monitor) cudaStreamDestroy(monitor);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
-    if (ctrl_host) cudaFreeHost(ctrl_host);
+    if (cancel_dev) cudaFree(cancel_dev);
+    if (one_host) cudaFreeHost(one_host);
   }
 };
 
@@ -945,7 +949,8 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     CUDA_CHECK(cudaMemsetAsync(ws->levels.p, 0, nj * kLevelSlots * sizeof(LevelSlot), ws->stream));
     CUDA_CHECK(cudaMemsetAsync(ws->queue.p, 0, sizeof(QueueCtl), ws->stream));
     CUDA_CHECK(cudaMemsetAsync(ws->status.p, 0, sizeof(unsigned long long), ws->stream));
-    ws->ctrl_host[0] = 0;
+    CUDA_CHECK(cudaMemsetAsync(ws->cancel_dev, 0, sizeof(int32_t), ws->stream));
+    bool cancel_sent = false;
 
     bool all_bitmask = true;
     for (size_t j = 0; j < nj; ++j) all_bitmask = all_bitmask && pjs[j].desc.k2 != 0;
@@ -955,7 +960,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     if (!tiles.empty()) {
       kernel<<<grid, kBlock, smem, ws->stream>>>(
           static_cast<const JobDesc*>(ws->jobs.p), static_cast<const Tile*>(ws->tiles.p),
-          static_cast<uint32_t>(tiles.size()), static_cast<QueueCtl*>(ws->queue.p), ws->ctrl_dev,
+          static_cast<uint32_t>(tiles.size()), static_cast<QueueCtl*>(ws->queue.p), ws->cancel_dev,
           static_cast<unsigned long long*>(ws->status.p), nullptr);
       CUDA_CHECK(cudaGetLastError());
     }
@@ -1003,7 +1008,11 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
           if (srcs[j]->callback(&st, srcs[j]->user) != 0) stop = true;
         }
       }
-      if (stop) ws->ctrl_host[0] = 1;
+      if (stop && !cancel_sent) {
+        CUDA_CHECK(cudaMemcpyAsync(ws->cancel_dev, ws->one_host, sizeof(int32_t), cudaMemcpyHostToDevice,
+                                   ws->monitor));
+        cancel_sent = true;
+      }
     }
     CUDA_CHECK(cudaGetLastError());
     float ms = 0.f;
