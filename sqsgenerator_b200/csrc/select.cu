@@ -56,7 +56,7 @@ constexpr size_t kBounceBytes = 32u << 20;
 // Device-to-host copy into pageable memory. Large copies go through two pinned buffers: the copy
 // engine fills one while the host drains the other (several times the driver's pageable rate).
 void copy_out(SelectScratch& S, cudaStream_t st, void* dst, const void* src, size_t bytes) {
-  if (bytes < (4u << 20)) {
+  if (bytes < (64u << 10)) {
     SEL_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
     return;
   }
