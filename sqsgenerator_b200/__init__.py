@@ -7,11 +7,13 @@ the optimisation loop runs in hand-written sm_100a CUDA kernels behind the C ABI
 from .config import parse_config
 from .core import (IterationMode, LogLevel, ParseError, ParseErrorCode, Prec, ShellRadiiDetection, SqsConfiguration,
                    SqsResult, SqsResultPack, SqsResultSplit, SqsStatistics, Structure, SublatticeMode)
+from .io import dump_result_pack, load_result_pack
 from .optimize import optimize, prepare
 from .serve import Server
 
 __all__ = [
-    "parse_config", "optimize", "prepare", "IterationMode", "LogLevel", "ParseError", "ParseErrorCode", "Prec",
+    "parse_config", "optimize", "prepare", "load_result_pack", "dump_result_pack", "IterationMode", "LogLevel",
+    "ParseError", "ParseErrorCode", "Prec",
     "ShellRadiiDetection", "SqsConfiguration", "SqsResult", "SqsResultPack", "SqsResultSplit", "SqsStatistics",
     "Structure", "SublatticeMode", "Server",
 ]

@@ -303,8 +303,26 @@ class SqsResultPack:
     def __len__(self) -> int:
         return len(self.results)
 
+    def __getitem__(self, index):
+        return self.results[index]
+
+    def num_objectives(self) -> int:
+        return len(self.results)
+
     def num_results(self) -> int:
         return sum(len(v) for _, v in self.results)
+
+    def bytes(self) -> bytes:
+        """The msgpack document of the pack (``pack.bytes()`` of the reference, io/json.h:264-275)."""
+        from .io import dump_result_pack
+
+        return dump_result_pack(self)
+
+    @staticmethod
+    def from_bytes(data: bytes, prec: Prec = Prec.single) -> "SqsResultPack":
+        from .io import load_result_pack
+
+        return load_result_pack(data, prec)
 
     def best(self):
         if not self.results:
