@@ -263,8 +263,13 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
         }
         shell_end[sh] = static_cast<uint32_t>(k2_entries.size() / 4);
       }
+      uint32_t ones = 0;
+      for (uint32_t x = 0; x < N; ++x) ones += sl.species[x] != 0 ? 1u : 0u;
       // degree classes: sites grouped by their number of shell-s pairs (either end), so that
-      // n01 + n10 = sum_x b_x deg_s(x) - 2 n11 costs one popcount per class
+      // n01 + n10 = sum_x b_x deg_s(x) - 2 n11 costs one popcount per class. The number of ones is
+      // the same in every configuration, so the largest class c* needs none: the sum is
+      // deg_c* * ones + sum over the other classes of (deg_c - deg_c*) * popc (mod 2^32), and a
+      // lattice whose sites all have one degree (every Bravais lattice) needs no popcount at all.
       for (uint32_t sh = 0; sh < sl.n_shells; ++sh) {
         std::vector<uint32_t> deg(N, 0);
         for (uint32_t i = 0; i < N; ++i) {
@@ -273,20 +278,26 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
           for (uint32_t j = 0; j < N; ++j)
             if ((m >> (N - 1 - j)) & 1ull) deg[j]++;
         }
-        std::map<uint32_t, unsigned long long> classes;
-        for (uint32_t x = 0; x < N; ++x)
-          if (deg[x]) classes[deg[x]] |= 1ull << (N - 1 - x);
+        std::map<uint32_t, unsigned long long> classes;  // degree 0 included: the classes cover all sites
+        for (uint32_t x = 0; x < N; ++x) classes[deg[x]] |= 1ull << (N - 1 - x);
+        uint32_t dstar = 0;
+        int best = -1;
+        for (auto& [dv, m] : classes)
+          if (__builtin_popcountll(m) > best) best = __builtin_popcountll(m), dstar = dv;
         const uint32_t d0 = static_cast<uint32_t>(k2_entries.size() / 4);
         for (auto& [dv, m] : classes) {
+          if (dv == dstar) continue;
           k2_entries.push_back(static_cast<uint32_t>(m));
           k2_entries.push_back(static_cast<uint32_t>(m >> 32));
-          k2_entries.push_back(dv);
+          k2_entries.push_back(dv - dstar);
           k2_entries.push_back(0);
         }
         k2_shells.push_back(ps[sh]);
         k2_shells.push_back(shell_end[sh]);
         k2_shells.push_back(d0);
         k2_shells.push_back(static_cast<uint32_t>(k2_entries.size() / 4));
+        k2_shells.push_back(dstar * ones);
+        for (int pad = 0; pad < 3; ++pad) k2_shells.push_back(0);
       }
       // neighbour masks indexed by the bit position p = N-1-i of site i, for the per-configuration
       // loop over the set bits of the minority species
@@ -297,8 +308,6 @@ static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
           k2_nbp.push_back(static_cast<uint32_t>(m));
           if (slots == 64) k2_nbp.push_back(static_cast<uint32_t>(m >> 32));
         }
-      uint32_t ones = 0;
-      for (uint32_t x = 0; x < N; ++x) ones += sl.species[x] != 0 ? 1u : 0u;
       P.k2_zeros = 2 * ones > N ? 1u : 0u;
     }
     // blob section layout: cubes | windows | species codes | binary-path masks | pair stream. The

@@ -103,7 +103,8 @@ struct PartDesc {
   // binary fast path (K == 2, N <= 64): per (shell, site) neighbour masks, see run_tile_k2
   uint32_t k2_off;        // entries: uint4 {mask lo, mask hi, site | shell << 8, popcount}
   uint32_t k2_entries;
-  uint32_t k2_shell_off;  // S x (pairs in shell, end of its entries, degree classes [begin, end))
+  uint32_t k2_shell_off;  // S x (pairs in shell, end of its entries, degree classes [begin, end),
+                          //      degree sum of the largest class, 3 x 0)
   uint32_t k2_binom_off;  // blob offset (global, not staged) of C(m, j), m <= window, j <= ones
   uint32_t k2_nbp_off;    // neighbour masks by bit position: u32 [S][32] (N <= 32) or uint2 [S][64]
   uint32_t k2_zeros;      // 1: count over the zeros (species 0 is the minority), else over the ones

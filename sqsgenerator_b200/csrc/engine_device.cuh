@@ -602,14 +602,15 @@ template <int W> struct Word;
 template <> struct Word<1> {
   using type = uint32_t;
   static __device__ __forceinline__ uint32_t pc(type v, uint32_t lo, uint32_t) { return __popc(v & lo); }
-  static __device__ __forceinline__ int ctz(type v) { return __ffs(static_cast<int>(v)) - 1; }
+  // trailing zeros of v != 0 as one popcount (a find-first-set is a bit reverse plus a leading-zero count)
+  static __device__ __forceinline__ int ctz(type v) { return __popc(~v & (v - 1)); }
 };
 template <> struct Word<2> {
   using type = unsigned long long;
   static __device__ __forceinline__ uint32_t pc(type v, uint32_t lo, uint32_t hi) {
     return __popc(static_cast<uint32_t>(v) & lo) + __popc(static_cast<uint32_t>(v >> 32) & hi);
   }
-  static __device__ __forceinline__ int ctz(type v) { return __ffsll(static_cast<long long>(v)) - 1; }
+  static __device__ __forceinline__ int ctz(type v) { return __popcll(~v & (v - 1)); }  // v != 0
 };
 
 template <class V> __device__ __forceinline__ V low_mask(uint32_t n) {
@@ -650,8 +651,9 @@ __device__ __forceinline__ uint32_t k2_nbp_count(const uint8_t* tab, int s, int 
 
 // What the objective needs per shell: n11, n01 + n10 and n00. With deg_s(x) the number of shell-s
 // pairs at site x, sum_x b_x deg_s(x) = 2 n11 + n01 + n10 (the degree classes, sites of equal degree
-// as one mask, give it in one popcount per class) and sum_x deg_s(x) = 2 P_s, so one count of the
-// pairs inside the minority species fixes all three.
+// as one mask, give it in one popcount per class but the largest, whose share follows from the fixed
+// number of ones) and sum_x deg_s(x) = 2 P_s, so one count of the pairs inside the minority species
+// fixes all three.
 
 template <class T>
 __device__ __forceinline__ T k2_term(T obj, uint32_t n, const T* f, const T* w, const T* tg, uint32_t d) {
@@ -676,8 +678,8 @@ __device__ __forceinline__ void k2_materialize(uint8_t* smem, const PartDesc& P,
   uint32_t e0 = 0;
   for (uint32_t s = 0; s < P.n_shells; ++s) {
     uint32_t n00, n01, n10, n11;
-    k2_counts<V, W>(ent, e0, sh[4 * s + 1], sh[4 * s], v, n00, n01, n10, n11);
-    e0 = sh[4 * s + 1];
+    k2_counts<V, W>(ent, e0, sh[8 * s + 1], sh[8 * s], v, n00, n01, n10, n11);
+    e0 = sh[8 * s + 1];
     hist[(s * 2 + 0) * kBlock] = n00 | (n01 << 16);
     hist[(s * 2 + 1) * kBlock] = n10 | (n11 << 16);
   }
@@ -767,7 +769,7 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
       const V vv = P.k2_zeros ? ~v : v;
       V x = vv & low_mask<V>(N);
       uint32_t a[kK2MaxShells] = {};
-      while (x) {
+      while (x) {  // the loop-carried chain (x &= x - 1) stays off the popcount unit
         const int bp = Word<W>::ctz(x);
         x &= x - 1;
 #pragma unroll
@@ -777,12 +779,12 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
 #pragma unroll
       for (int s = 0; s < kK2MaxShells; ++s) {
         if (s >= static_cast<int>(S)) break;
-        uint32_t DE = 0;  // sum over the ones of their shell-s degree: 2 n11 + n01 + n10
-        for (uint32_t e = sh[4 * s + 2]; e < sh[4 * s + 3]; ++e) {
+        uint32_t DE = sh[8 * s + 4];  // sum over the ones of their shell-s degree: 2 n11 + n01 + n10
+        for (uint32_t e = sh[8 * s + 2]; e < sh[8 * s + 3]; ++e) {
           const uint4 q = ent[e];
           DE += q.z * Word<W>::pc(v, q.x, q.y);
         }
-        const uint32_t ps = sh[4 * s];
+        const uint32_t ps = sh[8 * s];
         uint32_t n00, nx, n11;
         if (P.k2_zeros) {
           n00 = a[s];
