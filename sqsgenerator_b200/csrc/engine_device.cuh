@@ -649,6 +649,17 @@ __device__ __forceinline__ uint32_t k2_nbp_count(const uint8_t* tab, int s, int 
   }
 }
 
+// Pairs inside the minority species (the set bits x of vv), shell by shell, for NS shells.
+template <class V, int W, int NS>
+__device__ __forceinline__ void k2_minority_pairs(const uint8_t* nbp, V vv, V x, uint32_t* a) {
+  while (x) {  // the loop-carried chain (x &= x - 1) stays off the popcount unit
+    const int bp = Word<W>::ctz(x);
+    x &= x - 1;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) a[s] += k2_nbp_count<V, W>(nbp, s, bp, vv);
+  }
+}
+
 // What the objective needs per shell: n11, n01 + n10 and n00. With deg_s(x) the number of shell-s
 // pairs at site x, sum_x b_x deg_s(x) = 2 n11 + n01 + n10 (the degree classes, sites of equal degree
 // as one mask, give it in one popcount per class but the largest, whose share follows from the fixed
@@ -769,12 +780,12 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
       const V vv = P.k2_zeros ? ~v : v;
       V x = vv & low_mask<V>(N);
       uint32_t a[kK2MaxShells] = {};
-      while (x) {  // the loop-carried chain (x &= x - 1) stays off the popcount unit
-        const int bp = Word<W>::ctz(x);
-        x &= x - 1;
-#pragma unroll
-        for (int s = 0; s < kK2MaxShells; ++s)
-          if (s < static_cast<int>(S)) a[s] += k2_nbp_count<V, W>(part + P.k2_nbp_off, s, bp, vv);
+      const uint8_t* nbp = part + P.k2_nbp_off;
+      switch (S) {  // one copy of the loop per shell count: no predicated work for absent shells
+        case 1: k2_minority_pairs<V, W, 1>(nbp, vv, x, a); break;
+        case 2: k2_minority_pairs<V, W, 2>(nbp, vv, x, a); break;
+        case 3: k2_minority_pairs<V, W, 3>(nbp, vv, x, a); break;
+        default: k2_minority_pairs<V, W, 4>(nbp, vv, x, a); break;
       }
 #pragma unroll
       for (int s = 0; s < kK2MaxShells; ++s) {
