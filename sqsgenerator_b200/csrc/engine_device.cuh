@@ -389,6 +389,29 @@ struct WarpState {
   }
 };
 
+// Per-warp level accumulators of the bit-mask path, indexed by position in the warp list: count,
+// low and high checksum halves of the configurations kept at list[i] (3 x 32 words per warp). While
+// the list does not change, a kept value is at the position its lower-bound search found, so each
+// lane adds itself there with three shared-memory atomics instead of the warp looping over distinct
+// values; before the list changes and at the end of every tile the warp moves them into the CTA table.
+static __shared__ uint32_t s_wacc[kBlock / 32 * 96];
+
+__device__ __forceinline__ uint32_t* warp_acc() { return s_wacc + (threadIdx.x >> 5) * 96; }
+
+__device__ __forceinline__ void warp_acc_flush(const WarpState& ws, LevelSlot* ctab, const JobDesc& J) {
+  __syncwarp();
+  uint32_t* acc = warp_acc();
+  const int lane = threadIdx.x & 31;
+  const uint32_t c = acc[lane];
+  if (c) {
+    cta_level_add(ctab, J, ord_bits(ws.list), c, acc[32 + lane], acc[64 + lane]);
+    acc[lane] = 0;
+    acc[32 + lane] = 0;
+    acc[64 + lane] = 0;
+  }
+  __syncwarp();
+}
+
 template <class T>
 __device__ __forceinline__ void write_record(const JobDesc& J, uint8_t* smem, uint64_t idx, T total, uint64_t id,
                                              int t) {
@@ -431,7 +454,9 @@ struct NoPrep {
 
 // `prep` runs right before a record is written (the binary path materialises the lane's species and
 // bond counts in shared memory only then).
-template <class T, class Prep = NoPrep>
+// ACC (bit-mask path): kept configurations go to the warp's level accumulators while the list is
+// unchanged; otherwise straight to the CTA table.
+template <class T, bool ACC = false, class Prep = NoPrep>
 __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, WarpState& ws,
                                                   bool pass, T total, T thr_g, uint64_t id, int t,
                                                   const Prep& prep = Prep()) {
@@ -443,8 +468,9 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
   // Membership: the lower bound of each lane's value in the ascending list (one entry per lane),
   // found by a five-step shuffle search; then one insertion per distinct new value, lane order.
   bool fresh = pass && v_mine < ws.list_thr;
-  if (__any_sync(0xffffffffu, fresh)) {
-    int lo = 0;
+  int lo = 0;
+  bool moved = false;
+  if (ACC || __any_sync(0xffffffffu, fresh)) {
 #pragma unroll
     for (int step = 16; step > 0; step >>= 1) {
       const double e = __shfl_sync(0xffffffffu, ws.list, lo + step - 1);
@@ -453,6 +479,10 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
     const double at = __shfl_sync(0xffffffffu, ws.list, lo);  // every lane takes part in the shuffle
     fresh = fresh && at != v_mine;
     unsigned fm = __ballot_sync(0xffffffffu, fresh);
+    if (ACC && fm) {  // list positions are about to move
+      warp_acc_flush(ws, ctab, J);
+      moved = true;
+    }
     while (fm) {
       const double v = __shfl_sync(0xffffffffu, v_mine, __ffs(fm) - 1);
       fm &= ~__ballot_sync(0xffffffffu, v_mine == v);  // lanes with the same value: one insertion
@@ -484,10 +514,19 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
   const bool keep_it = pass && v_mine <= bound;
   const unsigned km = __ballot_sync(0xffffffffu, keep_it);
   if (!km) return;
-  // objective levels: one shared-memory update per distinct value per warp. The reductions run with
-  // the full warp mask, one distinct value per round (a reduction whose mask differs between the
-  // threads executing it is not allowed).
-  {
+  if (ACC && !moved) {
+    // no insertion this step: a kept value (<= the (keep+1)-th entry) is in the list at lo
+    if (keep_it) {
+      const unsigned long long h = mix64(id);
+      uint32_t* acc = warp_acc();
+      atomicAdd(&acc[lo], 1u);
+      atomicAdd(&acc[32 + lo], static_cast<unsigned>(h));
+      atomicAdd(&acc[64 + lo], static_cast<unsigned>(h >> 32));
+    }
+  } else {
+    // objective levels: one shared-memory update per distinct value per warp. The reductions run
+    // with the full warp mask, one distinct value per round (a reduction whose mask differs between
+    // the threads executing it is not allowed).
     const unsigned long long mykey = ord_bits(v_mine);
     const unsigned long long h = mix64(id);
     unsigned pending = km;
@@ -816,8 +855,8 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
     const bool pass = active && static_cast<double>(total) <= bound;
     const uint64_t id = tile.start + my_off + it;
     const V vv = v;
-    handle_candidates<T>(J, smem, ctab, ws, pass, total, thr_g, id, t,
-                         [&]() { k2_materialize<V, W>(smem, P, t, vv); });
+    handle_candidates<T, true>(J, smem, ctab, ws, pass, total, thr_g, id, t,
+                               [&]() { k2_materialize<V, W>(smem, P, t, vv); });
     if (J.trace && active) {
       k2_materialize<V, W>(smem, P, t, v);
       write_trace<T>(J, smem, id - J.trace_base, total, id, t);
@@ -829,6 +868,7 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
       v = (v & ~wmask) | ((nx << wshift) & wmask);
     }
   }
+  warp_acc_flush(ws, ctab, J);  // the CTA table is complete for this tile
 }
 
 // ------------------------------------------------------------------------------ persistent kernel
@@ -941,6 +981,8 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
     s_fail = 0;
   }
   for (int i = threadIdx.x; i < kCtaLevelSlots; i += kBlock) ctab[i] = LevelSlot{0ull, 0ull, 0u, 0u};
+  if constexpr (MASK)
+    for (int i = threadIdx.x; i < kBlock / 32 * 96; i += kBlock) s_wacc[i] = 0u;
   const bool live = q->capacity != 0;
   int cur = -1;
   uint32_t cur_gen = 0;
