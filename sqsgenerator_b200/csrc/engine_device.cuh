@@ -479,10 +479,8 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
     const double at = __shfl_sync(0xffffffffu, ws.list, lo);  // every lane takes part in the shuffle
     fresh = fresh && at != v_mine;
     unsigned fm = __ballot_sync(0xffffffffu, fresh);
-    if (ACC && fm) {  // list positions are about to move
-      warp_acc_flush(ws, ctab, J);
-      moved = true;
-    }
+    moved = fm != 0;
+    if (ACC && moved) warp_acc_flush(ws, ctab, J);  // list positions are about to move
     while (fm) {
       const double v = __shfl_sync(0xffffffffu, v_mine, __ffs(fm) - 1);
       fm &= ~__ballot_sync(0xffffffffu, v_mine == v);  // lanes with the same value: one insertion
@@ -497,7 +495,7 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
       }
     }
   }
-  if (lane == 0) {
+  if (lane == 0 && moved) {  // the bounds only change with the list
     const unsigned long long ot = ord_bits(ws.list_thr);
     if (ot < ws.published_thr) {
       atomicMin(&J.counters[kThreshold], ot);
