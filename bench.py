@@ -105,15 +105,59 @@ def mixed_jobs(n: int, seed: int = 2026, rate: float = 200.0, budget=(1e5, 1e8))
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML read every 5 ms from a
+    thread, with one sample taken on entry and one on exit so that even a region of a few
+    milliseconds has two; nvidia-smi at 200 ms when NVML is not importable. Read-only."""
+
+    # NVML clocks-event reason bits (nvml.h): sw power cap, hw slowdown, sw thermal, hw thermal
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device: int):
-        self.path = tempfile.mktemp(suffix=".csv")
-        self.proc = None
         self.device = device
+        self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
+        self.nvml = None
+        self.proc = None
+        self.path = None
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:  # noqa: BLE001 — fall back to the NVML index
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _sample(self):
+        nv, h = self.nvml
+        try:
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                              float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)), int(get_reasons(h))))
+        except Exception:  # noqa: BLE001 — a failed read is a missing sample
+            pass
+
+    def _loop(self):
+        while not self._stop.wait(0.005):
+            self._sample()
 
     def __enter__(self):
         try:
+            self.nvml = self._handle()
+        except Exception:  # noqa: BLE001
+            self.nvml = None
+        if self.nvml:
+            self._sample()
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+            return self
+        try:
+            self.path = tempfile.mktemp(suffix=".csv")
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={SMI_FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
@@ -123,6 +167,11 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self._sample()
+            self._stop.set()
+            self._thread.join(timeout=5)
+            return
         if self.proc:
             self.proc.terminate()
             try:
@@ -130,24 +179,22 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
             self.f.close()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in open(self.path):
+                r = [p.strip() for p in line.split(",")]
+                if len(r) >= 9 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                    bits = sum(self.REASON_BITS[names[k]] for k in range(4) if r[5 + k].lower() == "active")
+                    self.rows.append((float(r[1]), float(r[2]), bits))
 
     def summary(self):
-        if not self.proc or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        if not rows:
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
-        loaded = [v for v in sm if v > 0.5 * (max(mx) if mx else 1)] or sm
-        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
-                "samples": len(rows), "reasons": reasons}
+        sm = [r[0] for r in self.rows]
+        mx = max(r[1] for r in self.rows)
+        reasons = sorted({n for r in self.rows for n, b in self.REASON_BITS.items() if r[2] & b})
+        loaded = [v for v in sm if v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "samples": len(self.rows),
+                "source": "nvml" if self.nvml else "nvidia-smi", "reasons": reasons}
 
 
 def cpu_sample(seconds: float, keep: int, workload: str = "systematic"):
