@@ -686,10 +686,13 @@ __device__ __forceinline__ uint32_t k2_nbp_count(const uint8_t* tab, int s, int 
   }
 }
 
-// Pairs inside the minority species (the set bits x of vv), shell by shell, for NS shells.
+// Pairs inside the minority species (the nb set bits x of vv), shell by shell, for NS shells. Every
+// configuration of a job has the same nb, so the loop is counted and unrolled: the scheduler sees
+// several bits' loads and popcounts at once.
 template <class V, int W, int NS>
-__device__ __forceinline__ void k2_minority_pairs(const uint8_t* nbp, V vv, V x, uint32_t* a) {
-  while (x) {  // the loop-carried chain (x &= x - 1) stays off the popcount unit
+__device__ __forceinline__ void k2_minority_pairs(const uint8_t* nbp, V vv, V x, uint32_t* a, int nb) {
+#pragma unroll 4
+  for (int k = 0; k < nb; ++k) {  // the loop-carried chain (x &= x - 1) stays off the popcount unit
     const int bp = Word<W>::ctz(x);
     x &= x - 1;
 #pragma unroll
@@ -756,6 +759,9 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
   V v0 = 0;  // the packed initial arrangement
   for (uint32_t x = 0; x < N; ++x)
     if (part[P.species_off + x]) v0 |= V(1) << (N - 1 - x);
+  // minority sites: the same number in every configuration (shuffles keep the composition)
+  int nb = 0;
+  for (V y = (P.k2_zeros ? ~v0 : v0) & low_mask<V>(N); y; y &= y - 1) ++nb;
   V v = v0;
   uint32_t wn = 0, wshift = 0;
   V wmask = 0;
@@ -819,10 +825,10 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
       uint32_t a[kK2MaxShells] = {};
       const uint8_t* nbp = part + P.k2_nbp_off;
       switch (S) {  // one copy of the loop per shell count: no predicated work for absent shells
-        case 1: k2_minority_pairs<V, W, 1>(nbp, vv, x, a); break;
-        case 2: k2_minority_pairs<V, W, 2>(nbp, vv, x, a); break;
-        case 3: k2_minority_pairs<V, W, 3>(nbp, vv, x, a); break;
-        default: k2_minority_pairs<V, W, 4>(nbp, vv, x, a); break;
+        case 1: k2_minority_pairs<V, W, 1>(nbp, vv, x, a, nb); break;
+        case 2: k2_minority_pairs<V, W, 2>(nbp, vv, x, a, nb); break;
+        case 3: k2_minority_pairs<V, W, 3>(nbp, vv, x, a, nb); break;
+        default: k2_minority_pairs<V, W, 4>(nbp, vv, x, a, nb); break;
       }
 #pragma unroll
       for (int s = 0; s < kK2MaxShells; ++s) {
