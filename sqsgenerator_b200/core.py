@@ -132,6 +132,17 @@ class Structure:
             raise ValueError("Species size mismatch")
         return Structure(self.lattice.copy(), self.frac_coords.copy(), list(species), self.pbc)
 
+    def bytes(self) -> bytes:
+        from .io import dump_structure
+
+        return dump_structure(self)
+
+    @staticmethod
+    def from_bytes(data: bytes, prec: Prec = Prec.double) -> "Structure":
+        from .io import load_structure
+
+        return load_structure(data, prec)
+
 
 @dataclass
 class Sublattice:
@@ -164,6 +175,22 @@ class SqsConfiguration:
     def structure(self) -> Structure:
         a, b, c = self.supercell
         return self.structure_config.supercell(a, b, c)
+
+    def bytes(self) -> bytes:
+        from .io import dump_configuration
+
+        return dump_configuration(self)
+
+    def json(self) -> str:
+        from .io import configuration_json
+
+        return configuration_json(self)
+
+    @staticmethod
+    def from_bytes(data: bytes, prec: Prec = Prec.single) -> "SqsConfiguration":
+        from .io import load_configuration
+
+        return load_configuration(data, prec)
 
 
 @dataclass

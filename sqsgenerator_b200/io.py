@@ -14,10 +14,14 @@ The reference stores a result pack as the msgpack encoding of one JSON document
 - cubes of the configuration (prefactors, pair weights, targets) are nested ``[S][K][K]`` lists.
 
 ``dump_result_pack`` writes that document; ``load_result_pack`` reads it back into a
-``SqsResultPack`` (the precision is not stored, as in the reference, and is passed in).
+``SqsResultPack`` (the precision is not stored, as in the reference, and is passed in). Structures and
+configurations have the same ``bytes()`` / ``from_bytes`` pair, and configurations a compact
+``json()``, with the documents of ``io/json.h:138-212``. Object keys are written sorted, as
+``nlohmann::json`` keeps them.
 """
 from __future__ import annotations
 
+import json
 import os
 from typing import Any
 
@@ -126,9 +130,62 @@ def pack_to_doc(pack: SqsResultPack) -> dict:
     }
 
 
+def _sorted(doc):
+    """Object keys in sorted order at every level, as nlohmann::json (a std::map) writes them."""
+    if isinstance(doc, dict):
+        return {k: _sorted(doc[k]) for k in sorted(doc)}
+    if isinstance(doc, list):
+        return [_sorted(x) for x in doc]
+    return doc
+
+
+def _pack(doc) -> bytes:
+    return msgpack.packb(_sorted(doc), use_bin_type=True)
+
+
+def _unpack(data) -> dict:
+    return msgpack.unpackb(bytes(data), raw=False, strict_map_key=False)
+
+
+def structure_to_doc(s: Structure) -> dict:
+    """``adl_serializer<core::structure<T>>`` (include/sqsgen/io/json.h:138-156)."""
+    return {"lattice": np.asarray(s.lattice).tolist(), "species": [int(z) for z in s.species],
+            "frac_coords": np.asarray(s.frac_coords).tolist(), "pbc": [bool(x) for x in s.pbc]}
+
+
+def structure_from_doc(doc: dict, prec: Prec) -> Structure:
+    T = dtype_of(prec)
+    return Structure(np.asarray(doc["lattice"], dtype=T), np.asarray(doc["frac_coords"], dtype=T).reshape(-1, 3),
+                     [int(z) for z in doc["species"]], tuple(bool(x) for x in doc["pbc"]))
+
+
+def dump_structure(s: Structure) -> bytes:
+    """``Structure.bytes()`` of the reference (python/extension/sqsgen.cpp:182)."""
+    return _pack(structure_to_doc(s))
+
+
+def load_structure(data: bytes, prec: Prec = Prec.double) -> Structure:
+    return structure_from_doc(_unpack(data), prec)
+
+
+def dump_configuration(c: SqsConfiguration) -> bytes:
+    """``SqsConfiguration.bytes()`` of the reference (python/extension/sqsgen.cpp:222)."""
+    return _pack(config_to_doc(c))
+
+
+def configuration_json(c: SqsConfiguration) -> str:
+    """``SqsConfiguration.json()`` of the reference: the compact dump, keys sorted
+    (python/extension/sqsgen.cpp:223-227)."""
+    return json.dumps(_sorted(config_to_doc(c)), separators=(",", ":"))
+
+
+def load_configuration(data: bytes, prec: Prec = Prec.single) -> SqsConfiguration:
+    return config_from_doc(_unpack(data), prec)
+
+
 def dump_result_pack(pack: SqsResultPack, path: str | os.PathLike | None = None) -> bytes:
     """The msgpack bytes of the pack's document; also written to ``path`` when given."""
-    data = msgpack.packb(pack_to_doc(pack), use_bin_type=True)
+    data = _pack(pack_to_doc(pack))
     if path is not None:
         with open(path, "wb") as f:
             f.write(data)
@@ -141,7 +198,7 @@ def load_result_pack(data: bytes | str | os.PathLike, prec: Prec = Prec.single) 
     if not isinstance(data, (bytes, bytearray)):
         with open(data, "rb") as f:
             data = f.read()
-    doc = msgpack.unpackb(data, raw=False, strict_map_key=False)
+    doc = _unpack(data)
     config = config_from_doc(doc["config"], prec)
     parts = prepare(config)
     T = dtype_of(config.prec)

@@ -1,4 +1,4 @@
-"""Result packs written and read in the reference's msgpack document layout.
+"""Result packs, configurations and structures written and read in the reference's msgpack layout.
 
 The CPU tests build packs from synthetic results (species drawn from the configuration's composition,
 random SRO cubes) and check the round trip and the document layout of include/sqsgen/io/json.h:120-287.
@@ -154,3 +154,38 @@ def test_structure_pack_io(prec):
         np.testing.assert_allclose(sa.lattice, sb.lattice)
         np.testing.assert_allclose(sa.frac_coords, sb.frac_coords)
         assert list(sa.species) == list(sb.species)
+
+
+@pytest.mark.parametrize("make", [cases.fcc32, cases.rocksalt_split])
+def test_configuration_bytes_and_json(make):
+    import json
+
+    c = S.parse_config(make("double"))
+    back = S.SqsConfiguration.from_bytes(c.bytes(), S.Prec.double)
+    assert back.sublattice_mode == c.sublattice_mode and back.iteration_mode == c.iteration_mode
+    assert back.supercell == tuple(c.supercell) and back.keep == c.keep and back.seed == list(c.seed)
+    assert [sl.sites for sl in back.composition] == [sorted(sl.sites) for sl in c.composition]
+    assert [sl.composition for sl in back.composition] == [sl.composition for sl in c.composition]
+    for x, y in zip(back.target_objective, c.target_objective):
+        np.testing.assert_array_equal(x, y)
+    doc = json.loads(c.json())
+    assert list(doc) == sorted(doc)  # nlohmann::json keeps object keys sorted
+    assert set(doc) == {"sublattice_mode", "iteration_mode", "seed", "structure", "composition", "shell_radii",
+                        "shell_weights", "prefactors", "pair_weights", "target_objective", "iterations",
+                        "chunk_size", "thread_config", "keep", "max_results_per_objective"}
+    assert " " not in c.json()  # compact dump
+    # the configuration's prepared data is the same after the round trip
+    for a, b in zip(S.prepare(c), S.prepare(back)):
+        np.testing.assert_array_equal(a.pairs, b.pairs)
+        np.testing.assert_array_equal(a.species_packed, b.species_packed)
+
+
+def test_structure_bytes_round_trip():
+    s = S.parse_config(cases.rocksalt_split("single")).structure()
+    doc = msgpack.unpackb(s.bytes(), raw=False)
+    assert list(doc) == ["frac_coords", "lattice", "pbc", "species"]
+    back = S.Structure.from_bytes(s.bytes(), S.Prec.single)
+    assert back.lattice.dtype == np.float32
+    np.testing.assert_array_equal(back.lattice, s.lattice)
+    np.testing.assert_array_equal(back.frac_coords, s.frac_coords)
+    assert back.species == s.species and back.pbc == tuple(s.pbc)
