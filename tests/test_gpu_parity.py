@@ -401,6 +401,22 @@ def test_fast_path_64_sites():
 
 
 @pytest.mark.parametrize("prec", ["double", "single"])
+def test_fast_path_sites_of_different_degree(prec):
+    """Perovskite positions, one binary composition over all 40 sites: shell 1 has sites of degree 0, 2
+    and 6, shell 2 of degree 0 and 12, so the bit-mask path's degree classes (all but the largest,
+    with wrapped negative coefficients) carry the mixed-pair count."""
+    cfg = dict(prec=prec, structure=dict(lattice=(np.eye(3) * 4.0).tolist(),
+                                         coords=[[0, 0, 0], [0.5, 0.5, 0.5], [0.5, 0.5, 0], [0.5, 0, 0.5],
+                                                 [0, 0.5, 0.5]],
+                                         species=[1] * 5, supercell=[2, 2, 2]),
+               composition={"Ti": 20, "Al": 20}, shell_weights={"1": 1.0, "2": 0.5}, iterations=4000, seed=11,
+               thread_config=1, keep=10)
+    c, d, pack, sp, bd, ob, ids = cases.trace(cfg, 4000)
+    assert len(d[0].species_packed) == 40 and len(ob) == 4000
+    assert cases.trace_mismatches(d, sp, bd, ob, prec) == []
+
+
+@pytest.mark.parametrize("prec", ["double", "single"])
 def test_fast_path_partial_window_systematic(prec):
     """A 20-site window inside a 64-site cell of the same background species (two species overall)."""
     cfg = cases.fcc32(prec, iteration_mode="systematic", seed=None, iterations=None, keep=4, pair_weights=None)
