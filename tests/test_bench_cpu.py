@@ -1,4 +1,5 @@
-"""Host logic of bench.py that needs no GPU: the clock sampler against a fake NVML (reads only)."""
+"""Host logic of bench.py that needs no GPU: the clock sampler against a fake NVML (reads only) and
+the reference arm's JSON line."""
 from __future__ import annotations
 
 import time
@@ -56,3 +57,25 @@ def test_idle_samples_do_not_pull_the_median_down():
     with s:
         time.sleep(0.03)
     assert s.summary()["sm_mhz"] == 1965.0  # samples below half the max clock are idle, not load
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` runs on host cores only and prints one JSON line with the keys the
+    benchmark contract asks for."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0", "--ref-seconds", "0.2"], capture_output=True, text=True, timeout=300,
+                         cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
