@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SQSG_ABI_VERSION 1
+#define SQSG_ABI_VERSION 2
 
 typedef enum {
   SQSG_OK = 0,
@@ -126,6 +126,15 @@ typedef struct {
   const void* prefactors;     /* S x K x K */
   const void* pair_weights;   /* S x K x K, already multiplied by the shell weights */
   const void* target;         /* S x K x K */
+  /* Optional supercell hint (NULL: none). When the structure is a supercell of cells[0] x cells[1] x
+   * cells[2] copies of a unit cell, lattice holds per site (sorted order) 4 values: the index of its
+   * unit-cell site among this structure's unit-cell sites (0..n_basis-1) and its cell indices along
+   * the three lattice vectors. The library checks the hint against the pair list: when every shell's
+   * pairs are whole translation classes it counts bonds with translated bit planes (SQSG_PATH_LATTICE,
+   * up to 64 cells); otherwise the hint is ignored. Results do not depend on it. */
+  const uint32_t* lattice;
+  uint32_t cells[3];
+  uint32_t n_basis;
 } sqsg_sublattice;
 
 typedef struct {
@@ -205,6 +214,42 @@ sqsg_status sqsg_run_transfer(const sqsg_run* run, uint64_t* h2d_bytes, uint64_t
 sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t capacity, uint64_t* count,
                                 uint8_t* species, uint32_t* bonds, void* objective, uint64_t* id);
 
+/* ------------------------------------------------------------------------------------------------
+ * Options and launch plans (no reference counterpart: the reference's only knobs are the thread
+ * count and chunk size, include/sqsgen/io/config/combined.h:122-136).
+ *
+ * Process-wide options, read when a job is prepared:
+ *   "force_general"      0/1   1: every job takes the general pair-stream path (the bit-mask path is
+ *                              skipped); results are identical, only the speed differs.
+ *   "stage_wait_ns"      > 0   bound of the device's wait for a job's staged data (default 2e9).
+ *   "debug_skip_staging" 0/1   debug: the device expects the staged data but no copy is issued, so
+ *                              that the bounded wait runs out and the call returns SQSG_ERR_TIMEOUT.
+ * Unknown names give SQSG_ERR_INVALID_ARGUMENT. */
+sqsg_status sqsg_set_option(const char* name, int64_t value);
+sqsg_status sqsg_get_option(const char* name, int64_t* value);
+
+enum { SQSG_PATH_GENERAL = 0, SQSG_PATH_BITMASK = 1, SQSG_PATH_LATTICE = 2 };
+
+typedef struct {
+  int32_t path;           /* SQSG_PATH_* */
+  int32_t stream_narrow;  /* general path: 16-bit neighbour offsets (sites <= 512) */
+  int32_t stream_staged;  /* general path: pair stream staged in shared memory (0: read through L1) */
+  int32_t reserved;
+} sqsg_part_plan;
+
+typedef struct {
+  uint32_t n_parts;
+  uint32_t smem_bytes;    /* dynamic shared memory per CTA */
+  uint32_t ctas_per_sm;   /* resident CTAs per SM (0 when no device is visible) */
+  uint32_t record_bytes;  /* bytes per candidate record in device memory */
+  char kernel[32];        /* the engine kernel a sqsg_optimize call launches */
+  sqsg_part_plan parts[8];
+} sqsg_plan;
+
+/* How sqsg_optimize would run the job: per optimised structure the evaluation path, and the launch
+ * shape. Validates the job like sqsg_optimize; needs no device (ctas_per_sm is then 0). */
+sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan);
+
 /* Peak-rate microbenchmarks used as roofline denominators (no reference counterpart).
  * kind 0: shared-memory load bandwidth (bytes/s); kind 1: 32-bit integer lane operations per second. */
 sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds);
@@ -215,12 +260,16 @@ sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds)
  * device scratch lives in one static __device__ array of about 3.6 MiB that every GPU loading this
  * library holds until exit, and it calls no cudaMalloc/cudaFree or other allocating routine.
  * Outputs: the keep+1 best objectives with exact counts and id checksums (*n_levels: in = capacity,
- * out = count) and the statistics — the values sqsg_run_levels / sqsg_run_statistics give for the same
- * job — but no configuration records. Limits: staged job data <= 3 MiB, <= 16448 tiles; no callback
- * or cancellation; `stream` may be NULL (legacy default stream). The first call on a device looks up
- * the array's device address, so make it before any stream capture. Calls share the array: the call
- * resets what must start at zero and serialises calls from one process, but calls that overlap on the
- * GPU (another process, or work still running on the same context) race. Messages go to err. */
+ * out = count) — the values sqsg_run_levels gives for the same job — and, of the statistics, finished,
+ * best_objective and the total/loop timings; best_rank is set to UINT64_MAX (not reported: no
+ * configuration records are kept). Limits: staged job data <= 3 MiB, <= 16448 tiles; no callback or
+ * cancellation; `stream` may be NULL (legacy default stream). The first call on a device looks up the
+ * array's device address, so make it before any stream capture. Calls share the array: each call
+ * resets what must start at zero, calls from one process are serialised by a lock, and a call returns
+ * only after its kernel has finished, also on error paths. Separate processes each have their own copy
+ * of the array. Work of this process that still uses the array on the GPU when another call starts
+ * (which the lock and the wait above rule out for this entry point's own calls) would race with it.
+ * Messages go to err. */
 sqsg_status sqsg_optimize_levels_noalloc(const sqsg_job* job, void* stream, uint32_t* n_levels, double* values,
                                          uint64_t* counts, uint64_t* checksums, sqsg_statistics* stats, char* err,
                                          size_t err_len);
@@ -261,6 +310,9 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
  * statistics carry the job latency in timings_ns[SQSG_TIMING_TOTAL] (submission to result). */
 sqsg_status sqsg_server_wait(sqsg_server* server, uint64_t ticket, int64_t timeout_us, sqsg_run** run);
 sqsg_status sqsg_server_stats(sqsg_server* server, sqsg_server_counters* stats);
+/* Persistent-kernel launches still running. CTAs leave after a bounded number of empty polls of
+ * their ring (about 0.5 ms), so this drops to 0 soon after the server runs out of work. */
+sqsg_status sqsg_server_running(sqsg_server* server, uint32_t* launches);
 sqsg_status sqsg_server_destroy(sqsg_server* server);
 
 #ifdef __cplusplus

@@ -36,7 +36,10 @@ EXPORTED = (
     "sqsg_optimize_trace", "sqsg_optimize_batch", "sqsg_run_levels", "sqsg_run_info",
     "sqsg_microbench", "sqsg_run_transfer", "sqsg_optimize_levels_noalloc",
     "sqsg_server_create", "sqsg_server_submit", "sqsg_server_wait", "sqsg_server_stats", "sqsg_server_destroy",
+    "sqsg_server_running", "sqsg_set_option", "sqsg_get_option", "sqsg_plan_job",
 )
+
+PATH_NAMES = {0: "general", 1: "bitmask", 2: "lattice"}
 
 
 class NativeError(RuntimeError):
@@ -62,6 +65,9 @@ class SqsgSublattice(C.Structure):
         ("prefactors", C.c_void_p),
         ("pair_weights", C.c_void_p),
         ("target", C.c_void_p),
+        ("lattice", C.c_void_p),
+        ("cells", C.c_uint32 * 3),
+        ("n_basis", C.c_uint32),
     ]
 
 
@@ -99,6 +105,16 @@ class SqsgJob(C.Structure):
         ("range_first", C.c_uint64),
         ("range_count", C.c_uint64),
     ]
+
+
+class SqsgPartPlan(C.Structure):
+    _fields_ = [("path", C.c_int32), ("stream_narrow", C.c_int32), ("stream_staged", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class SqsgPlan(C.Structure):
+    _fields_ = [("n_parts", C.c_uint32), ("smem_bytes", C.c_uint32), ("ctas_per_sm", C.c_uint32),
+                ("record_bytes", C.c_uint32), ("kernel", C.c_char * 32), ("parts", SqsgPartPlan * 8)]
 
 
 class SqsgServerOptions(C.Structure):
@@ -165,6 +181,10 @@ def lib():
         L.sqsg_server_wait.argtypes = [vp, u64, C.c_int64, C.POINTER(vp)]
         L.sqsg_server_stats.argtypes = [vp, C.POINTER(SqsgServerCounters)]
         L.sqsg_server_destroy.argtypes = [vp]
+        L.sqsg_server_running.argtypes = [vp, C.POINTER(u32)]
+        L.sqsg_set_option.argtypes = [C.c_char_p, C.c_int64]
+        L.sqsg_get_option.argtypes = [C.c_char_p, C.POINTER(C.c_int64)]
+        L.sqsg_plan_job.argtypes = [C.POINTER(SqsgJob), C.POINTER(SqsgPlan)]
         L.sqsg_microbench.argtypes = [C.c_int, C.c_int, C.POINTER(dbl), C.POINTER(dbl)]
         for name in EXPORTED:
             if name not in ("sqsg_version", "sqsg_last_error", "sqsg_device_count", "sqsg_run_count",
@@ -191,6 +211,45 @@ def ptr(a: np.ndarray):
 
 def prec_code(dtype) -> int:
     return 1 if np.dtype(dtype) == np.float64 else 0
+
+
+def set_option(name: str, value: int) -> None:
+    check(lib().sqsg_set_option(name.encode(), int(value)))
+
+
+def get_option(name: str) -> int:
+    v = C.c_int64()
+    check(lib().sqsg_get_option(name.encode(), C.byref(v)))
+    return int(v.value)
+
+
+class options:
+    """Context manager that sets process-wide library options and restores them on exit."""
+
+    def __init__(self, **values):
+        self.values = values
+        self.saved = {}
+
+    def __enter__(self):
+        for k, v in self.values.items():
+            self.saved[k] = get_option(k)
+            set_option(k, v)
+        return self
+
+    def __exit__(self, *exc):
+        for k, v in self.saved.items():
+            set_option(k, v)
+
+
+def plan(job) -> dict:
+    """sqsg_plan_job of a native job: kernel, shared memory, CTAs per SM and each part's path."""
+    p = SqsgPlan()
+    check(lib().sqsg_plan_job(C.byref(job), C.byref(p)))
+    parts = [dict(path=PATH_NAMES.get(p.parts[k].path, str(p.parts[k].path)),
+                  stream_narrow=bool(p.parts[k].stream_narrow), stream_staged=bool(p.parts[k].stream_staged))
+             for k in range(p.n_parts)]
+    return dict(kernel=p.kernel.decode(), smem_bytes=int(p.smem_bytes), ctas_per_sm=int(p.ctas_per_sm),
+                record_bytes=int(p.record_bytes), parts=parts)
 
 
 def device_count() -> int:

@@ -13,6 +13,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -23,7 +24,10 @@
 #include <unordered_set>
 #include <vector>
 
-#include "engine_device.cuh"
+#include "attr_tracker.h"
+#include "kernels.h"
+#include "permutation.h"
+#include "prepare.h"
 #include "select.h"
 #include "sqsg_internal.h"
 #include "tiles.h"
@@ -33,416 +37,41 @@ namespace sqsg {
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
+// ------------------------------------------------------------------------------------------------
+// Process-wide options
+static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}};
+static const char* const kOptionNames[kOptCount] = {"force_general", "stage_wait_ns", "debug_skip_staging"};
+
+long long option(Option o) { return g_options[o].load(std::memory_order_relaxed); }
+
+static int option_index(const char* name) {
+  if (!name) return -1;
+  for (int k = 0; k < kOptCount; ++k)
+    if (std::strcmp(name, kOptionNames[k]) == 0) return k;
+  return -1;
+}
+
+static DynamicSmemTracker& smem_tracker() {
+  static auto* t = new DynamicSmemTracker();  // never destroyed: used until exit
+  return *t;
+}
+
+int raise_dynamic_smem(const void* kernel, size_t bytes) {
+  int dev = 0;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return static_cast<int>(e);
+  return smem_tracker().raise(dev, kernel, bytes, [&](size_t b) {
+    return static_cast<int>(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(b)));
+  });
+}
+
 #define CUDA_CHECK(expr)                                                                              \
   do {                                                                                                \
     cudaError_t err__ = (expr);                                                                       \
     if (err__ != cudaSuccess)                                                                         \
       throw cuda_error(std::string(#expr) + ": " + cudaGetErrorString(err__));                       \
   } while (0)
-
-static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-static inline uint32_t host_site_off(uint32_t x) { return (x >> 2) * (kBlock * 4) + (x & 3); }
-
-// ------------------------------------------------------------------------------------------------
-// Job preparation (host)
-struct PartMeta {
-  uint32_t N, K, S;
-};
-
-struct PreparedJob {
-  JobDesc desc{};               // device pointers filled at upload
-  std::vector<uint8_t> blob;    // staged sections of all parts
-  std::vector<PartMeta> parts;
-  int prec = 1;
-  bool systematic = false;
-  uint64_t total = 0;           // configurations
-  uint64_t keep = 1;
-  int64_t max_rpo = -1;
-  size_t record_bytes = 0;
-  size_t tsz = 8;               // sizeof(T)
-  uint32_t configs_per_thread = 1;
-  uint64_t max_results = 0;     // caller's record capacity (0 = default)
-  uint64_t range_first = 0, range_count = 0;  // share of the configuration space to evaluate
-  // a re-run of an overflowed job: record capacity, starting threshold, passes already made
-  uint64_t rerun_capacity = 0;
-  double rerun_threshold = 0.0;
-  int passes = 0;
-};
-
-template <class T> static void copy_cube(std::vector<uint8_t>& blob, size_t off, const void* src, size_t n) {
-  std::memcpy(blob.data() + off, src, n * sizeof(T));
-}
-
-// Pair stream of a part: for each shell s and site i (ascending) a header word (s | cnt << 8), the
-// byte offset of i in a species column, and cnt byte offsets of its neighbours j > i in shell s.
-// The grouped pair stream of one part: for each (shell s, site i) the sites j > i of its pairs, in
-// groups of at most kMaxGroup. Narrow form (every column offset below 2^16, i.e. N <= 512): one
-// header word  ioff | s << 16 | cnt << 24  and the cnt column offsets as 16-bit halves, two per
-// word. Wide form: header words  s | cnt << 8  and  ioff, then one word per offset.
-static bool narrow_stream(uint32_t n_sites) { return host_site_off(n_sites ? n_sites - 1 : 0) < 0x10000u; }
-
-// CTAs of the general-path kernel (sqsg_engine_wide, at most kMinBlocksWide) that fit on one SM of
-// `device` with `dynamic_smem` bytes each, from the device's shared memory per SM and per-block
-// reservation and the kernel's static shared memory (an estimate that needs no CUDA context).
-static int ctas_per_sm(int device, size_t dynamic_smem) {
-  static std::mutex m;
-  static std::map<int, std::pair<size_t, size_t>> cache;  // device -> (smem per SM, reserved per block)
-  std::pair<size_t, size_t> dev{233472, 1024};
-  {
-    std::lock_guard<std::mutex> l(m);
-    auto it = cache.find(device);
-    if (it != cache.end()) {
-      dev = it->second;
-    } else {
-      int per_sm = 0, reserved = 0;
-      if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) == cudaSuccess &&
-          cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) == cudaSuccess)
-        dev = {static_cast<size_t>(per_sm), static_cast<size_t>(reserved)};
-      else
-        cudaGetLastError();
-      cache[device] = dev;
-    }
-  }
-  const size_t static_smem = sizeof(JobDesc) + kCtaLevelSlots * sizeof(LevelSlot) + 128;
-  const size_t per_cta = align_up(dynamic_smem + static_smem, 128) + dev.second;
-  return static_cast<int>(std::min<size_t>(kMinBlocksWide, dev.first / per_cta));
-}
-
-static std::vector<uint32_t> build_stream(const sqsg_sublattice& sl) {
-  const uint32_t N = sl.n_sites, S = sl.n_shells, P = sl.n_pairs;
-  std::vector<std::vector<uint32_t>> by(static_cast<size_t>(S) * N);
-  std::vector<uint64_t> per_shell(S, 0);
-  for (uint32_t p = 0; p < P; ++p) {
-    uint32_t i = sl.pairs[3 * p], j = sl.pairs[3 * p + 1], s = sl.pairs[3 * p + 2];
-    if (i >= N || j >= N) throw std::out_of_range("pair index out of range");
-    if (s >= S) throw std::out_of_range("pair shell index out of range");
-    if (i == j) throw std::invalid_argument("pair with i == j");
-    if (i > j) std::swap(i, j);  // ordered counts are defined for i < j (structure.h:445-447)
-    by[static_cast<size_t>(s) * N + i].push_back(j);
-    per_shell[s]++;
-  }
-  for (uint32_t s = 0; s < S; ++s)
-    if (per_shell[s] > 0xffffu)
-      throw unsupported_error("a shell holds more than 65535 pairs; the 16-bit bond counters cannot hold it");
-  const bool narrow = narrow_stream(N);
-  std::vector<uint32_t> st;
-  st.reserve(P + 2 * static_cast<size_t>(S) * N);
-  for (uint32_t s = 0; s < S; ++s)
-    for (uint32_t i = 0; i < N; ++i) {
-      auto& js = by[static_cast<size_t>(s) * N + i];
-      std::sort(js.begin(), js.end());
-      for (size_t b = 0; b < js.size(); b += kMaxGroup) {
-        uint32_t cnt = static_cast<uint32_t>(std::min<size_t>(kMaxGroup, js.size() - b));
-        if (narrow) {
-          st.push_back(host_site_off(i) | (s << 16) | (cnt << 24));
-          for (uint32_t e = 0; e < cnt; e += 2) {
-            const uint32_t lo = host_site_off(js[b + e]);
-            const uint32_t hi = e + 1 < cnt ? host_site_off(js[b + e + 1]) : 0u;
-            st.push_back(lo | (hi << 16));
-          }
-        } else {
-          st.push_back(s | (cnt << 8));
-          st.push_back(host_site_off(i));
-          for (uint32_t e = 0; e < cnt; ++e) st.push_back(host_site_off(js[b + e]));
-        }
-      }
-    }
-  return st;
-}
-
-static uint64_t window_permutations(const sqsg_sublattice& sl, PartDesc& pd) {
-  const uint32_t lo = sl.windows[0], hi = sl.windows[1];
-  uint32_t counts[256] = {0};
-  for (uint32_t x = lo; x < hi; ++x) counts[sl.species[x]]++;
-  uint32_t k = 0;
-  uint32_t dense[kMaxSpecies];
-  for (uint32_t v = 0; v < 256; ++v)
-    if (counts[v]) {
-      if (k >= kMaxSpecies) throw unsupported_error("more than 8 species in the systematic window");
-      pd.unrank_rev[k] = static_cast<uint8_t>(v);
-      pd.unrank_hist[k] = counts[v];
-      dense[k] = counts[v];
-      ++k;
-    }
-  pd.unrank_k = k;
-  uint64_t total = 0;
-  if (!num_permutations_counts(dense, static_cast<int>(k), &total))
-    throw std::out_of_range("The number of permutations to test does not fit in 64 bits");
-  return total;
-}
-
-static PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
-  PreparedJob pj;
-  if (job.prec != SQSG_PREC_SINGLE && job.prec != SQSG_PREC_DOUBLE) throw std::invalid_argument("invalid prec");
-  if (job.iteration_mode != SQSG_ITERATION_RANDOM && job.iteration_mode != SQSG_ITERATION_SYSTEMATIC)
-    throw std::invalid_argument("invalid iteration mode");
-  if (job.sublattice_mode != SQSG_SUBLATTICE_INTERACT && job.sublattice_mode != SQSG_SUBLATTICE_SPLIT)
-    throw std::invalid_argument("invalid sublattice mode");
-  if (!job.sublattices || job.n_sublattices == 0) throw std::invalid_argument("no sublattices");
-  if (job.sublattice_mode == SQSG_SUBLATTICE_INTERACT && job.n_sublattices != 1)
-    throw std::invalid_argument("interact mode takes one optimised structure (windows carry the sublattices)");
-  if (job.n_sublattices > static_cast<uint32_t>(kMaxParts))
-    throw unsupported_error("more than 8 sublattices in split mode");
-  if (job.iteration_mode == SQSG_ITERATION_SYSTEMATIC && job.sublattice_mode == SQSG_SUBLATTICE_SPLIT)
-    throw std::invalid_argument(
-        "It is not possible to do an exhaustive search on multiple sublattices in mode \"split\"");
-  if (job.keep == 0) throw std::invalid_argument("The number of best kept structures must be greater than 0");
-  if (job.keep > 31) throw unsupported_error("keep > 31 is not supported by the warp-level best list");
-  pj.prec = job.prec;
-  pj.tsz = job.prec == SQSG_PREC_DOUBLE ? 8 : 4;
-  pj.systematic = job.iteration_mode == SQSG_ITERATION_SYSTEMATIC;
-  pj.keep = job.keep;
-  pj.max_rpo = job.max_results_per_objective;
-  pj.max_results = job.max_results;
-  JobDesc& d = pj.desc;
-  d.prec = static_cast<uint32_t>(job.prec);
-  d.mode = pj.systematic ? 1 : 0;
-  d.n_parts = job.n_sublattices;
-  d.keep = static_cast<uint32_t>(job.keep);
-  d.kw = 1;
-
-  size_t blob_size = 0, smem = 0;
-  size_t rec = 16, tsp = 0, tbd = 0;
-  std::vector<std::vector<uint32_t>> streams(job.n_sublattices);
-  std::vector<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>> k2_data;
-  std::vector<std::vector<uint32_t>> k2_nbp_data;
-  for (uint32_t p = 0; p < job.n_sublattices; ++p) {
-    const sqsg_sublattice& sl = job.sublattices[p];
-    PartDesc& P = d.parts[p];
-    if (sl.n_sites == 0) throw std::invalid_argument("empty structure");
-    if (sl.n_species == 0 || sl.n_shells == 0) throw std::out_of_range("no coordination shells selected");
-    if (sl.n_species > static_cast<uint32_t>(kMaxSpecies))
-      throw unsupported_error("more than 8 species in one optimised structure");
-    if (sl.n_shells > 255) throw unsupported_error("more than 255 shells");
-    if (!sl.species || !sl.prefactors || !sl.pair_weights || !sl.target || (sl.n_pairs && !sl.pairs))
-      throw std::invalid_argument("null array in sublattice");
-    if (sl.n_windows == 0 || !sl.windows) throw std::invalid_argument("no shuffle window");
-    if (sl.n_windows > static_cast<uint32_t>(kMaxWindows)) throw unsupported_error("more than 16 shuffle windows");
-    for (uint32_t x = 0; x < sl.n_sites; ++x)
-      if (sl.species[x] >= sl.n_species) throw std::out_of_range("packed species index >= n_species");
-    for (uint32_t w = 0; w < sl.n_windows; ++w) {
-      if (sl.windows[2 * w] >= sl.windows[2 * w + 1] || sl.windows[2 * w + 1] > sl.n_sites)
-        throw std::out_of_range("invalid shuffle window");
-      if (w > 0 && sl.windows[2 * w] < sl.windows[2 * w - 1]) throw std::invalid_argument("overlapping windows");
-    }
-    if (pj.systematic && sl.n_windows != 1)
-      throw std::invalid_argument("In \"systematic\" iteration mode only one sublattice is allowed");
-    P.n_sites = sl.n_sites;
-    P.n_species = sl.n_species;
-    P.n_shells = sl.n_shells;
-    P.n_windows = sl.n_windows;
-    P.hw = (sl.n_species + 1) / 2;
-    if (sl.n_species > 4) d.kw = 2;
-    streams[p] = build_stream(sl);
-    P.stream_words = static_cast<uint32_t>(streams[p].size());
-    P.stream_narrow = narrow_stream(sl.n_sites) ? 1u : 0u;
-    const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
-    // binary fast path data: per (shell, site) mask of the neighbours j > i (bit N-1-j)
-    const bool k2 = job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64 && sl.n_shells <= kK2MaxShells;
-    std::vector<uint32_t> k2_entries, k2_shells, k2_nbp;
-    if (k2) {
-      const uint32_t N = sl.n_sites;
-      std::vector<unsigned long long> nb(static_cast<size_t>(sl.n_shells) * N, 0ull);
-      std::vector<uint32_t> ps(sl.n_shells, 0);
-      for (uint32_t e = 0; e < sl.n_pairs; ++e) {
-        uint32_t i = sl.pairs[3 * e], j = sl.pairs[3 * e + 1];
-        const uint32_t sh = sl.pairs[3 * e + 2];
-        if (i > j) std::swap(i, j);
-        nb[static_cast<size_t>(sh) * N + i] |= 1ull << (N - 1 - j);
-        ps[sh]++;
-      }
-      std::vector<uint32_t> shell_end(sl.n_shells);
-      for (uint32_t sh = 0; sh < sl.n_shells; ++sh) {
-        for (uint32_t i = 0; i < N; ++i) {
-          const unsigned long long m = nb[static_cast<size_t>(sh) * N + i];
-          if (!m) continue;
-          k2_entries.push_back(static_cast<uint32_t>(m));
-          k2_entries.push_back(static_cast<uint32_t>(m >> 32));
-          k2_entries.push_back(N - 1 - i);
-          k2_entries.push_back(static_cast<uint32_t>(__builtin_popcountll(m)));
-        }
-        shell_end[sh] = static_cast<uint32_t>(k2_entries.size() / 4);
-      }
-      uint32_t ones = 0;
-      for (uint32_t x = 0; x < N; ++x) ones += sl.species[x] != 0 ? 1u : 0u;
-      // degree classes: sites grouped by their number of shell-s pairs (either end), so that
-      // n01 + n10 = sum_x b_x deg_s(x) - 2 n11 costs one popcount per class. The number of ones is
-      // the same in every configuration, so the largest class c* needs none: the sum is
-      // deg_c* * ones + sum over the other classes of (deg_c - deg_c*) * popc (mod 2^32), and a
-      // lattice whose sites all have one degree (every Bravais lattice) needs no popcount at all.
-      for (uint32_t sh = 0; sh < sl.n_shells; ++sh) {
-        std::vector<uint32_t> deg(N, 0);
-        for (uint32_t i = 0; i < N; ++i) {
-          const unsigned long long m = nb[static_cast<size_t>(sh) * N + i];
-          deg[i] += static_cast<uint32_t>(__builtin_popcountll(m));
-          for (uint32_t j = 0; j < N; ++j)
-            if ((m >> (N - 1 - j)) & 1ull) deg[j]++;
-        }
-        std::map<uint32_t, unsigned long long> classes;  // degree 0 included: the classes cover all sites
-        for (uint32_t x = 0; x < N; ++x) classes[deg[x]] |= 1ull << (N - 1 - x);
-        uint32_t dstar = 0;
-        int best = -1;
-        for (auto& [dv, m] : classes)
-          if (__builtin_popcountll(m) > best) best = __builtin_popcountll(m), dstar = dv;
-        const uint32_t d0 = static_cast<uint32_t>(k2_entries.size() / 4);
-        for (auto& [dv, m] : classes) {
-          if (dv == dstar) continue;
-          k2_entries.push_back(static_cast<uint32_t>(m));
-          k2_entries.push_back(static_cast<uint32_t>(m >> 32));
-          k2_entries.push_back(dv - dstar);
-          k2_entries.push_back(0);
-        }
-        k2_shells.push_back(ps[sh]);
-        k2_shells.push_back(shell_end[sh]);
-        k2_shells.push_back(d0);
-        k2_shells.push_back(static_cast<uint32_t>(k2_entries.size() / 4));
-        k2_shells.push_back(dstar * ones);
-        for (int pad = 0; pad < 3; ++pad) k2_shells.push_back(0);
-      }
-      // neighbour masks indexed by the bit position p = N-1-i of site i, for the per-configuration
-      // loop over the set bits of the minority species
-      const uint32_t slots = N <= 32 ? 32 : 64;
-      for (uint32_t sh = 0; sh < sl.n_shells; ++sh)
-        for (uint32_t bp = 0; bp < slots; ++bp) {
-          const unsigned long long m = bp < N ? nb[static_cast<size_t>(sh) * N + (N - 1 - bp)] : 0ull;
-          k2_nbp.push_back(static_cast<uint32_t>(m));
-          if (slots == 64) k2_nbp.push_back(static_cast<uint32_t>(m >> 32));
-        }
-      P.k2_zeros = 2 * ones > N ? 1u : 0u;
-    }
-    // blob section layout: cubes | windows | species codes | binary-path masks | pair stream. The
-    // stream is staged into shared memory with the rest when that costs no CTA per SM; otherwise
-    // (large cells, split jobs, the binary path that does not read it) it is read from the blob
-    // through L1: one copy per SM for all its CTAs, leaving the shared memory to more CTAs.
-    size_t off = 0;
-    P.cube_off = 0;
-    off = align_up(3 * skk * pj.tsz, 16);
-    P.win_off = static_cast<uint32_t>(off);
-    off = align_up(off + 8ull * sl.n_windows, 16);
-    P.species_off = static_cast<uint32_t>(off);
-    off = align_up(off + sl.n_sites, 16);
-    if (k2) {
-      P.k2_off = static_cast<uint32_t>(off);
-      P.k2_entries = static_cast<uint32_t>(k2_entries.size() / 4);
-      off = align_up(off + 4 * k2_entries.size(), 16);
-      P.k2_shell_off = static_cast<uint32_t>(off);
-      off = align_up(off + 4 * k2_shells.size(), 16);
-      P.k2_nbp_off = static_cast<uint32_t>(off);
-      off = align_up(off + 4 * k2_nbp.size(), 16);
-      k2_data.emplace_back(std::move(k2_entries), std::move(k2_shells));
-      k2_nbp_data.emplace_back(std::move(k2_nbp));
-    } else {
-      k2_data.emplace_back();
-      k2_nbp_data.emplace_back();
-    }
-    P.stream_off = static_cast<uint32_t>(off);
-    const size_t with_stream = align_up(off + 4ull * streams[p].size(), 16);
-    const size_t lanes = (static_cast<size_t>((sl.n_sites + 3) / 4) +
-                          static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw) * kBlock * 4;
-    const bool staged = !k2 && job.n_sublattices == 1 &&
-                        ctas_per_sm(job.device, with_stream + lanes) >= ctas_per_sm(job.device, off + lanes);
-    P.stream_global = staged ? 0u : 1u;
-    P.static_bytes = static_cast<uint32_t>(staged ? with_stream : off);
-    P.blob_off = static_cast<uint32_t>(blob_size);
-    blob_size += with_stream;
-    off = P.static_bytes;
-    // shared memory: staged section, species columns, histogram
-    P.smem_off = static_cast<uint32_t>(smem);
-    P.col_off = static_cast<uint32_t>(off);
-    off += static_cast<size_t>((sl.n_sites + 3) / 4) * kBlock * 4;
-    P.hist_off = static_cast<uint32_t>(off);
-    off += static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw * kBlock * 4;
-    smem += align_up(off, 16);
-    // candidate record layout
-    P.rec_species_off = static_cast<uint32_t>(rec);
-    rec = align_up(rec + sl.n_sites, 8);
-    P.rec_obj_off = static_cast<uint32_t>(rec);
-    rec += 8;
-    P.rec_sro_off = static_cast<uint32_t>(rec);
-    rec = align_up(rec + skk * pj.tsz, 8);
-    P.trace_species_off = static_cast<uint32_t>(tsp);
-    tsp += sl.n_sites;
-    P.trace_bonds_off = static_cast<uint32_t>(tbd);
-    tbd += skk;
-    pj.parts.push_back(PartMeta{sl.n_sites, sl.n_species, sl.n_shells});
-    if (pj.systematic) pj.total = window_permutations(sl, P);
-    if (k2 && (!pj.systematic || (P.unrank_k == 2 && P.unrank_rev[0] == 0 && P.unrank_rev[1] == 1)))
-      d.k2 = sl.n_sites <= 32 ? 1 : 2;
-  }
-  if (!pj.systematic) pj.total = job.iterations;
-  d.total = pj.total;
-  if (job.range_first > pj.total) throw std::out_of_range("range_first beyond the configuration space");
-  pj.range_first = job.range_first;
-  pj.range_count = job.range_count ? job.range_count : pj.total - job.range_first;
-  if (pj.range_count > pj.total - pj.range_first) throw std::out_of_range("range beyond the configuration space");
-  d.trace_base = pj.range_first + (pj.systematic ? 1 : 0);
-  d.record_bytes = static_cast<uint32_t>(align_up(rec, 16));
-  pj.record_bytes = d.record_bytes;
-  d.smem_bytes = static_cast<uint32_t>(smem);
-  d.trace = trace_capacity > 0 ? 1 : 0;
-  d.trace_capacity = trace_capacity;
-  d.trace_species_stride = static_cast<uint32_t>(tsp);
-  d.trace_bonds_stride = static_cast<uint32_t>(tbd);
-  if (job.has_seed) {
-    d.seed = job.seed;
-  } else {
-    std::random_device rd;  // core/shuffle.h:16-21 draws an unseeded run's seed the same way
-    d.seed = (static_cast<uint64_t>(rd()) << 32) ^ rd();
-  }
-  pj.blob.assign(blob_size, 0);
-  for (uint32_t p = 0; p < job.n_sublattices; ++p) {
-    const sqsg_sublattice& sl = job.sublattices[p];
-    const PartDesc& P = d.parts[p];
-    const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
-    uint8_t* base = pj.blob.data() + P.blob_off;
-    std::memcpy(base + P.cube_off, sl.prefactors, skk * pj.tsz);
-    std::memcpy(base + P.cube_off + skk * pj.tsz, sl.pair_weights, skk * pj.tsz);
-    std::memcpy(base + P.cube_off + 2 * skk * pj.tsz, sl.target, skk * pj.tsz);
-    std::memcpy(base + P.win_off, sl.windows, 8ull * sl.n_windows);
-    std::memcpy(base + P.stream_off, streams[p].data(), 4ull * streams[p].size());
-    for (uint32_t x = 0; x < sl.n_sites; ++x) base[P.species_off + x] = static_cast<uint8_t>(sl.species[x] << 3);
-    const auto& k2d = k2_data[p];
-    if (!k2d.first.empty()) std::memcpy(base + P.k2_off, k2d.first.data(), 4 * k2d.first.size());
-    if (!k2d.second.empty()) std::memcpy(base + P.k2_shell_off, k2d.second.data(), 4 * k2d.second.size());
-    if (!k2_nbp_data[p].empty())
-      std::memcpy(base + P.k2_nbp_off, k2_nbp_data[p].data(), 4 * k2_nbp_data[p].size());
-  }
-  // binary systematic path: binomials C(m, j) for m <= window size, j <= ones in the window, kept in
-  // global memory after the staged sections (read through the L1 by the per-thread unrank)
-  if (d.k2 && pj.systematic) {
-    PartDesc& P = d.parts[0];
-    const uint32_t n = job.sublattices[0].windows[1] - job.sublattices[0].windows[0];
-    const uint32_t ones = P.unrank_hist[1], cols = ones + 1;
-    const size_t off = align_up(pj.blob.size(), 16);
-    pj.blob.resize(off + 8ull * (n + 1) * cols, 0);
-    P.k2_binom_off = static_cast<uint32_t>(off);
-    unsigned long long* b = reinterpret_cast<unsigned long long*>(pj.blob.data() + off);
-    for (uint32_t m = 0; m <= n; ++m)
-      for (uint32_t j = 0; j <= ones; ++j)
-        b[m * cols + j] = (j == 0) ? 1ull : (m == 0 ? 0ull : b[(m - 1) * cols + j - 1] + b[(m - 1) * cols + j]);
-  }
-  return pj;
-}
-
-// A job may have at most this many tiles (about 1.4e14 configurations at full-size tiles).
-constexpr size_t kMaxJobTiles = 1u << 24;
-
-static void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles,
-                       uint64_t max_per_thread = 1u << 16) {
-  size_t added = 0;
-  for_each_tile(
-      pj.range_first, pj.range_count, pj.systematic,
-      [&](Tile t) -> bool {
-        if (++added > kMaxJobTiles) return false;
-        t.job = job_index;
-        tiles.push_back(t);
-        return true;
-      },
-      max_per_thread);
-  if (added > kMaxJobTiles)
-    throw unsupported_error("the job has more than " + std::to_string(kMaxJobTiles) +
-                            " tiles; split it with range_first/range_count");
-}
 
 // ------------------------------------------------------------------------------------------------
 // Device workspaces: grow-only buffers and streams, pooled per device.
@@ -541,25 +170,21 @@ using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, 
                               unsigned long long*, volatile uint32_t*);
 
 // The general path runs in sqsg_engine_wide (128 registers); a launch whose jobs all take the binary
-// bit-mask path runs in sqsg_engine (96 registers, 5 CTAs per SM).
+// bit-mask path runs in sqsg_engine_mask (96 registers, 5 CTAs per SM).
 static EngineKernel engine_for(bool all_bitmask) { return all_bitmask ? sqsg_engine_mask : sqsg_engine_wide; }
 
+// The dynamic shared-memory attribute is per device: it is raised on the current device (every
+// caller has made the job's device current).
 static void configure_kernel(size_t smem) {
-  static std::mutex m;
-  static size_t configured = 0;
-  std::lock_guard<std::mutex> l(m);
-  if (smem > configured) {
-    CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)));
-    CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)));
-    CUDA_CHECK(cudaFuncSetAttribute(sqsg_engine_mask, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)));
-    configured = smem;
+  for (const void* k : {reinterpret_cast<const void*>(sqsg_engine_wide), reinterpret_cast<const void*>(sqsg_engine_mask)}) {
+    const int err = raise_dynamic_smem(k, smem);
+    if (err != 0)
+      throw cuda_error(std::string("cudaFuncSetAttribute(MaxDynamicSharedMemorySize): ") +
+                       cudaGetErrorString(static_cast<cudaError_t>(err)));
   }
 }
 
-static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel kernel = sqsg_engine) {
+static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel kernel) {
   configure_kernel(smem);
   int per_sm = 0;
   CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem));
@@ -571,11 +196,10 @@ static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel k
 static size_t max_dynamic_smem(int dev) {
   int v = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes a{}, b{}, c{};
-  CUDA_CHECK(cudaFuncGetAttributes(&a, sqsg_engine));
+  cudaFuncAttributes b{}, c{};
   CUDA_CHECK(cudaFuncGetAttributes(&b, sqsg_engine_wide));
   CUDA_CHECK(cudaFuncGetAttributes(&c, sqsg_engine_mask));
-  return static_cast<size_t>(v) - std::max({a.sharedSizeBytes, b.sharedSizeBytes, c.sharedSizeBytes});
+  return static_cast<size_t>(v) - std::max(b.sharedSizeBytes, c.sharedSizeBytes);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -727,7 +351,10 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
 
 // Candidate sets at least this large are selected on the device.
 constexpr uint64_t kDeviceSelectMin = 32768;
-// Device memory a re-run may give a job's records when the first pass overflowed (random runs over
+// Candidate capacity of a job that leaves max_results at 0 (64 MiB of candidates; a job whose
+// buffer overflows runs again with a buffer sized from its exact level counts).
+constexpr uint64_t kDefaultCandidates = 1u << 22;
+// Device memory a re-run may give a job's candidates when the first pass overflowed (random runs over
 // small configuration spaces revisit configurations and store every visit at or below T*).
 constexpr uint64_t kRerunRecordBytes = 16ull << 30;
 
@@ -745,25 +372,6 @@ static RecordLayout record_layout(const PreparedJob& pj) {
     L.sro_bytes[p] = static_cast<uint32_t>(static_cast<size_t>(P.n_shells) * P.n_species * P.n_species * pj.tsz);
   }
   return L;
-}
-
-// Selects the result set of device-resident records into run (exact levels required). Returns false
-// when the device path does not apply; the caller then downloads the records and selects on the host.
-static bool select_records_on_device(SelectScratch& scratch, cudaStream_t stream, const PreparedJob& pj,
-                                     const uint8_t* d_records, uint64_t n, const std::vector<double>& levels,
-                                     Run& run) {
-  if (n < kDeviceSelectMin) return false;  // small sets: the host is quicker than the launches
-  SelectedSet set;
-  if (!select_on_device(scratch, stream, record_layout(pj), d_records, n, levels, !pj.systematic, pj.max_rpo,
-                        pj.range_first + pj.range_count + 1, set))
-    return false;
-  run.count = set.count;
-  run.objective = std::move(set.objective);
-  run.sub_objective = std::move(set.sub_objective);
-  run.species = std::move(set.species);
-  run.sro = std::move(set.sro);
-  run.id = std::move(set.id);
-  return true;
 }
 
 // What one pass of a job left behind: its exact objective levels (keep+1 smallest distinct
@@ -786,12 +394,9 @@ struct Outcome {
   std::vector<uint64_t> count, checksum;
 };
 
-template <class T>
-static void levels_from_records(const PreparedJob& pj, const std::vector<uint8_t>& recs, uint64_t n, Outcome& o) {
-  const size_t rb = pj.record_bytes;
+static void levels_from_records(const PreparedJob& pj, const std::vector<Cand>& recs, uint64_t n, Outcome& o) {
   std::vector<std::pair<unsigned long long, uint64_t>> e(n);
-  for (uint64_t i = 0; i < n; ++i)
-    e[i] = {ord_bits(static_cast<double>(read_t<T>(&recs[i * rb]))), mix64(read_t<uint64_t>(&recs[i * rb + 8]))};
+  for (uint64_t i = 0; i < n; ++i) e[i] = {ord_bits(recs[i].objective), mix64(recs[i].id)};
   std::sort(e.begin(), e.end());
   for (size_t i = 0; i < e.size() && o.value.size() <= pj.keep;) {
     size_t k = i;
@@ -808,7 +413,7 @@ static void levels_from_records(const PreparedJob& pj, const std::vector<uint8_t
 }
 
 static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, const std::vector<LevelSlot>& lv,
-                      const std::vector<uint8_t>& recs, uint64_t stored, uint64_t capacity, bool may_rerun,
+                      const std::vector<Cand>& recs, uint64_t stored, uint64_t capacity, bool may_rerun,
                       uint64_t max_capacity) {
   Outcome o;
   const bool full = cnt[kRecordsFull] != 0 || cnt[kCandidates] > capacity;
@@ -834,10 +439,7 @@ static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, cons
     }
     return o;
   }
-  if (pj.prec == 1)
-    levels_from_records<double>(pj, recs, stored, o);
-  else
-    levels_from_records<float>(pj, recs, stored, o);
+  levels_from_records(pj, recs, stored, o);
   if (!full) {
     o.levels_exact = true;
     if (o.value.size() > pj.keep) o.tstar = o.value[pj.keep];
@@ -850,6 +452,85 @@ static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, cons
     o.rerun_threshold = o.value[pj.keep];
   }
   return o;
+}
+
+// The result set of a finished job's n device-resident candidates. Large sets with exact levels are
+// selected on the device (select_on_device); otherwise the candidates are filtered (objective <= T*)
+// and ordered (objective, id) on the host, systematic runs are capped per objective, the selected
+// candidates' full records are rebuilt on the device (sqsg_materialize) and select_results removes
+// repeats and applies the cap. `host_cands` may hold the candidates already downloaded.
+static void finish_selection(SelectScratch& scratch, cudaStream_t stream, const PreparedJob& pj, const JobDesc& dev_desc,
+                             const Cand* d_cands, uint64_t n, std::vector<Cand>& host_cands, const Outcome& o,
+                             bool table_exact, Run& run, uint64_t& d2h_bytes) {
+  Materializer mat;
+  mat.job = dev_desc;
+  mat.smem = pj.desc.smem_full;
+  if (n >= kDeviceSelectMin && table_exact && o.levels_exact) {
+    SelectedSet set;
+    if (select_on_device(scratch, stream, record_layout(pj), d_cands, n, o.value, !pj.systematic, pj.max_rpo,
+                         pj.range_first + pj.range_count + 1, mat, set)) {
+      run.count = set.count;
+      run.objective = std::move(set.objective);
+      run.sub_objective = std::move(set.sub_objective);
+      run.species = std::move(set.species);
+      run.sro = std::move(set.sro);
+      run.id = std::move(set.id);
+      d2h_bytes += run.objective.size() + run.sub_objective.size() + run.species.size() + run.sro.size() +
+                   run.id.size() * 8;
+      return;
+    }
+  }
+  if (host_cands.size() != n) {
+    host_cands.resize(n);
+    if (n) CUDA_CHECK(cudaMemcpyAsync(host_cands.data(), d_cands, n * sizeof(Cand), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    d2h_bytes += n * sizeof(Cand);
+  }
+  // keep+1 best distinct objectives among the stored candidates when the levels are not exact
+  double tstar = o.tstar;
+  if (!o.levels_exact) {
+    std::vector<double> v;
+    v.reserve(n);
+    for (auto& c : host_cands) v.push_back(c.objective);
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    tstar = v.size() > pj.keep ? v[pj.keep] : std::numeric_limits<double>::infinity();
+  }
+  std::vector<Cand> sel;
+  for (auto& c : host_cands)
+    if (c.objective <= tstar) sel.push_back(c);
+  std::sort(sel.begin(), sel.end(), [](const Cand& a, const Cand& b) {
+    return a.objective != b.objective ? a.objective < b.objective : a.id < b.id;
+  });
+  if (pj.systematic && pj.max_rpo >= 0) {  // ranks are unique: the cap applies before rebuilding
+    std::vector<Cand> capped;
+    uint64_t cur = 0;
+    for (size_t k = 0; k < sel.size(); ++k) {
+      cur = (k == 0 || sel[k].objective != sel[k - 1].objective) ? 0 : cur + 1;
+      if (cur <= static_cast<uint64_t>(pj.max_rpo)) capped.push_back(sel[k]);
+    }
+    sel.swap(capped);
+  }
+  const uint64_t m = sel.size();
+  std::vector<uint8_t> recs(m * pj.record_bytes);
+  if (m) {
+    if (scratch.stream != stream) {
+      scratch.release();
+      scratch.stream = stream;
+    }
+    auto* d_sel = static_cast<Cand*>(scratch.get(7, m * sizeof(Cand)));
+    auto* d_recs = static_cast<uint8_t*>(scratch.get(19, m * pj.record_bytes));
+    CUDA_CHECK(cudaMemcpyAsync(d_sel, sel.data(), m * sizeof(Cand), cudaMemcpyHostToDevice, stream));
+    if (materialize(scratch, stream, mat, d_sel, static_cast<uint32_t>(m), d_recs) != 0)
+      throw cuda_error("internal error: a rebuilt record's objective differs from the engine's");
+    CUDA_CHECK(cudaMemcpyAsync(recs.data(), d_recs, recs.size(), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    d2h_bytes += recs.size();
+  }
+  if (pj.prec == 1)
+    select_results<double>(pj, recs, m, run, true, tstar);
+  else
+    select_results<float>(pj, recs, m, run, true, tstar);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -891,8 +572,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     smem = std::max<size_t>(smem, pjs[j].desc.smem_bytes);
     blob_off[j] = blob_total;
     blob_total = align_up(blob_total + pjs[j].blob.size(), 256);
-    const uint64_t budget = (512ull << 20) / pjs[j].record_bytes;
-    capacity[j] = pjs[j].max_results ? pjs[j].max_results : std::max<uint64_t>(1024, std::min<uint64_t>(1u << 20, budget));
+    capacity[j] = pjs[j].max_results ? pjs[j].max_results : kDefaultCandidates;
     if (pjs[j].rerun_capacity) {
       capacity[j] = pjs[j].rerun_capacity;
       fixed_threshold[j] = true;
@@ -908,7 +588,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     rec_total = 0;
     for (size_t j = 0; j < nj; ++j) {
       rec_off[j] = rec_total;
-      rec_total = align_up(rec_total + capacity[j] * pjs[j].record_bytes, 256);
+      rec_total = align_up(rec_total + capacity[j] * sizeof(Cand), 256);
     }
     ws->blob.ensure(std::max<size_t>(blob_total, 256));
     ws->records.ensure(std::max<size_t>(rec_total, 256));
@@ -1038,7 +718,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     // the level table overflowed (the levels are then rebuilt from them on the host) or the set is
     // small; otherwise the result set is selected on the device and only it is copied out.
     bool rerun = false;
-    std::vector<std::vector<uint8_t>> recs(nj);
+    std::vector<std::vector<Cand>> recs(nj);
     std::vector<Outcome> outc(nj);
     uint64_t d2h_bytes = cnt.size() * sizeof(unsigned long long) + 8;
     for (size_t j = 0; j < nj; ++j) {
@@ -1049,14 +729,14 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       d2h_bytes += kLevelSlots * sizeof(LevelSlot);
       const uint64_t n = std::min<uint64_t>(cj[kCandidates], capacity[j]);
       if (cj[kLevelOverflow]) {
-        recs[j].resize(n * pjs[j].record_bytes);
+        recs[j].resize(n);
         if (n)
-          CUDA_CHECK(cudaMemcpy(recs[j].data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], recs[j].size(),
+          CUDA_CHECK(cudaMemcpy(recs[j].data(), static_cast<uint8_t*>(ws->records.p) + rec_off[j], n * sizeof(Cand),
                                 cudaMemcpyDeviceToHost));
-        d2h_bytes += recs[j].size();
+        d2h_bytes += n * sizeof(Cand);
       }
       const bool may_rerun = !pjs[j].max_results && pjs[j].passes + attempt < 2;
-      outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, kRerunRecordBytes / pjs[j].record_bytes);
+      outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, kRerunRecordBytes / sizeof(Cand));
       if (outc[j].rerun) {
         capacity[j] = outc[j].rerun_capacity;
         fixed_threshold[j] = true;
@@ -1085,23 +765,9 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       r.levels_exact = o.levels_exact;
       r.candidates = cj[kCandidates];
       r.truncated = cj[kRecordsFull] != 0 || r.candidates > capacity[j];
-      const uint8_t* d_recs = static_cast<const uint8_t*>(ws->records.p) + rec_off[j];
-      bool done = false;
-      if (!cj[kLevelOverflow] && o.levels_exact)
-        done = select_records_on_device(ws->select, ws->stream, pjs[j], d_recs, n, o.value, r);
-      if (!done) {
-        if (recs[j].empty() && n) {
-          recs[j].resize(n * pjs[j].record_bytes);
-          CUDA_CHECK(cudaMemcpy(recs[j].data(), d_recs, recs[j].size(), cudaMemcpyDeviceToHost));
-          d2h_bytes += recs[j].size();
-        }
-        if (pjs[j].prec == 1)
-          select_results<double>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
-        else
-          select_results<float>(pjs[j], recs[j], n, r, o.levels_exact, o.tstar);
-      } else {
-        d2h_bytes += r.objective.size() + r.sub_objective.size() + r.species.size() + r.sro.size() + r.id.size() * 8;
-      }
+      const Cand* d_cands = reinterpret_cast<const Cand*>(static_cast<const uint8_t*>(ws->records.p) + rec_off[j]);
+      finish_selection(ws->select, ws->stream, pjs[j], descs[j], d_cands, n, recs[j], o, !cj[kLevelOverflow], r,
+                       d2h_bytes);
       r.level_value = std::move(o.value);
       r.level_count = std::move(o.count);
       r.level_checksum = std::move(o.checksum);
@@ -1207,6 +873,7 @@ struct ServerJob {
   uint64_t ring_begin = 0, ring_end = 0;
   uint64_t t_submit = 0, t_admit = 0;
   uint64_t h2d_bytes = 0;
+  JobDesc dev_desc{};         // the descriptor as uploaded (device pointers into the arena)
 };
 
 struct LaunchSlot {
@@ -1215,7 +882,7 @@ struct LaunchSlot {
   bool busy = false;
 };
 
-// One ring of tiles per shared-memory class; launches of sqsg_engine serve a ring on the SMs that
+// One ring of tiles per shared-memory class; launches of its kernel serve a ring on the SMs that
 // the owner table gives it.
 struct Ring {
   EngineKernel kernel = nullptr;  // ring 0: sqsg_engine_mask (bit-mask jobs); others: sqsg_engine_wide
@@ -1259,7 +926,7 @@ struct ServerState {
     std::unique_ptr<ServerJob> job;
     std::vector<unsigned long long> cnt;
     std::vector<LevelSlot> levels;
-    std::vector<uint8_t> records;
+    std::vector<Cand> records;
   };
   std::deque<Collected> collected;
   std::mutex m;
@@ -1318,7 +985,7 @@ static void arena_free(ServerState& S, size_t off, size_t bytes) {
 }
 
 static size_t job_footprint(const ServerJob& J) {
-  return align_up(J.pj.blob.size(), 256) + align_up(J.capacity * J.pj.record_bytes, 256);
+  return align_up(J.pj.blob.size(), 256) + align_up(J.capacity * sizeof(Cand), 256);
 }
 
 // Admits the oldest pending job if a slot, ring space and arena memory are free: uploads its data,
@@ -1368,6 +1035,7 @@ static bool try_admit(ServerState& S) {
   // copies only: a memset kernel would wait for SMs held by the running persistent kernels
   CUDA_CHECK(cudaMemcpyAsync(d.levels, S.h_zero, kLevelSlots * sizeof(LevelSlot), cudaMemcpyHostToDevice, S.copy));
   CUDA_CHECK(cudaMemcpyAsync(S.d_jobs + slot, &d, sizeof(d), cudaMemcpyHostToDevice, S.copy));
+  J.dev_desc = d;
   const uint64_t n = J.tiles.size();
   const uint64_t pos = R.published % kRingCap;
   const uint64_t first = std::min<uint64_t>(n, kRingCap - pos);
@@ -1407,8 +1075,8 @@ static void collect(ServerState& S, uint32_t slot) {
   CUDA_CHECK(cudaStreamSynchronize(S.copy));
   const uint64_t n = std::min<uint64_t>(c.cnt[kCandidates], J.capacity);
   if (c.cnt[kLevelOverflow] && n) {
-    c.records.resize(n * J.pj.record_bytes);
-    CUDA_CHECK(cudaMemcpyAsync(c.records.data(), S.arena + J.arena_off + J.blob_bytes, c.records.size(),
+    c.records.resize(n);
+    CUDA_CHECK(cudaMemcpyAsync(c.records.data(), S.arena + J.arena_off + J.blob_bytes, n * sizeof(Cand),
                                cudaMemcpyDeviceToHost, S.copy));
     CUDA_CHECK(cudaStreamSynchronize(S.copy));
   }
@@ -1442,10 +1110,11 @@ static void finalizer_loop(ServerState* Sp) {
     const unsigned long long* cnt = c.cnt.data();
     const uint64_t n = std::min<uint64_t>(cnt[kCandidates], J.capacity);
     const uint64_t arena_records =
-        (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) / J.pj.record_bytes;
+        (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) / sizeof(Cand);
     Run r;
     std::string error;
     Outcome o;
+    uint64_t fin_d2h = c.records.size() * sizeof(Cand);
     try {
       o = assess(J.pj, cnt, c.levels, c.records, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
       if (!o.rerun) {
@@ -1456,22 +1125,10 @@ static void finalizer_loop(ServerState* Sp) {
         r.levels_exact = o.levels_exact;
         r.candidates = cnt[kCandidates];
         r.truncated = cnt[kRecordsFull] != 0 || r.candidates > J.capacity;
-        const uint8_t* d_recs = S.arena + J.arena_off + J.blob_bytes;
-        bool done = false;
-        if (!cnt[kLevelOverflow] && o.levels_exact && stream)
-          done = select_records_on_device(scratch, stream, J.pj, d_recs, n, o.value, r);
-        if (!done) {
-          if (c.records.empty() && n) {
-            if (!stream) throw cuda_error("no stream to download records on");
-            c.records.resize(n * J.pj.record_bytes);
-            CUDA_CHECK(cudaMemcpyAsync(c.records.data(), d_recs, c.records.size(), cudaMemcpyDeviceToHost, stream));
-            CUDA_CHECK(cudaStreamSynchronize(stream));
-          }
-          if (J.pj.prec == 1)
-            select_results<double>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
-          else
-            select_results<float>(J.pj, c.records, n, r, o.levels_exact, o.tstar);
-        }
+        if (!stream) throw cuda_error("no stream to select the result set on");
+        const Cand* d_cands = reinterpret_cast<const Cand*>(S.arena + J.arena_off + J.blob_bytes);
+        finish_selection(scratch, stream, J.pj, J.dev_desc, d_cands, n, c.records, o, !cnt[kLevelOverflow], r,
+                         fin_d2h);
         r.level_value = std::move(o.value);
         r.level_count = std::move(o.count);
         r.level_checksum = std::move(o.checksum);
@@ -1488,8 +1145,7 @@ static void finalizer_loop(ServerState* Sp) {
         r.stats.timings_ns[SQSG_TIMING_CHUNK_SETUP] = J.t_admit - J.t_submit;
         r.stats.timings_ns[SQSG_TIMING_LOOP] = t_end - J.t_admit;
         r.h2d_bytes = J.h2d_bytes;
-        r.d2h_bytes = kLevelSlots * sizeof(LevelSlot) + kNumCounters * 8 + c.records.size() + r.objective.size() +
-                      r.sub_objective.size() + r.species.size() + r.sro.size() + r.id.size() * 8;
+        r.d2h_bytes = kLevelSlots * sizeof(LevelSlot) + kNumCounters * 8 + fin_d2h;
       }
     } catch (std::exception const& ex) {
       error = ex.what();
@@ -1694,7 +1350,7 @@ struct sqsg_run {
 
 extern "C" {
 
-const char* sqsg_version(void) { return "sqsgen_b200 0.1.0 (abi 1, sm_100a)"; }
+const char* sqsg_version(void) { return "sqsgen_b200 0.2.0 (abi 2, sm_100a)"; }
 
 size_t sqsg_last_error(char* buf, size_t len) {
   const std::string& e = g_last_error;
@@ -1817,6 +1473,56 @@ static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, co
       for (size_t k = 0; k < idx.size(); ++k) done[idx[k]].reset(new sqsg_run{std::move(runs[k])});
     }
     for (uint32_t j = 0; j < n; ++j) out[j] = done[j].release();
+  });
+}
+
+sqsg_status sqsg_set_option(const char* name, int64_t value) {
+  return guarded([&] {
+    const int k = option_index(name);
+    if (k < 0) throw std::invalid_argument(std::string("unknown option: ") + (name ? name : "(null)"));
+    if (k == kOptStageWaitNs && value <= 0) throw std::out_of_range("stage_wait_ns must be positive");
+    g_options[k].store(value);
+  });
+}
+
+sqsg_status sqsg_get_option(const char* name, int64_t* value) {
+  return guarded([&] {
+    const int k = option_index(name);
+    if (k < 0) throw std::invalid_argument(std::string("unknown option: ") + (name ? name : "(null)"));
+    if (!value) throw std::invalid_argument("null pointer");
+    *value = g_options[k].load();
+  });
+}
+
+sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
+  return guarded([&] {
+    if (!job || !plan) throw std::invalid_argument("null pointer");
+    PreparedJob pj = prepare(*job, 0);
+    std::memset(plan, 0, sizeof(*plan));
+    const JobDesc& d = pj.desc;
+    plan->n_parts = d.n_parts;
+    plan->smem_bytes = d.smem_bytes;
+    plan->record_bytes = d.record_bytes;
+    const bool bitmask = d.k2 != 0;
+    std::snprintf(plan->kernel, sizeof(plan->kernel), "%s", bitmask ? "sqsg_engine_mask" : "sqsg_engine_wide");
+    for (uint32_t p = 0; p < d.n_parts; ++p) {
+      const PartDesc& P = d.parts[p];
+      plan->parts[p].path = bitmask ? SQSG_PATH_BITMASK : SQSG_PATH_GENERAL;
+      plan->parts[p].stream_narrow = static_cast<int32_t>(P.stream_narrow);
+      plan->parts[p].stream_staged = P.stream_global ? 0 : 1;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) == cudaSuccess && job->device >= 0 && job->device < ndev) {
+      CUDA_CHECK(cudaSetDevice(job->device));
+      if (d.smem_bytes <= max_dynamic_smem(job->device)) {
+        configure_kernel(d.smem_bytes);
+        int per_sm = 0;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_for(bitmask), kBlock, d.smem_bytes));
+        plan->ctas_per_sm = static_cast<uint32_t>(per_sm);
+      }
+    } else {
+      cudaGetLastError();
+    }
   });
 }
 
@@ -2096,6 +1802,18 @@ sqsg_status sqsg_server_stats(sqsg_server* server, sqsg_server_counters* stats) 
     size_t free_bytes = 0;
     for (auto& [o, n] : S.free_list) free_bytes += n;
     stats->arena_free_bytes = free_bytes;
+  });
+}
+
+sqsg_status sqsg_server_running(sqsg_server* server, uint32_t* launches) {
+  return guarded([&] {
+    if (!server || !launches) throw std::invalid_argument("null pointer");
+    ServerState& S = server->s;
+    std::lock_guard<std::mutex> l(S.m);
+    uint32_t n = 0;
+    for (auto& R : S.rings)
+      for (auto& L : R.ls) n += L.busy ? 1u : 0u;
+    *launches = n;
   });
 }
 

@@ -38,17 +38,27 @@ __host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
 }
 
 
+// splitmix64 finalizer (Steele, Lea, Flood 2014): the per-id hash behind the order-independent level
+// checksums.
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
 constexpr int kBlock = 128;       // threads per CTA (each owns one configuration)
-constexpr int kMinBlocks = 5;     // sqsg_engine: CTAs per SM the register budget must allow (<= 102 registers)
+constexpr int kMinBlocks = 5;     // sqsg_engine_mask: CTAs per SM the register budget must allow (<= 102 registers)
 constexpr int kK2MaxShells = 4;   // shells of the binary bit-mask path (per-shell counters in registers)
 constexpr int kMinBlocksWide = 4; // sqsg_engine_wide (general path): 128 registers, no spills in the pair loop
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
 constexpr int kMaxSpecies = 8;    // K per part handled by the packed-row counter
 constexpr int kMaxGroup = 255;    // neighbours per (shell, site) group (8-bit row fields)
-constexpr uint32_t kWaitLimit = 1u << 26;  // bounded mbarrier wait (iterations)
+constexpr uint64_t kWaitNs = 2000000000ull;  // default bound of a staging wait (2 s of %globaltimer)
 constexpr int kCtaLevelSlots = 64;       // per-CTA objective-level hash (shared memory)
 constexpr int kLevelSlots = 4096;        // per-job objective-level hash (global memory)
+constexpr int kMaxKeep = 1023;           // largest `keep` this build handles
 
 // Counters of one job in device memory (unsigned long long each).
 enum Counter : int {
@@ -65,6 +75,19 @@ enum Counter : int {
 };
 
 enum DeviceError : unsigned long long { kErrNone = 0, kErrStageTimeout = 1, kErrBadJob = 2 };
+
+// JobDesc::debug bits (set through sqsg_set_option, never by default).
+enum DebugFlag : uint32_t {
+  kDebugSkipStaging = 1u,  // expect the staged bytes but issue no copy: the staging wait runs out
+};
+
+// A candidate in the job's record buffer: the objective (as double: exact for float jobs too) and the
+// configuration id. Configurations depend only on (job, id), so the full record (species, per-part
+// objective, SRO) is rebuilt on the device for the selected candidates only (sqsg_materialize).
+struct Cand {
+  double objective;
+  unsigned long long id;
+};
 
 // One distinct objective value seen at or below the search threshold, with the number of
 // evaluations that produced it and two order-independent 32-bit sums of hashes of their ids.
@@ -117,8 +140,11 @@ struct JobDesc {
   uint32_t kw;            // 1: every part has K <= 4 (32-bit row), 2: K <= 8 (64-bit row)
   uint32_t k2;            // 0: general path; 1: binary bitmask path with N <= 32; 2: with N <= 64
   uint32_t keep;
-  uint32_t record_bytes;
-  uint32_t smem_bytes;
+  uint32_t record_bytes;  // bytes of a full (materialized) record; the engine itself writes Cand
+  uint32_t smem_bytes;    // dynamic shared memory of the engine launch
+  uint32_t smem_full;     // dynamic shared memory of the general layout (materialize, trace)
+  uint32_t big_off;       // keep >= 32: per-warp best lists of big_len doubles at this offset
+  uint32_t big_len;       // entries per warp list in shared memory (0: the list is one register per lane)
   uint32_t trace;         // 1: write every evaluated configuration to the trace buffers
   uint32_t trace_species_stride, trace_bonds_stride;
   uint64_t seed;
@@ -134,6 +160,9 @@ struct JobDesc {
   uint64_t* trace_id;
   uint64_t trace_capacity;
   uint64_t trace_base;    // id of the first traced configuration
+  uint64_t wait_ns;       // bound of the staging wait (%globaltimer nanoseconds)
+  uint32_t debug;         // DebugFlag bits
+  uint32_t reserved_dbg;
   PartDesc parts[kMaxParts];
 };
 

@@ -1,4 +1,4 @@
-// Device side of the SQS engine (included once, by engine.cu).
+// Device side of the SQS engine (included by the kernel translation units kernel_*.cu).
 //
 // Per configuration a thread
 //   1. (random mode) Fisher-Yates-shuffles every window of every part of the packed initial
@@ -68,10 +68,18 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
-// Bounded wait for the phase `parity` of bar; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for the phase `parity` of bar, bounded by limit_ns of the global timer (read every 64 polls);
+// false when the bound ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long limit_ns) {
   const uint32_t addr = smem_u32(bar);
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+  const unsigned long long t0 = global_ns();
+  for (uint32_t it = 1;; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -79,8 +87,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 63u) == 0 && global_ns() - t0 > limit_ns) return false;
   }
-  return false;
 }
 
 // ------------------------------------------------------------------------------ per-part kernels
@@ -303,15 +311,6 @@ __device__ __forceinline__ void unrank_window(uint8_t* col, const PartDesc& P, u
 }
 
 // ------------------------------------------------------------------------------ objective levels
-// splitmix64 finalizer (Steele, Lea, Flood 2014): the per-id hash behind the order-independent level
-// checksums.
-__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
-  z += 0x9e3779b97f4a7c15ull;
-  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-  return z ^ (z >> 31);
-}
-
 __device__ __forceinline__ uint32_t level_hash(unsigned long long key, uint32_t mask) {
   return static_cast<uint32_t>(mix64(key)) & mask;
 }
@@ -369,31 +368,89 @@ __device__ __forceinline__ void flush_levels(LevelSlot* tab, const JobDesc& J) {
 }
 
 // ------------------------------------------------------------------------------ best-N bookkeeping
-// Each warp keeps the up-to-32 best distinct objectives it has seen, one per lane, ascending. Its
-// (keep+1)-th entry bounds the job's (keep+1)-th best distinct objective from above, like the
-// reference's search threshold nth_best(keep) (results.h:78-82, sqs.h:203-206); the minimum over
+// Each warp keeps the best distinct objectives it has seen, ascending: with keep <= 31 one entry per
+// lane (32 entries in registers), with larger keep a list of big_len >= keep+1 entries in shared
+// memory. Its (keep+1)-th entry bounds the job's (keep+1)-th best distinct objective from above, like
+// the reference's search threshold nth_best(keep) (results.h:78-82, sqs.h:203-206); the minimum over
 // warps is kept in the job's threshold counter. Every configuration whose objective is at or below
 // the current bound is appended to the candidate buffer, so the buffer holds every configuration at
 // or below the final (keep+1)-th best distinct objective.
 struct WarpState {
-  double list;          // lane's entry of the warp list (+inf = empty)
+  double list;          // lane's entry of the register list (+inf = empty); unused with `big`
   double list_thr;      // warp-uniform (keep+1)-th entry
+  double* big;          // keep >= 32: this warp's list in shared memory (nullptr otherwise)
+  uint32_t big_len;
   unsigned long long published_thr, published_best;
   bool records_full;    // lane 0: the job's record buffer is known to be full (it never empties)
-  __device__ void reset() {
+  // Called by every thread of the warp at a job switch.
+  __device__ void reset(const JobDesc& J, uint8_t* smem) {
     list = __longlong_as_double(0x7ff0000000000000ll);
     list_thr = list;
     published_thr = ~0ull;
     published_best = ~0ull;
     records_full = false;
+    big = nullptr;
+    big_len = J.big_len;
+    if (big_len) {
+      big = reinterpret_cast<double*>(smem + J.big_off) + (threadIdx.x >> 5) * big_len;
+      for (uint32_t k = threadIdx.x & 31; k < big_len; k += 32) big[k] = list;
+      __syncwarp();
+    }
   }
 };
+
+struct BigUpdate {
+  double thr;
+  bool moved;
+};
+
+// The shared-memory list (keep >= 32): membership of each lane's value by binary search, then one
+// insertion per distinct new value below the (keep+1)-th entry, lane order; an insertion at `pos`
+// moves entries [pos, len-1) up by one, highest block of 32 first (each block is read before it is
+// written, and its lowest entry reads the block below, which is written later). Rare after the first
+// tiles, so it is kept out of line.
+static __device__ __noinline__ BigUpdate big_list_update(double* L, uint32_t n, double v_mine, bool fresh, uint32_t keep,
+                                                  double thr) {
+  const int lane = threadIdx.x & 31;
+  if (fresh) {
+    uint32_t lo = 0, hi = n;  // first entry >= v_mine
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (L[mid] < v_mine)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo < n && L[lo] == v_mine) fresh = false;
+  }
+  unsigned fm = __ballot_sync(0xffffffffu, fresh);
+  const bool moved = fm != 0;
+  while (fm) {
+    const double v = __shfl_sync(0xffffffffu, v_mine, __ffs(fm) - 1);
+    fm &= ~__ballot_sync(0xffffffffu, v_mine == v);  // lanes with the same value: one insertion
+    if (v < thr) {
+      uint32_t c = 0;
+      for (uint32_t k = lane; k < n; k += 32) c += L[k] < v ? 1u : 0u;
+      const uint32_t pos = __reduce_add_sync(0xffffffffu, c);
+      for (int blk = static_cast<int>(n >> 5) - 1; blk >= static_cast<int>(pos >> 5); --blk) {
+        const uint32_t idx = static_cast<uint32_t>(blk) * 32 + lane;
+        const double nv = idx > pos ? L[idx - 1] : v;
+        __syncwarp();
+        if (idx >= pos) L[idx] = nv;
+        __syncwarp();
+      }
+      thr = L[keep];
+    }
+  }
+  return BigUpdate{thr, moved};
+}
 
 // Per-warp level accumulators of the bit-mask path, indexed by position in the warp list: count,
 // low and high checksum halves of the configurations kept at list[i] (3 x 32 words per warp). While
 // the list does not change, a kept value is at the position its lower-bound search found, so each
 // lane adds itself there with three shared-memory atomics instead of the warp looping over distinct
 // values; before the list changes and at the end of every tile the warp moves them into the CTA table.
+// (Register list only: with a shared-memory list the per-value loop runs instead.)
 static __shared__ uint32_t s_wacc[kBlock / 32 * 96];
 
 __device__ __forceinline__ uint32_t* warp_acc() { return s_wacc + (threadIdx.x >> 5) * 96; }
@@ -410,21 +467,6 @@ __device__ __forceinline__ void warp_acc_flush(const WarpState& ws, LevelSlot* c
     acc[64 + lane] = 0;
   }
   __syncwarp();
-}
-
-template <class T>
-__device__ __forceinline__ void write_record(const JobDesc& J, uint8_t* smem, uint64_t idx, T total, uint64_t id,
-                                             int t) {
-  uint8_t* rec = J.records + idx * J.record_bytes;
-  *reinterpret_cast<T*>(rec) = total;
-  *reinterpret_cast<uint64_t*>(rec + 8) = id;
-  for (uint32_t p = 0; p < J.n_parts; ++p) {
-    const PartDesc& P = J.parts[p];
-    const uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
-    for (uint32_t x = 0; x < P.n_sites; ++x) rec[P.rec_species_off + x] = col[site_off(x)] >> 3;
-    T* sro = reinterpret_cast<T*>(rec + P.rec_sro_off);
-    *reinterpret_cast<T*>(rec + P.rec_obj_off) = objective_part<T>(smem, P, t, sro);
-  }
 }
 
 template <class T>
@@ -448,29 +490,29 @@ __device__ __forceinline__ void write_trace(const JobDesc& J, uint8_t* smem, uin
   J.trace_id[g] = id;
 }
 
-struct NoPrep {
-  __device__ __forceinline__ void operator()() const {}
-};
-
-// `prep` runs right before a record is written (the binary path materialises the lane's species and
-// bond counts in shared memory only then).
 // ACC (bit-mask path): kept configurations go to the warp's level accumulators while the list is
-// unchanged; otherwise straight to the CTA table.
-template <class T, bool ACC = false, class Prep = NoPrep>
-__device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, WarpState& ws,
-                                                  bool pass, T total, T thr_g, uint64_t id, int t,
-                                                  const Prep& prep = Prep()) {
+// unchanged; otherwise (and always with a shared-memory list) straight to the CTA table.
+template <class T, bool ACC = false>
+__device__ __forceinline__ void handle_candidates(const JobDesc& J, LevelSlot* ctab, WarpState& ws, bool pass, T total,
+                                                  T thr_g, uint64_t id, int t) {
   const int lane = t & 31;
   unsigned m = __ballot_sync(0xffffffffu, pass);
   if (!m) return;
   const double v_mine = static_cast<double>(total);
   // Only values below the warp's (keep+1)-th entry that are not in its list yet change the list.
-  // Membership: the lower bound of each lane's value in the ascending list (one entry per lane),
-  // found by a five-step shuffle search; then one insertion per distinct new value, lane order.
   bool fresh = pass && v_mine < ws.list_thr;
   int lo = 0;
   bool moved = false;
-  if (ACC || __any_sync(0xffffffffu, fresh)) {
+  const bool big = !ACC && ws.big != nullptr;  // warp-uniform; bit-mask jobs keep the register list (keep < 32)
+  if (big) {
+    if (__any_sync(0xffffffffu, fresh)) {
+      const BigUpdate u = big_list_update(ws.big, ws.big_len, v_mine, fresh, J.keep, ws.list_thr);
+      ws.list_thr = u.thr;
+      moved = u.moved;
+    }
+  } else if (ACC || __any_sync(0xffffffffu, fresh)) {
+    // Membership: the lower bound of each lane's value in the ascending list (one entry per lane),
+    // found by a five-step shuffle search; then one insertion per distinct new value, lane order.
 #pragma unroll
     for (int step = 16; step > 0; step >>= 1) {
       const double e = __shfl_sync(0xffffffffu, ws.list, lo + step - 1);
@@ -501,7 +543,7 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
       atomicMin(&J.counters[kThreshold], ot);
       ws.published_thr = ot;
     }
-    const unsigned long long ob = ord_bits(ws.list);
+    const unsigned long long ob = ord_bits(big ? ws.big[0] : ws.list);
     if (ob < ws.published_best) {
       atomicMin(&J.counters[kBest], ob);
       ws.published_best = ob;
@@ -512,7 +554,7 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
   const bool keep_it = pass && v_mine <= bound;
   const unsigned km = __ballot_sync(0xffffffffu, keep_it);
   if (!km) return;
-  if (ACC && !moved) {
+  if (ACC && !big && !moved) {
     // no insertion this step: a kept value (<= the (keep+1)-th entry) is in the list at lo
     if (keep_it) {
       const unsigned long long h = mix64(id);
@@ -558,10 +600,7 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, uint8_t* sme
   base = __shfl_sync(0xffffffffu, base, 0);
   if (keep_it && base != ~0ull) {
     const uint64_t idx = base + __popc(km & ((1u << lane) - 1u));
-    if (idx < J.capacity) {
-      prep();
-      write_record<T>(J, smem, idx, total, id, t);
-    }
+    if (idx < J.capacity) reinterpret_cast<Cand*>(J.records)[idx] = Cand{v_mine, id};
   }
 }
 
@@ -616,7 +655,7 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
     const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
     const bool pass = active && static_cast<double>(total) <= bound;
     const uint64_t id = tile.start + my_off + it;
-    handle_candidates<T>(J, smem, ctab, ws, pass, total, thr_g, id, t);
+    handle_candidates<T>(J, ctab, ws, pass, total, thr_g, id, t);
     if (J.trace && active) write_trace<T>(J, smem, id - J.trace_base, total, id, t);
     if (systematic && active && it + 1 < my_count)
       next_permutation(part_base(smem, J.parts[0]) + J.parts[0].col_off + 4 * t, wlo, wn);
@@ -858,9 +897,7 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
     const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
     const bool pass = active && static_cast<double>(total) <= bound;
     const uint64_t id = tile.start + my_off + it;
-    const V vv = v;
-    handle_candidates<T, true>(J, smem, ctab, ws, pass, total, thr_g, id, t,
-                               [&]() { k2_materialize<V, W>(smem, P, t, vv); });
+    handle_candidates<T, true>(J, ctab, ws, pass, total, thr_g, id, t);
     if (J.trace && active) {
       k2_materialize<V, W>(smem, P, t, v);
       write_trace<T>(J, smem, id - J.trace_base, total, id, t);
@@ -992,7 +1029,7 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
   uint32_t cur_gen = 0;
   uint32_t phase = 0;
   WarpState ws;
-  ws.reset();
+  ws.big = nullptr;  // set with the first job
   if (threadIdx.x == 0) {
     s_counted = 0;
     if (live) {
@@ -1034,11 +1071,17 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
         uint32_t bytes = 0;
         for (uint32_t p = 0; p < sj.n_parts; ++p) bytes += sj.parts[p].static_bytes;
         mbar_expect_tx(&s_bar, bytes);
-        for (uint32_t p = 0; p < sj.n_parts; ++p)
-          bulk_copy_g2s(smem + sj.parts[p].smem_off, sj.blob + sj.parts[p].blob_off, sj.parts[p].static_bytes,
-                        &s_bar);
+        if (!(sj.debug & kDebugSkipStaging))  // debug: nothing arrives, the wait below runs out
+          for (uint32_t p = 0; p < sj.n_parts; ++p)
+            bulk_copy_g2s(smem + sj.parts[p].smem_off, sj.blob + sj.parts[p].blob_off, sj.parts[p].static_bytes,
+                          &s_bar);
       }
-      if (!mbar_wait(&s_bar, phase)) atomicOr(&s_fail, 1u);
+      if (!mbar_wait(&s_bar, phase, sj.wait_ns)) {
+        atomicOr(&s_fail, 1u);
+        // copies that were issued may still be landing in this CTA's shared memory: give them one
+        // more bounded wait before the CTA leaves
+        if (!(sj.debug & kDebugSkipStaging)) mbar_wait(&s_bar, phase, sj.wait_ns);
+      }
       phase ^= 1u;
       __syncthreads();
       if (s_fail) {
@@ -1050,7 +1093,7 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
       }
       cur = static_cast<int>(tile.job);
       cur_gen = tile.gen;
-      ws.reset();
+      ws.reset(sj, smem);
     }
     if (sj.mode == 1)
       dispatch_tile<true, GENERAL, MASK>(sj, smem, ctab, tile, ws);
@@ -1082,30 +1125,6 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
     if (s_counted) atomicAdd(&q->alive[sm_id()], ~0u);
     atomicAdd(&q->exited, 1u);
   }
-}
-
-// The same engine compiled three ways. sqsg_engine_mask: the binary bit-mask path alone at 96
-// registers (5 CTAs per SM; without the general path's code nothing forces spills).
-// sqsg_engine_wide: the general path alone at 128 registers (its pair loop spills at 96 and its
-// shared memory allows at most 4 CTAs anyway); a bit-mask job given to it runs the general path,
-// which holds all its data too and gives the same result. sqsg_engine: both paths at 96 registers,
-// for callers that launch one kernel for any job.
-__global__ void __launch_bounds__(kBlock, kMinBlocks)
-    sqsg_engine(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
-                const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body<true, true>(jobs, tiles, n_tiles, q, cancel, status, done);
-}
-
-__global__ void __launch_bounds__(kBlock, kMinBlocks)
-    sqsg_engine_mask(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
-                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body<false, true>(jobs, tiles, n_tiles, q, cancel, status, done);
-}
-
-__global__ void __launch_bounds__(kBlock, kMinBlocksWide)
-    sqsg_engine_wide(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
-                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body<true, false>(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
 }  // namespace sqsg

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <string>
 
+#include "kernels.h"
 #include "select.h"
 #include "sqsg_internal.h"
 
@@ -34,7 +35,7 @@ namespace sqsg {
 // Stream-ordered allocations: growing a buffer never waits for other streams' kernels (a plain
 // cudaFree would wait for the whole device, including persistent kernels of other jobs).
 void SelectScratch::release() {
-  for (int k = 0; k < 16; ++k) {
+  for (int k = 0; k < kSlots; ++k) {
     if (buf[k]) cudaFreeAsync(buf[k], stream);
     buf[k] = nullptr;
     size[k] = 0;
@@ -116,23 +117,14 @@ void* SelectScratch::get(int slot, size_t bytes) {
 
 namespace {
 
-constexpr int kMaxLevels = 32;
-
-struct Levels {
-  unsigned long long key[kMaxLevels];  // ord_bits of the level values, ascending
-  uint32_t n;
-};
-
-__device__ __forceinline__ double record_objective(const uint8_t* r, uint32_t tsz) {
-  return tsz == 8 ? *reinterpret_cast<const double*>(r) : static_cast<double>(*reinterpret_cast<const float*>(r));
-}
-
-__device__ __forceinline__ int level_of(const Levels& L, unsigned long long key) {
-  int lo = 0, hi = static_cast<int>(L.n) - 1;
+// Level keys (ord_bits of the keep+1 smallest distinct objectives, ascending) in device memory.
+__device__ __forceinline__ int level_of(const unsigned long long* __restrict__ L, uint32_t nl, unsigned long long key) {
+  int lo = 0, hi = static_cast<int>(nl) - 1;
   while (lo <= hi) {
     const int mid = (lo + hi) >> 1;
-    if (L.key[mid] == key) return mid;
-    if (L.key[mid] < key)
+    const unsigned long long k = L[mid];
+    if (k == key) return mid;
+    if (k < key)
       lo = mid + 1;
     else
       hi = mid - 1;
@@ -140,38 +132,43 @@ __device__ __forceinline__ int level_of(const Levels& L, unsigned long long key)
   return -1;
 }
 
-__global__ void k_flag_levels(const uint8_t* __restrict__ recs, uint32_t rb, uint32_t tsz, uint32_t n, Levels L,
-                              uint8_t* __restrict__ flag, uint32_t* __restrict__ iota) {
+__global__ void k_flag_levels(const Cand* __restrict__ c, uint32_t n, const unsigned long long* __restrict__ L,
+                              uint32_t nl, uint8_t* __restrict__ flag, uint32_t* __restrict__ iota) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  flag[i] = level_of(L, ord_bits(record_objective(recs + static_cast<size_t>(i) * rb, tsz))) >= 0 ? 1 : 0;
+  flag[i] = level_of(L, nl, ord_bits(c[i].objective)) >= 0 ? 1 : 0;
   iota[i] = i;
 }
 
-__global__ void k_keys(const uint8_t* __restrict__ recs, RecordLayout lay, const uint32_t* __restrict__ sel,
-                       uint32_t m, Levels L, uint32_t id_bits, bool with_hash, unsigned long long* __restrict__ key,
-                       uint32_t* __restrict__ pos, unsigned long long* __restrict__ hash) {
+__global__ void k_keys(const Cand* __restrict__ c, const uint32_t* __restrict__ sel, uint32_t m,
+                       const unsigned long long* __restrict__ L, uint32_t nl, uint32_t id_bits,
+                       unsigned long long* __restrict__ key, uint32_t* __restrict__ pos) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= m) return;
-  const uint8_t* r = recs + static_cast<size_t>(sel[j]) * lay.record_bytes;
-  const int lev = level_of(L, ord_bits(record_objective(r, lay.tsz)));
-  const unsigned long long id = *reinterpret_cast<const unsigned long long*>(r + 8);
-  key[j] = (static_cast<unsigned long long>(lev) << id_bits) | id;
+  const Cand x = c[sel[j]];
+  key[j] = (static_cast<unsigned long long>(level_of(L, nl, ord_bits(x.objective))) << id_bits) | x.id;
   pos[j] = j;
-  if (with_hash) {
-    unsigned long long h = 0xcbf29ce484222325ull;  // FNV-1a over the species bytes of all parts
-    for (uint32_t p = 0; p < lay.n_parts; ++p)
-      for (uint32_t x = 0; x < lay.n_sites[p]; ++x) h = (h ^ r[lay.species_off[p] + x]) * 0x100000001b3ull;
-    hash[j] = h;
-  }
 }
 
-__global__ void k_gather_hash(const unsigned long long* __restrict__ hash, const uint32_t* __restrict__ pos_s,
-                              uint32_t m, unsigned long long* __restrict__ h2, uint32_t* __restrict__ iota) {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= m) return;
-  h2[p] = hash[pos_s[p]];
-  iota[p] = p;
+// out[k] = candidate of sorted position order[k]
+__global__ void k_gather_cands(const Cand* __restrict__ c, const uint32_t* __restrict__ sel,
+                               const uint32_t* __restrict__ pos_s, const uint32_t* __restrict__ order, uint32_t m,
+                               Cand* __restrict__ out) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  out[k] = c[sel[pos_s[order ? order[k] : k]]];
+}
+
+__global__ void k_hash(const uint8_t* __restrict__ recs, RecordLayout lay, uint32_t m, unsigned long long* __restrict__ hash,
+                       uint32_t* __restrict__ iota) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint8_t* r = recs + static_cast<size_t>(j) * lay.record_bytes;
+  unsigned long long h = 0xcbf29ce484222325ull;  // FNV-1a over the species bytes of all parts
+  for (uint32_t p = 0; p < lay.n_parts; ++p)
+    for (uint32_t x = 0; x < lay.n_sites[p]; ++x) h = (h ^ r[lay.species_off[p] + x]) * 0x100000001b3ull;
+  hash[j] = h;
+  iota[j] = j;
 }
 
 __device__ __forceinline__ bool same_species(const uint8_t* a, const uint8_t* b, const RecordLayout& lay) {
@@ -181,22 +178,22 @@ __device__ __forceinline__ bool same_species(const uint8_t* a, const uint8_t* b,
   return true;
 }
 
-// r runs over the (hash, level, id) order; q[r] is the (level, id) position. A record is a repeat
-// when an earlier record of its hash run has the same level and the same species.
-__global__ void k_mark_repeats(const uint8_t* __restrict__ recs, RecordLayout lay, const uint32_t* __restrict__ sel,
-                               const uint32_t* __restrict__ pos_s, const unsigned long long* __restrict__ key_s,
-                               const unsigned long long* __restrict__ h2s, const uint32_t* __restrict__ q, uint32_t m,
-                               uint32_t id_bits, uint8_t* __restrict__ keep) {
+// Records are in (level, id) order; r runs over the (hash, position) order and q[r] is the record.
+// A record is a repeat when an earlier record of its hash run has the same level and the same species
+// (an earlier position in (level, id) order: the smallest id stays).
+__global__ void k_mark_repeats(const uint8_t* __restrict__ recs, RecordLayout lay,
+                               const unsigned long long* __restrict__ key_s, const unsigned long long* __restrict__ hs,
+                               const uint32_t* __restrict__ q, uint32_t m, uint32_t id_bits, uint8_t* __restrict__ keep) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= m) return;
   const uint32_t p = q[r];
   const unsigned long long lev = key_s[p] >> id_bits;
-  const uint8_t* a = recs + static_cast<size_t>(sel[pos_s[p]]) * lay.record_bytes;
+  const uint8_t* a = recs + static_cast<size_t>(p) * lay.record_bytes;
   bool repeat = false;
-  for (uint32_t r2 = r; r2 > 0 && h2s[r2 - 1] == h2s[r]; --r2) {
+  for (uint32_t r2 = r; r2 > 0 && hs[r2 - 1] == hs[r]; --r2) {
     const uint32_t p2 = q[r2 - 1];
     if ((key_s[p2] >> id_bits) != lev) continue;
-    if (same_species(recs + static_cast<size_t>(sel[pos_s[p2]]) * lay.record_bytes, a, lay)) {
+    if (same_species(recs + static_cast<size_t>(p2) * lay.record_bytes, a, lay)) {
       repeat = true;
       break;
     }
@@ -204,11 +201,9 @@ __global__ void k_mark_repeats(const uint8_t* __restrict__ recs, RecordLayout la
   keep[p] = repeat ? 0 : 1;
 }
 
-__global__ void k_fill(uint8_t* __restrict__ v, uint32_t m, uint8_t value, uint32_t* __restrict__ iota) {
+__global__ void k_iota(uint32_t m, uint32_t* __restrict__ iota) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  v[i] = value;
-  iota[i] = i;
+  if (i < m) iota[i] = i;
 }
 
 // kp: kept positions in (level, id) order. start[level] = index in kp of the level's first record.
@@ -239,14 +234,13 @@ struct OutLayout {
   uint32_t species_prefix[kMaxParts], sro_prefix[kMaxParts];
 };
 
-// One warp per selected record.
-__global__ void k_gather(const uint8_t* __restrict__ recs, RecordLayout lay, const uint32_t* __restrict__ sel,
-                         const uint32_t* __restrict__ pos_s, const uint32_t* __restrict__ order, uint32_t m,
-                         OutLayout o) {
+// One warp per selected record: record order[t] (or t) into dense output row t.
+__global__ void k_gather(const uint8_t* __restrict__ recs, RecordLayout lay, const uint32_t* __restrict__ order,
+                         uint32_t m, OutLayout o) {
   const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   if (t >= m) return;
-  const uint8_t* r = recs + static_cast<size_t>(sel[pos_s[order[t]]]) * lay.record_bytes;
+  const uint8_t* r = recs + static_cast<size_t>(order ? order[t] : t) * lay.record_bytes;
   const uint32_t tsz = lay.tsz;
   if (lane < tsz) o.objective[static_cast<size_t>(t) * tsz + lane] = r[lane];
   if (lane < 8) reinterpret_cast<uint8_t*>(o.id)[static_cast<size_t>(t) * 8 + lane] = r[8 + lane];
@@ -293,32 +287,71 @@ void sort_pairs(SelectScratch& S, cudaStream_t st, const K* kin, K* kout, const 
   SEL_CHECK(cub::DeviceRadixSort::SortPairs(tmp, b, kin, kout, vin, vout, n, 0, end_bit, st));
 }
 
+// Per-level cap on positions kp (m entries, (level, id) order): returns the kept count, into out.
+uint32_t cap_levels(SelectScratch& S, cudaStream_t st, const uint32_t* kp, const unsigned long long* key_s, uint32_t m,
+                    uint32_t id_bits, uint32_t n_levels, int64_t cap, uint32_t* out) {
+  auto* start = static_cast<uint32_t*>(S.get(13, size_t(n_levels) * 4));
+  auto* cflag = static_cast<uint8_t*>(S.get(11, m));
+  SEL_CHECK(cudaMemsetAsync(start, 0, size_t(n_levels) * 4, st));
+  k_level_starts<<<blocks(m, 256), 256, 0, st>>>(kp, key_s, m, id_bits, start);
+  SEL_CHECK(cudaGetLastError());
+  k_cap<<<blocks(m, 256), 256, 0, st>>>(kp, key_s, m, id_bits, start, static_cast<unsigned long long>(cap), cflag);
+  SEL_CHECK(cudaGetLastError());
+  return select_flagged(S, st, kp, cflag, out, m);
+}
+
 }  // namespace
 
-bool select_on_device(SelectScratch& S, cudaStream_t st, const RecordLayout& lay, const uint8_t* d_records,
-                      uint64_t n64, const std::vector<double>& levels, bool dedup, int64_t max_per_objective,
-                      uint64_t id_limit, SelectedSet& out) {
+uint64_t materialize(SelectScratch& S, cudaStream_t st, const Materializer& mat, const Cand* d_cands, uint32_t m,
+                     uint8_t* d_out) {
+  if (S.stream != st) {
+    S.release();
+    S.stream = st;
+  }
+  if (m == 0) return 0;
+  auto* d_job = static_cast<JobDesc*>(S.get(16, sizeof(JobDesc)));
+  auto* d_bad = static_cast<unsigned long long*>(S.get(17, 256));
+  SEL_CHECK(cudaMemcpyAsync(d_job, &mat.job, sizeof(JobDesc), cudaMemcpyHostToDevice, st));
+  SEL_CHECK(cudaMemsetAsync(d_bad, 0, 8, st));
+  const int err = raise_dynamic_smem(reinterpret_cast<const void*>(sqsg_materialize), mat.smem);
+  if (err != 0) throw cuda_error(std::string("cudaFuncSetAttribute(sqsg_materialize): ") +
+                                 cudaGetErrorString(static_cast<cudaError_t>(err)));
+  sqsg_materialize<<<blocks(m, kBlock), kBlock, mat.smem, st>>>(d_job, d_cands, m, d_out, d_bad);
+  SEL_CHECK(cudaGetLastError());
+  unsigned long long bad = 0;
+  SEL_CHECK(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, st));
+  SEL_CHECK(cudaStreamSynchronize(st));
+  return bad;
+}
+
+bool select_on_device(SelectScratch& S, cudaStream_t st, const RecordLayout& lay, const Cand* d_cands, uint64_t n64,
+                      const std::vector<double>& levels, bool dedup, int64_t max_per_objective, uint64_t id_limit,
+                      const Materializer& mat, SelectedSet& out) {
   out = SelectedSet{};
   if (S.stream != st) {  // buffers follow the stream they are used on
     S.release();
     S.stream = st;
   }
   if (n64 == 0 || levels.empty()) return true;
-  if (levels.size() > static_cast<size_t>(kMaxLevels) || n64 >= (1ull << 32)) return false;
+  if (n64 >= (1ull << 32)) return false;
+  uint32_t lev_bits = 1;
+  while ((1ull << lev_bits) < levels.size()) ++lev_bits;
   uint32_t id_bits = 1;
   while (id_bits < 64 && (id_limit >> id_bits) != 0) ++id_bits;
-  if (id_bits + 5 > 63) return false;
+  if (id_bits + lev_bits > 63) return false;
   const uint32_t n = static_cast<uint32_t>(n64);
-  Levels L{};
-  L.n = static_cast<uint32_t>(levels.size());
-  for (size_t k = 0; k < levels.size(); ++k) L.key[k] = ord_bits(levels[k]);
-  std::sort(L.key, L.key + L.n);
+  const uint32_t nl = static_cast<uint32_t>(levels.size());
+  std::vector<unsigned long long> keys_h(nl);
+  for (uint32_t k = 0; k < nl; ++k) keys_h[k] = ord_bits(levels[k]);
+  std::sort(keys_h.begin(), keys_h.end());
+  auto* d_levels = static_cast<unsigned long long*>(S.get(18, size_t(nl) * 8));
+  SEL_CHECK(cudaMemcpyAsync(d_levels, keys_h.data(), size_t(nl) * 8, cudaMemcpyHostToDevice, st));
 
-  // 1. records at one of the levels
+  // 1. candidates at one of the levels
   auto* flag = static_cast<uint8_t*>(S.get(0, n));
   auto* iota = static_cast<uint32_t*>(S.get(1, size_t(n) * 4));
   auto* sel = static_cast<uint32_t*>(S.get(2, size_t(n) * 4));
-  k_flag_levels<<<blocks(n, 256), 256, 0, st>>>(d_records, lay.record_bytes, lay.tsz, n, L, flag, iota);
+  k_flag_levels<<<blocks(n, 256), 256, 0, st>>>(d_cands, n, d_levels, nl, flag, iota);
   SEL_CHECK(cudaGetLastError());
   const uint32_t m = select_flagged(S, st, iota, flag, sel, n);
   if (m == 0) return true;
@@ -328,48 +361,59 @@ bool select_on_device(SelectScratch& S, cudaStream_t st, const RecordLayout& lay
   auto* key_s = static_cast<unsigned long long*>(S.get(4, size_t(m) * 8));
   auto* pos = static_cast<uint32_t*>(S.get(5, size_t(m) * 4));
   auto* pos_s = static_cast<uint32_t*>(S.get(6, size_t(m) * 4));
-  auto* hash = dedup ? static_cast<unsigned long long*>(S.get(7, size_t(m) * 8)) : nullptr;
-  k_keys<<<blocks(m, 256), 256, 0, st>>>(d_records, lay, sel, m, L, id_bits, dedup, key, pos, hash);
+  k_keys<<<blocks(m, 256), 256, 0, st>>>(d_cands, sel, m, d_levels, nl, id_bits, key, pos);
   SEL_CHECK(cudaGetLastError());
-  sort_pairs(S, st, key, key_s, pos, pos_s, m, static_cast<int>(id_bits + 5));
+  sort_pairs(S, st, key, key_s, pos, pos_s, m, static_cast<int>(id_bits + lev_bits));
 
-  // 3. repeats (random mode)
-  auto* keep = flag;  // reused: one byte per (level, id) position
-  uint32_t* iota2 = iota;
-  if (dedup) {
-    auto* h2 = static_cast<unsigned long long*>(S.get(10, size_t(m) * 8));
-    auto* h2s = key;  // the unsorted keys are no longer needed
-    auto* q = pos;    // nor the unsorted positions
-    k_gather_hash<<<blocks(m, 256), 256, 0, st>>>(hash, pos_s, m, h2, iota2);
+  // 3. systematic runs have no repeats: the per-objective cap applies before the records are rebuilt
+  const uint32_t* order = nullptr;  // positions (in sorted order) of what is rebuilt
+  uint32_t m1 = m;
+  if (!dedup && max_per_objective >= 0) {
+    auto* seq = static_cast<uint32_t*>(S.get(12, size_t(m) * 4));
+    k_iota<<<blocks(m, 256), 256, 0, st>>>(m, seq);
     SEL_CHECK(cudaGetLastError());
-    sort_pairs(S, st, h2, h2s, iota2, q, m, 64);
-    k_mark_repeats<<<blocks(m, 256), 256, 0, st>>>(d_records, lay, sel, pos_s, key_s, h2s, q, m, id_bits, keep);
-    SEL_CHECK(cudaGetLastError());
-  } else {
-    k_fill<<<blocks(m, 256), 256, 0, st>>>(keep, m, 1, iota2);
-    SEL_CHECK(cudaGetLastError());
-  }
-  auto* kp = static_cast<uint32_t*>(S.get(12, size_t(m) * 4));
-  uint32_t m2 = select_flagged(S, st, iota2, keep, kp, m);
-
-  // 4. per-objective cap
-  const uint32_t* order = kp;
-  if (max_per_objective >= 0 && m2 > 0) {
-    auto* start = static_cast<uint32_t*>(S.get(13, kMaxLevels * 4));
-    auto* cflag = static_cast<uint8_t*>(S.get(11, m2));
-    auto* fin = static_cast<uint32_t*>(S.get(14, size_t(m2) * 4));
-    SEL_CHECK(cudaMemsetAsync(start, 0, kMaxLevels * 4, st));
-    k_level_starts<<<blocks(m2, 256), 256, 0, st>>>(kp, key_s, m2, id_bits, start);
-    SEL_CHECK(cudaGetLastError());
-    k_cap<<<blocks(m2, 256), 256, 0, st>>>(kp, key_s, m2, id_bits, start,
-                                           static_cast<unsigned long long>(max_per_objective), cflag);
-    SEL_CHECK(cudaGetLastError());
-    m2 = select_flagged(S, st, kp, cflag, fin, m2);
+    auto* fin = static_cast<uint32_t*>(S.get(14, size_t(m) * 4));
+    m1 = cap_levels(S, st, seq, key_s, m, id_bits, nl, max_per_objective, fin);
     order = fin;
+    if (m1 == 0) return true;
+  }
+
+  // 4. full records of the selected candidates, in (level, id) order
+  auto* sc = static_cast<Cand*>(S.get(7, size_t(m1) * sizeof(Cand)));
+  k_gather_cands<<<blocks(m1, 256), 256, 0, st>>>(d_cands, sel, pos_s, order, m1, sc);
+  SEL_CHECK(cudaGetLastError());
+  auto* recs = static_cast<uint8_t*>(S.get(19, size_t(m1) * lay.record_bytes));
+  if (materialize(S, st, mat, sc, m1, recs) != 0)
+    throw cuda_error("internal error: a rebuilt record's objective differs from the engine's");
+
+  // 5. random mode: repeats, then the cap
+  const uint32_t* fin_order = nullptr;
+  uint32_t m2 = m1;
+  if (dedup) {
+    auto* hash = static_cast<unsigned long long*>(S.get(10, size_t(m1) * 8));
+    auto* hs = key;   // the unsorted keys are no longer needed
+    auto* q = pos;    // nor the unsorted positions
+    auto* seq = static_cast<uint32_t*>(S.get(12, size_t(m1) * 4));
+    k_hash<<<blocks(m1, 256), 256, 0, st>>>(recs, lay, m1, hash, seq);
+    SEL_CHECK(cudaGetLastError());
+    sort_pairs(S, st, hash, hs, seq, q, m1, 64);
+    // records are in key_s order (no cap was applied before rebuilding): record p has key key_s[p]
+    k_mark_repeats<<<blocks(m1, 256), 256, 0, st>>>(recs, lay, key_s, hs, q, m1, id_bits, flag);
+    SEL_CHECK(cudaGetLastError());
+    k_iota<<<blocks(m1, 256), 256, 0, st>>>(m1, seq);
+    SEL_CHECK(cudaGetLastError());
+    auto* kp = static_cast<uint32_t*>(S.get(15, size_t(m1) * 4));
+    m2 = select_flagged(S, st, seq, flag, kp, m1);
+    fin_order = kp;
+    if (max_per_objective >= 0 && m2 > 0) {
+      auto* fin = static_cast<uint32_t*>(S.get(14, size_t(m2) * 4));
+      m2 = cap_levels(S, st, kp, key_s, m2, id_bits, nl, max_per_objective, fin);
+      fin_order = fin;
+    }
   }
   if (m2 == 0) return true;
 
-  // 5. dense output arrays
+  // 6. dense output arrays
   OutLayout o{};
   uint32_t sp_total = 0, sro_total = 0;
   for (uint32_t p = 0; p < lay.n_parts; ++p) {
@@ -383,13 +427,13 @@ bool select_on_device(SelectScratch& S, cudaStream_t st, const RecordLayout& lay
   const size_t b_obj = size_t(m2) * lay.tsz, b_sub = size_t(m2) * lay.n_parts * lay.tsz,
                b_sp = size_t(m2) * sp_total, b_sro = size_t(m2) * sro_total, b_id = size_t(m2) * 8;
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-  auto* base = static_cast<uint8_t*>(S.get(15, al(b_obj) + al(b_sub) + al(b_sp) + al(b_sro) + al(b_id)));
+  auto* base = static_cast<uint8_t*>(S.get(3, al(b_obj) + al(b_sub) + al(b_sp) + al(b_sro) + al(b_id)));
   o.objective = base;
   o.sub_objective = o.objective + al(b_obj);
   o.species = o.sub_objective + al(b_sub);
   o.sro = o.species + al(b_sp);
   o.id = reinterpret_cast<unsigned long long*>(o.sro + al(b_sro));
-  k_gather<<<blocks(uint64_t(m2) * 32, 256), 256, 0, st>>>(d_records, lay, sel, pos_s, order, m2, o);
+  k_gather<<<blocks(uint64_t(m2) * 32, 256), 256, 0, st>>>(recs, lay, fin_order, m2, o);
   SEL_CHECK(cudaGetLastError());
   out.count = m2;
   out.objective.resize(b_obj);

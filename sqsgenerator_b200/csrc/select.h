@@ -68,8 +68,9 @@ struct SelectedSet {
 
 // Grow-only device scratch for select_on_device, bound to the stream it was last used on.
 struct SelectScratch {
-  void* buf[16] = {};
-  size_t size[16] = {};
+  static constexpr int kSlots = 20;
+  void* buf[kSlots] = {};
+  size_t size[kSlots] = {};
   cudaStream_t stream = nullptr;
   uint8_t* bounce[2] = {};        // pinned host buffers for large device-to-host copies
   cudaEvent_t bounce_done[2] = {};
@@ -79,13 +80,25 @@ struct SelectScratch {
   void release();
 };
 
-// Selects the records whose objective equals one of `levels` (the keep+1 smallest distinct
-// objectives, exact) from n device-resident records. Random runs (dedup) keep, among equal species,
-// the record with the smallest id. Returns false without doing anything when the ids do not leave
-// room for the level index in a 64-bit sort key (id_limit >= 2^58); the caller then selects on
-// the host.
-bool select_on_device(SelectScratch& scratch, cudaStream_t stream, const RecordLayout& layout,
-                      const uint8_t* d_records, uint64_t n, const std::vector<double>& levels, bool dedup,
-                      int64_t max_per_objective, uint64_t id_limit, SelectedSet& out);
+// Rebuilds full records of selected candidates on the device (sqsg_materialize) for one job.
+struct Materializer {
+  JobDesc job;        // the job's descriptor with device pointers (uploaded by materialize)
+  size_t smem = 0;    // dynamic shared memory of the launch (the job's general layout)
+};
+
+// Launches sqsg_materialize for m candidates (device array, in selection order) into m full records
+// at d_out, on `stream`; returns the number of objective mismatches (0 unless the engine is wrong),
+// after waiting for the stream. Scratch slots 16 and 17 of S hold the descriptor and the counter.
+uint64_t materialize(SelectScratch& S, cudaStream_t stream, const Materializer& mat, const Cand* d_cands, uint32_t m,
+                     uint8_t* d_out);
+
+// Selects, from n device-resident candidates, those whose objective equals one of `levels` (the
+// keep+1 smallest distinct objectives, exact), orders them by (objective, id), rebuilds their full
+// records, and (random runs, dedup) keeps among equal species the record with the smallest id, then at
+// most max_per_objective+1 per objective. Returns false without doing anything when the ids do not
+// leave room for the level index in a 64-bit sort key; the caller then selects on the host.
+bool select_on_device(SelectScratch& scratch, cudaStream_t stream, const RecordLayout& layout, const Cand* d_cands,
+                      uint64_t n, const std::vector<double>& levels, bool dedup, int64_t max_per_objective,
+                      uint64_t id_limit, const Materializer& mat, SelectedSet& out);
 
 }  // namespace sqsg

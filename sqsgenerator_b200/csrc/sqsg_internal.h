@@ -13,6 +13,19 @@ namespace sqsg {
 
 void set_error(const std::string& msg);
 
+// Process-wide options (sqsg_set_option / sqsg_get_option).
+enum Option : int {
+  kOptForceGeneral = 0,     // 1: every job takes the general pair-stream path
+  kOptStageWaitNs = 1,      // bound of the device's staging wait in nanoseconds
+  kOptDebugSkipStaging = 2, // debug: issue no staging copy, so that the bounded wait runs out
+  kOptCount
+};
+long long option(Option o);
+
+// Raises the dynamic shared-memory attribute of `kernel` on the current device to at least `bytes`
+// (per device, never lowered, one mutex for every entry point). Returns the CUDA status as int.
+int raise_dynamic_smem(const void* kernel, size_t bytes);
+
 // An error raised by the CUDA runtime or a device-side status word.
 struct cuda_error : std::runtime_error {
   using std::runtime_error::runtime_error;

@@ -120,10 +120,11 @@ def run_levels(run):
     """(values, counts, checksums) of a native run handle."""
     from sqsgenerator_b200 import _native as N
 
-    n = C.c_uint32(64)
-    v = np.zeros(64, np.float64)
-    cnt = np.zeros(64, np.uint64)
-    cs = np.zeros(64, np.uint64)
+    cap = 1100  # keep <= 1023: up to 1024 levels
+    n = C.c_uint32(cap)
+    v = np.zeros(cap, np.float64)
+    cnt = np.zeros(cap, np.uint64)
+    cs = np.zeros(cap, np.uint64)
     N.check(N.lib().sqsg_run_levels(run, C.byref(n), N.ptr(v), N.ptr(cnt), N.ptr(cs)))
     return [(float(v[i]), int(cnt[i]), int(cs[i])) for i in range(n.value)]
 

@@ -74,7 +74,8 @@ def parse_structure_kats(src: str) -> dict:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="root of a dgehringer/sqsgenerator 0.5.6 checkout (its tests/ folder is read)")
     args = ap.parse_args()
     ref = args.reference
     with open(os.path.join(ref, "tests/test_permutation.cpp")) as f:

@@ -225,7 +225,7 @@ def _oracle_core(d, res, keep):
 
 
 @pytest.mark.parametrize("prec", ["double", "single"])
-@pytest.mark.parametrize("keep", [1, 3, 10])
+@pytest.mark.parametrize("keep", [1, 3, 10, 64, 100])
 def test_systematic_result_set_equals_oracle(prec, keep):
     """fcc 2x2x2 A4B28 (35,960 permutations) with default pair weights: the device result set equals
     the restated reference collection's deterministic core, bit for bit (species, objective, sro)."""
@@ -259,16 +259,25 @@ def test_random_records_bit_exact_and_deduplicated():
     assert len(distinct) == 11
 
 
-@pytest.mark.parametrize("prec,keep,cap", [("double", 3, None), ("double", 10, 7), ("single", 5, 2)])
-def test_random_result_set_from_full_trace(prec, keep, cap):
-    """Every evaluation of a degenerate random run is traced; the result set must equal the rule
-    restated here on the trace: the keep+1 smallest distinct objectives, one record per distinct
-    configuration (the smallest id), ordered by objective then id, at most cap+1 per objective."""
-    cfg = cases.fcc32(prec, iterations=120000, seed=11, keep=keep)
+@pytest.mark.parametrize("cell,prec,keep,cap", [("fcc32", "double", 3, None), ("fcc32", "double", 10, 7),
+                                                ("fcc32", "single", 5, 2), ("fcc32", "double", 64, None),
+                                                ("fcc32", "single", 100, 3), ("quinary", "double", 100, None),
+                                                ("quinary", "single", 64, 1)])
+def test_random_result_set_from_full_trace(cell, prec, keep, cap):
+    """Every evaluation of a random run is traced; the result set must equal the rule restated here on
+    the trace: the keep+1 smallest distinct objectives, one record per distinct configuration (the
+    smallest id), ordered by objective then id, at most cap+1 per objective. keep >= 32 exercises the
+    warps' best lists in shared memory (the reference accepts any keep, io/config/combined.h:164-174)."""
+    if cell == "fcc32":
+        n = 120000
+        cfg = cases.fcc32(prec, iterations=n, seed=11, keep=keep)
+    else:
+        n = 30000
+        cfg = cases.quinary(prec, iterations=n, seed=12, keep=keep)
     if cap is not None:
         cfg["max_results_per_objective"] = cap
-    _, d, _, sp, _, ob, ids = cases.trace(cfg, 120000)
-    assert len(ob) == 120000
+    _, d, _, sp, _, ob, ids = cases.trace(cfg, n)
+    assert len(ob) == n
     levels = sorted(set(ob.tolist()))[: keep + 1]
     lset = set(levels)
     order = sorted((float(ob[k]), int(ids[k]), k) for k in range(len(ob)) if float(ob[k]) in lset)
@@ -307,11 +316,15 @@ def test_split_records_bit_exact():
 
 
 def test_max_results_per_objective():
+    """All 12,870 configurations of the 16-site cell have objective 0: with a cap of 5 the result set
+    is the 6 configurations of smallest rank (the reference's `>` test admits cap + 1)."""
     cfg = cases.settings_16("double")
     cfg["max_results_per_objective"] = 5
     c, d, recs, levels, info = native_run(cfg)
-    cnt = collections.Counter(recs["objective"].tolist())
-    assert max(cnt.values()) <= 6
+    assert recs["objective"].tolist() == [0.0] * 6
+    assert recs["id"].tolist() == [1, 2, 3, 4, 5, 6]
+    for k in range(6):
+        assert np.array_equal(recs["species"][k], oracle.unrank_permutation(d[0].species_packed, k + 1))
 
 
 def test_cancel_via_callback():
@@ -328,7 +341,7 @@ def test_cancel_via_callback():
 
 
 def test_unsupported_sizes_are_errors():
-    cfg = cases.fcc32("double", iterations=1000, keep=40)
+    cfg = cases.fcc32("double", iterations=1000, keep=2000)
     with pytest.raises(N.NativeError) as e:
         S.optimize(cfg)
     assert e.value.status_name == "SQSG_ERR_UNSUPPORTED"

@@ -158,3 +158,24 @@ def test_served_mixed_stream_equals_plain():
             assert records(run, c, d) == ref[k], k
             N.lib().sqsg_run_free(run)
         assert srv.stats()["launches"] >= 1
+
+
+def test_server_kernels_leave_when_idle():
+    """The ring's CTAs give up after a bounded number of empty polls (claim_live's idle limit): once
+    the last job is done, no persistent launch of the server stays on the GPU."""
+    import time as _time
+
+    with S.Server(0) as srv:
+        pack = srv.result(srv.submit(cases.fcc32("double", iterations=300000, seed=5)), timeout=120)
+        assert pack.num_results() > 0
+        running = C.c_uint32(1)
+        deadline = _time.monotonic() + 5.0
+        while _time.monotonic() < deadline:
+            N.check(N.lib().sqsg_server_running(srv._h, C.byref(running)))
+            if running.value == 0:
+                break
+            _time.sleep(0.005)
+        assert running.value == 0
+        # a job submitted after the kernels left starts a new launch and completes
+        pack = srv.result(srv.submit(cases.settings_16("double")), timeout=120)
+        assert pack.num_results() == 12870

@@ -1,0 +1,94 @@
+"""Host-side logic of the native library without a GPU: launch plans (which evaluation path a job
+takes), process-wide options, and the per-device bookkeeping of the dynamic shared-memory attribute."""
+import os
+import subprocess
+
+import pytest
+
+import cases
+import sqsgenerator_b200 as S
+from sqsgenerator_b200 import _native as N
+from sqsgenerator_b200.optimize import build_job
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def plan_of(cfg):
+    c = S.parse_config(cfg)
+    d = S.prepare(c)
+    job, bufs = build_job(c, d)
+    return N.plan(job)
+
+
+def test_plan_paths_without_a_device():
+    p = plan_of(cases.fcc32("double"))
+    assert p["kernel"] == "sqsg_engine_mask" and p["parts"][0]["path"] == "bitmask"
+    p = plan_of(cases.quinary("double", cells=(4, 4, 4)))
+    assert p["kernel"] == "sqsg_engine_wide" and p["parts"][0]["path"] == "general"
+    assert p["parts"][0]["stream_narrow"]
+    p = plan_of(cases.rocksalt_split("double", cells=(3, 3, 3)))
+    assert [x["path"] for x in p["parts"]] == ["general", "general"]
+    assert not any(x["stream_staged"] for x in p["parts"])  # split jobs read the stream through L1
+
+
+def test_force_general_option():
+    with N.options(force_general=1):
+        assert N.get_option("force_general") == 1
+        assert plan_of(cases.fcc32("double"))["parts"][0]["path"] == "general"
+    assert N.get_option("force_general") == 0
+    assert plan_of(cases.fcc32("double"))["parts"][0]["path"] == "bitmask"
+
+
+def test_option_errors():
+    with pytest.raises(N.NativeError) as e:
+        N.set_option("no_such_option", 1)
+    assert e.value.status_name == "SQSG_ERR_INVALID_ARGUMENT"
+    with pytest.raises(N.NativeError) as e:
+        N.set_option("stage_wait_ns", 0)
+    assert e.value.status_name == "SQSG_ERR_OUT_OF_RANGE"
+    assert N.get_option("stage_wait_ns") == 2_000_000_000
+
+
+def test_plan_validates_like_optimize():
+    with pytest.raises(N.NativeError) as e:
+        plan_of(cases.fcc32("double", keep=4000))
+    assert e.value.status_name == "SQSG_ERR_UNSUPPORTED"
+
+
+TRACKER_TEST = r"""
+#include <cstdio>
+#include <vector>
+#include "attr_tracker.h"
+int main() {
+  sqsg::DynamicSmemTracker t;
+  std::vector<std::pair<int, size_t>> calls;  // (device, bytes) of every attribute write
+  int dev = 0;
+  auto set = [&](size_t b) { calls.push_back({dev, b}); return 0; };
+  static int k1, k2;
+  dev = 0; if (t.raise(0, &k1, 100000, set)) return 1;
+  dev = 1; if (t.raise(1, &k1, 50000, set)) return 2;   // another device: must be set there too
+  dev = 0; if (t.raise(0, &k1, 80000, set)) return 3;   // below what device 0 has: no write
+  dev = 0; if (t.raise(0, &k2, 80000, set)) return 4;   // another kernel: its own record
+  dev = 1; if (t.raise(1, &k1, 120000, set)) return 5;  // raised on device 1 only
+  int fail_dev = 0;
+  auto failing = [&](size_t) { fail_dev = 1; return 7; };
+  if (t.raise(0, &k1, 200000, failing) != 7) return 6;  // a failed write leaves the record alone
+  if (t.current(0, &k1) != 100000 || t.current(1, &k1) != 120000 || t.current(0, &k2) != 80000) return 8;
+  const std::vector<std::pair<int, size_t>> want = {{0, 100000}, {1, 50000}, {0, 80000}, {1, 120000}};
+  if (calls != want) return 9;
+  std::printf("ok\n");
+  return 0;
+}
+"""
+
+
+def test_dynamic_smem_tracker_is_per_device(tmp_path):
+    """A process that launches on two devices must raise the attribute on each: the bookkeeping keeps
+    one record per (device, kernel) and only raises it (compiled here with g++ and a fake setter)."""
+    src = tmp_path / "tracker_test.cpp"
+    src.write_text(TRACKER_TEST)
+    exe = tmp_path / "tracker_test"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "sqsgenerator_b200", "csrc"), str(src),
+                    "-o", str(exe), "-pthread"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", (out.returncode, out.stdout, out.stderr)

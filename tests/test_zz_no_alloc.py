@@ -33,10 +33,11 @@ def regular(job):
 
 
 def noalloc(job):
-    n = C.c_uint32(32)
-    v = np.zeros(32, np.float64)
-    cnt = np.zeros(32, np.uint64)
-    cs = np.zeros(32, np.uint64)
+    cap = 1100
+    n = C.c_uint32(cap)
+    v = np.zeros(cap, np.float64)
+    cnt = np.zeros(cap, np.uint64)
+    cs = np.zeros(cap, np.uint64)
     st = N.SqsgStatistics()
     err = C.create_string_buffer(256)
     status = N.lib().sqsg_optimize_levels_noalloc(C.byref(job), None, C.byref(n), N.ptr(v), N.ptr(cnt), N.ptr(cs),
@@ -51,6 +52,7 @@ CASES = {
                                                          keep=5),
     "random_fcc32_double": lambda: cases.fcc32("double", iterations=300000, seed=17),
     "random_split_double": lambda: cases.rocksalt_split("double", iterations=50000, seed=5),
+    "random_quinary_keep100_double": lambda: cases.quinary("double", iterations=40000, seed=8, keep=100),
 }
 
 
