@@ -223,6 +223,8 @@ class OptimizationData:
     shell_radii: np.ndarray
     shell_weights: dict
     sublattices: list
+    lattice: np.ndarray | None = None  # (N, 4) per sorted site: unit-cell site, cell indices a, b, c
+    cells: tuple = (0, 0, 0)            # supercell repetitions along the three lattice vectors
 
 
 class SqsResult:

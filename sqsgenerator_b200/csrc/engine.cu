@@ -171,12 +171,21 @@ using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, 
 
 // The general path runs in sqsg_engine_wide (128 registers); a launch whose jobs all take the binary
 // bit-mask path runs in sqsg_engine_mask (96 registers, 5 CTAs per SM).
-static EngineKernel engine_for(bool all_bitmask) { return all_bitmask ? sqsg_engine_mask : sqsg_engine_wide; }
+// Kernel kinds: each job runs in the kernel that holds its path.
+enum KernelKind : int { kKindMask = 0, kKindWide = 1, kKindLat = 2 };
+static int kind_of(const JobDesc& d) { return d.k2 ? kKindMask : (d.lat ? kKindLat : kKindWide); }
+static EngineKernel kernel_of(int kind) {
+  return kind == kKindMask ? sqsg_engine_mask : (kind == kKindLat ? sqsg_engine_lat : sqsg_engine_wide);
+}
+static const char* kernel_name(int kind) {
+  return kind == kKindMask ? "sqsg_engine_mask" : (kind == kKindLat ? "sqsg_engine_lat" : "sqsg_engine_wide");
+}
 
 // The dynamic shared-memory attribute is per device: it is raised on the current device (every
 // caller has made the job's device current).
 static void configure_kernel(size_t smem) {
-  for (const void* k : {reinterpret_cast<const void*>(sqsg_engine_wide), reinterpret_cast<const void*>(sqsg_engine_mask)}) {
+  for (const void* k : {reinterpret_cast<const void*>(sqsg_engine_wide), reinterpret_cast<const void*>(sqsg_engine_mask),
+                        reinterpret_cast<const void*>(sqsg_engine_lat)}) {
     const int err = raise_dynamic_smem(k, smem);
     if (err != 0)
       throw cuda_error(std::string("cudaFuncSetAttribute(MaxDynamicSharedMemorySize): ") +
@@ -196,10 +205,11 @@ static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel k
 static size_t max_dynamic_smem(int dev) {
   int v = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes b{}, c{};
+  cudaFuncAttributes b{}, c{}, l{};
   CUDA_CHECK(cudaFuncGetAttributes(&b, sqsg_engine_wide));
   CUDA_CHECK(cudaFuncGetAttributes(&c, sqsg_engine_mask));
-  return static_cast<size_t>(v) - std::max(b.sharedSizeBytes, c.sharedSizeBytes);
+  CUDA_CHECK(cudaFuncGetAttributes(&l, sqsg_engine_lat));
+  return static_cast<size_t>(v) - std::max({b.sharedSizeBytes, c.sharedSizeBytes, l.sharedSizeBytes});
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -641,9 +651,16 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     CUDA_CHECK(cudaMemsetAsync(ws->cancel_dev, 0, sizeof(int32_t), ws->stream));
     bool cancel_sent = false;
 
-    bool all_bitmask = true;
-    for (size_t j = 0; j < nj; ++j) all_bitmask = all_bitmask && pjs[j].desc.k2 != 0;
-    const EngineKernel kernel = engine_for(all_bitmask);
+    // one kernel per launch: the jobs of a launch are of one kind, except that bit-mask jobs may share a
+    // launch of the general path (their columns and stream exist too); lattice jobs never mix
+    int kind = kind_of(pjs[0].desc);
+    for (size_t j = 1; j < nj; ++j) {
+      const int kj = kind_of(pjs[j].desc);
+      if (kj == kind) continue;
+      if (kj == kKindLat || kind == kKindLat) throw std::logic_error("lattice jobs mixed with others in one launch");
+      kind = kKindWide;
+    }
+    const EngineKernel kernel = kernel_of(kind);
     const uint32_t grid = launch_grid(device, smem, tiles.size(), kernel);
     CUDA_CHECK(cudaEventRecord(ws->ev_start, ws->stream));
     if (!tiles.empty()) {
@@ -713,6 +730,10 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     CUDA_CHECK(cudaMemcpy(&status, ws->status.p, sizeof(status), cudaMemcpyDeviceToHost));
     if (status == kErrStageTimeout) throw timeout_error("shared-memory staging wait timed out on the device");
     if (status != 0) throw cuda_error("device error code " + std::to_string(status));
+    for (size_t j = 0; j < nj; ++j)
+      if (cnt[j * kNumCounters + kMismatch])
+        throw cuda_error("internal error: " + std::to_string(cnt[j * kNumCounters + kMismatch]) +
+                         " lattice-path objectives differ from the pair-stream path's");
     // Every job's counters and level table come back; a job whose record buffer overflowed is re-run
     // (see assess) when the caller left the capacity to the library. Records come back only when
     // the level table overflowed (the levels are then rebuilt from them on the host) or the set is
@@ -842,10 +863,17 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
 // that finishes a job's last tile marks the job's slot done in host-mapped memory; the worker then
 // downloads its records and levels, selects the result set and wakes the waiting caller. A job's
 // result does not depend on what else runs: its tiles and Philox counters depend only on the job.
-// One ring per occupancy level: ring 0 runs sqsg_engine_mask at 5 CTAs per SM and takes binary bit-mask
-// jobs; rings 1-4 run sqsg_engine_wide at 4, 3, 2, 1 CTAs per SM. A job goes to the ring with the
-// largest shared-memory size it fits, i.e. the highest occupancy its data allow.
-constexpr int kBuckets = 5;
+// One ring per (kernel, occupancy level): ring 0 runs sqsg_engine_mask at 5 CTAs per SM and takes
+// binary bit-mask jobs; rings 1-4 run sqsg_engine_wide at 4, 3, 2, 1 CTAs per SM; rings 5-6 run
+// sqsg_engine_lat at 2 and 1 CTAs per SM. A job goes to the ring of its kernel with the largest
+// shared-memory size it fits, i.e. the highest occupancy its data allow.
+constexpr int kBuckets = 7;
+struct RingSpec {
+  int kind;  // KernelKind
+  int want;  // CTAs per SM
+};
+constexpr RingSpec kRingSpec[kBuckets] = {{kKindMask, 5}, {kKindWide, 4}, {kKindWide, 3}, {kKindWide, 2},
+                                          {kKindWide, 1}, {kKindLat, 2},  {kKindLat, 1}};
 constexpr int kMaxSm = 256;
 constexpr uint64_t kRingCap = 1u << 20;
 constexpr uint32_t kIdlePolls = 250;          // ~0.5 ms of empty polls before a CTA leaves its ring
@@ -1454,11 +1482,11 @@ static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, co
     configure_kernel(max_dynamic_smem(device));
     std::map<std::pair<int, int>, std::vector<uint32_t>> classes;
     for (uint32_t j = 0; j < n; ++j) {
-      const bool bitmask = pjs[j].desc.k2 != 0;
+      const int kind = kind_of(pjs[j].desc);
       int per_sm = 0;
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_for(bitmask), kBlock,
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_of(kind), kBlock,
                                                                pjs[j].desc.smem_bytes));
-      classes[{bitmask ? 0 : 1, -per_sm}].push_back(j);
+      classes[{kind, -per_sm}].push_back(j);
     }
     std::vector<std::unique_ptr<sqsg_run>> done(n);
     for (auto& [key, idx] : classes) {
@@ -1504,10 +1532,11 @@ sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
     plan->smem_bytes = d.smem_bytes;
     plan->record_bytes = d.record_bytes;
     const bool bitmask = d.k2 != 0;
-    std::snprintf(plan->kernel, sizeof(plan->kernel), "%s", bitmask ? "sqsg_engine_mask" : "sqsg_engine_wide");
+    const int kind = kind_of(d);
+    std::snprintf(plan->kernel, sizeof(plan->kernel), "%s", kernel_name(kind));
     for (uint32_t p = 0; p < d.n_parts; ++p) {
       const PartDesc& P = d.parts[p];
-      plan->parts[p].path = bitmask ? SQSG_PATH_BITMASK : SQSG_PATH_GENERAL;
+      plan->parts[p].path = bitmask ? SQSG_PATH_BITMASK : (d.lat ? SQSG_PATH_LATTICE : SQSG_PATH_GENERAL);
       plan->parts[p].stream_narrow = static_cast<int32_t>(P.stream_narrow);
       plan->parts[p].stream_staged = P.stream_global ? 0 : 1;
     }
@@ -1517,7 +1546,7 @@ sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
       if (d.smem_bytes <= max_dynamic_smem(job->device)) {
         configure_kernel(d.smem_bytes);
         int per_sm = 0;
-        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_for(bitmask), kBlock, d.smem_bytes));
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_of(kind), kBlock, d.smem_bytes));
         plan->ctas_per_sm = static_cast<uint32_t>(per_sm);
       }
     } else {
@@ -1666,13 +1695,13 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     configure_kernel(optin);
     for (int b = 0; b < kBuckets; ++b) {
       Ring& R = S.rings[b];
-      R.kernel = b == 0 ? sqsg_engine_mask : sqsg_engine_wide;
+      R.kernel = kernel_of(kRingSpec[b].kind);
       auto fits = [&](size_t smem) {
         int nb = 0;
         CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, R.kernel, kBlock, smem));
         return nb;
       };
-      const int want = kBuckets - b;
+      const int want = kRingSpec[b].want;
       size_t lo = 0, hi = optin;  // largest smem in [0, optin] with fits(smem) >= want
       if (fits(hi) >= want) {
         lo = hi;
@@ -1728,14 +1757,20 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
     J->pj = prepare(*job, 0);
     J->t_submit = now_ns();
     const size_t need = J->pj.desc.smem_bytes;
-    if (need > S.rings[kBuckets - 1].smem)
-      throw unsupported_error("the job needs more shared memory per CTA than this device offers");
-    J->bucket = kBuckets - 1;
-    for (int b = J->pj.desc.k2 ? 0 : 1; b < kBuckets; ++b)  // general-path jobs use the wide kernel
-      if (need <= S.rings[b].smem) {
+    const int kind = kind_of(J->pj.desc);
+    J->bucket = -1;
+    for (int b = 0; b < kBuckets; ++b)  // rings of one kernel are ordered by falling occupancy
+      if (kRingSpec[b].kind == kind && need <= S.rings[b].smem) {
         J->bucket = b;
         break;
       }
+    if (J->bucket < 0 && kind == kKindMask)  // a bit-mask job may run the general path as well
+      for (int b = 0; b < kBuckets; ++b)
+        if (kRingSpec[b].kind == kKindWide && need <= S.rings[b].smem) {
+          J->bucket = b;
+          break;
+        }
+    if (J->bucket < 0) throw unsupported_error("the job needs more shared memory per CTA than this device offers");
     J->user_capacity = job->max_results != 0;
     J->capacity = job->max_results ? job->max_results : S.opt.default_max_results;
     for (uint32_t p = 0; p < job->n_sublattices; ++p) J->pairs += job->sublattices[p].n_pairs;

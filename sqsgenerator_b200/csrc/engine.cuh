@@ -51,6 +51,7 @@ constexpr int kBlock = 128;       // threads per CTA (each owns one configuratio
 constexpr int kMinBlocks = 5;     // sqsg_engine_mask: CTAs per SM the register budget must allow (<= 102 registers)
 constexpr int kK2MaxShells = 4;   // shells of the binary bit-mask path (per-shell counters in registers)
 constexpr int kMinBlocksWide = 4; // sqsg_engine_wide (general path): 128 registers, no spills in the pair loop
+constexpr int kMinBlocksLat = 2;  // sqsg_engine_lat (lattice path): up to 255 registers, no spills
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
 constexpr int kMaxSpecies = 8;    // K per part handled by the packed-row counter
@@ -71,6 +72,7 @@ enum Counter : int {
   kLevelOverflow = 6,  // the job's level table ran out of slots
   kRecordsFull = 7,    // set once the candidate buffer is full (appends stop)
   kTilesLeft = 8,      // live queue: tiles of the job not yet finished
+  kMismatch = 9,       // trace mode: lattice-path objectives that differ from the pair-stream path's
   kNumCounters = 16
 };
 
@@ -131,6 +133,25 @@ struct PartDesc {
   uint32_t k2_binom_off;  // blob offset (global, not staged) of C(m, j), m <= window, j <= ones
   uint32_t k2_nbp_off;    // neighbour masks by bit position: u32 [S][32] (N <= 32) or uint2 [S][64]
   uint32_t k2_zeros;      // 1: count over the zeros (species 0 is the minority), else over the ones
+  // lattice path (a supercell whose pairs form whole translation classes, see run_tile_lat)
+  uint32_t lat_km;        // 0: not on the lattice path; else 2, 4 or 8 >= K (unrolled species count)
+  uint32_t lat_basis;     // unit-cell sites m
+  uint32_t lat_cells;     // cells A*B*C (<= 64: one 64-bit plane per unit-cell site and species)
+  uint32_t lat_chunks;    // ceil(cells / 4)
+  uint32_t lat_site_off;  // staged: u32 column offsets by (unit-cell site, cell), m x 4*chunks
+  uint32_t lat_ent_off;   // staged: u32 classes  beta | beta2 << 4 | translation << 8, by shell
+  uint32_t lat_shell_off; // staged: uint4 per shell (first class, first self-reverse class, end, pairs)
+  uint32_t lat_tr_off;    // staged: LatTr per translation
+  uint32_t lat_deg_off;   // staged: u32 shell-s neighbours of each unit-cell site, S x m
+  uint32_t lat_planes_off;// shared-memory-only: per lane m x (K-1) one-hot planes (u64, interleaved by lane)
+  unsigned long long lat_full;  // the cells' bits
+};
+
+// A translation of the cell grid (bit c = x + A*(y + B*z)) by (dx, dy, dz), as rotations inside rows
+// of A bits, blocks of A*B bits and the whole grid; a zero shift skips its stage.
+struct LatTr {
+  uint32_t sx, sxr, sy, syr, sz, szr, pad0, pad1;
+  unsigned long long mxh, mxl, myh, myl;
 };
 
 struct JobDesc {
@@ -145,6 +166,8 @@ struct JobDesc {
   uint32_t smem_full;     // dynamic shared memory of the general layout (materialize, trace)
   uint32_t big_off;       // keep >= 32: per-warp best lists of big_len doubles at this offset
   uint32_t big_len;       // entries per warp list in shared memory (0: the list is one register per lane)
+  uint32_t lat;           // 1: every part takes the lattice path
+  uint32_t lat_pad;
   uint32_t trace;         // 1: write every evaluated configuration to the trace buffers
   uint32_t trace_species_stride, trace_bonds_stride;
   uint64_t seed;

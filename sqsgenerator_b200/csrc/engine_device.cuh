@@ -912,6 +912,258 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
   warp_acc_flush(ws, ctab, J);  // the CTA table is complete for this tile
 }
 
+// ------------------------------------------------------------------------------ lattice path
+// A supercell of A x B x C copies of a unit cell with m sites: site (beta, c) is unit-cell site beta
+// in cell c = x + A*(y + B*z). Translating every site by one cell vector maps the pair list onto
+// itself (distances and shells depend only on the difference vector), so the pairs of one shell fall
+// into classes {(beta, c), (beta2, c + d)} over all cells c. With X[beta][a] the 64-bit set of cells
+// whose site beta holds species a, the pairs of one class with species {a, b} number
+//   popc(X[beta][a] & Y[b]) + popc(X[beta][b] & Y[a]),  Y[b] = X[beta2][b] translated by -d,
+// (one popcount of the OR: the two sets are disjoint), and a class that is its own reverse
+// (beta == beta2, 2d = 0) counts each pair twice. Counting only the species a, b < K-1 and closing with
+// the degree identity sum_b (1 + [a == b]) U(a, b) = sum_{sites i of species a} deg_s(i) gives the
+// unordered counts U(a, b) = bonds(s,a,b) + bonds(s,b,a) (a != b) and U(a, a) = bonds(s,a,a) that
+// core/optimization.h:79-103 reads, exactly. A class costs one AND (+ OR) and one popcount per
+// species pair instead of one gather per pair of sites.
+
+__device__ __forceinline__ unsigned long long lat_translate(unsigned long long v, const LatTr* t,
+                                                            unsigned long long full) {
+  const uint32_t sx = t->sx, sy = t->sy, sz = t->sz;
+  if (sx) v = ((v << sx) & t->mxh) | ((v >> t->sxr) & t->mxl);
+  if (sy) v = ((v << sy) & t->myh) | ((v >> t->syr) & t->myl);
+  if (sz) v = ((v << sz) | (v >> t->szr)) & full;
+  return v;
+}
+
+// The lane's one-hot planes X[beta][a] (a < K-1) from its species column: four sites per step, bit k
+// of each site's species gathered into a nibble (binary planes), then one-hot by AND/NOT.
+template <int KM>
+__device__ __forceinline__ void lat_planes(uint8_t* smem, const PartDesc& P, int t) {
+  uint8_t* part = part_base(smem, P);
+  const uint8_t* col = part + P.col_off + 4 * t;
+  const uint4* so4 = reinterpret_cast<const uint4*>(part + P.lat_site_off);
+  unsigned long long* X = reinterpret_cast<unsigned long long*>(part + P.lat_planes_off) + t;
+  const uint32_t km1 = P.n_species - 1, chunks = P.lat_chunks;
+  const unsigned long long full = P.lat_full;
+  constexpr int NB = KM <= 2 ? 1 : (KM <= 4 ? 2 : 3);
+  for (uint32_t beta = 0; beta < P.lat_basis; ++beta) {
+    unsigned long long B[NB];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) B[k] = 0ull;
+    for (uint32_t q = 0; q < chunks; ++q) {
+      const uint4 o = so4[beta * chunks + q];
+      const uint32_t w = static_cast<uint32_t>(col[o.x]) | (static_cast<uint32_t>(col[o.y]) << 8) |
+                         (static_cast<uint32_t>(col[o.z]) << 16) | (static_cast<uint32_t>(col[o.w]) << 24);
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {  // species codes are 8 * species: bit k of the species is bit 3 + k
+        const uint32_t nib = ((((w >> (3 + k)) & 0x01010101u) * 0x00204081u) >> 21) & 0xfu;
+        B[k] |= static_cast<unsigned long long>(nib) << (4 * q);
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < KM - 1; ++a) {
+      if (a >= static_cast<int>(km1)) break;
+      unsigned long long x = full;
+#pragma unroll
+      for (int k = 0; k < NB; ++k) x &= ((a >> k) & 1) ? B[k] : ~B[k];
+      X[(beta * km1 + a) * kBlock] = x;
+    }
+  }
+}
+
+template <int NA> __host__ __device__ constexpr int lat_idx(int a, int b) { return a * NA - a * (a - 1) / 2 + (b - a); }
+
+// Objective of one part (core/optimization.h:79-103, terms in the reference's order) from the lane's
+// planes.
+template <int KM, class T>
+__device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int t) {
+  using F = FP<T>;
+  constexpr int NA = KM - 1;  // species with planes, at most
+  constexpr int NT = NA * (NA + 1) / 2;
+  const uint8_t* part = part_base(smem, P);
+  const unsigned long long* X = reinterpret_cast<const unsigned long long*>(part + P.lat_planes_off) + t;
+  const uint32_t* ent = reinterpret_cast<const uint32_t*>(part + P.lat_ent_off);
+  const uint4* shl = reinterpret_cast<const uint4*>(part + P.lat_shell_off);
+  const LatTr* trs = reinterpret_cast<const LatTr*>(part + P.lat_tr_off);
+  const uint32_t* deg = reinterpret_cast<const uint32_t*>(part + P.lat_deg_off);
+  const uint32_t K = P.n_species, km1 = K - 1, S = P.n_shells, m = P.lat_basis;
+  const unsigned long long full = P.lat_full;
+  const uint32_t skk = S * K * K;
+  const T* f = reinterpret_cast<const T*>(part + P.cube_off);
+  const T* w = f + skk;
+  const T* tg = w + skk;
+  T obj = T(0);
+  for (uint32_t s = 0; s < S; ++s) {
+    uint32_t acc[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) acc[k] = 0u;
+    const uint4 sh = shl[s];
+    uint32_t key = ~0u, cur = ~0u;
+    unsigned long long Y[NA], Xa[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) Y[a] = Xa[a] = 0ull;
+    for (uint32_t e = sh.x; e < sh.z; ++e) {
+      if (e == sh.y) {  // self-reverse classes count every pair twice: double what came before
+#pragma unroll
+        for (int k = 0; k < NT; ++k) acc[k] <<= 1;
+      }
+      const uint32_t en = ent[e];
+      if ((en >> 4) != key) {  // (beta2, translation) changed: translate beta2's planes
+        key = en >> 4;
+        const uint32_t b2 = key & 0xfu;
+        const LatTr* tr = trs + (key >> 4);
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          if (a >= static_cast<int>(km1)) break;
+          Y[a] = lat_translate(X[(b2 * km1 + a) * kBlock], tr, full);
+        }
+      }
+      if ((en & 0xfu) != cur) {
+        cur = en & 0xfu;
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          if (a >= static_cast<int>(km1)) break;
+          Xa[a] = X[(cur * km1 + a) * kBlock];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+#pragma unroll
+        for (int b = a; b < NA; ++b) {
+          if (b >= static_cast<int>(km1)) break;
+          acc[lat_idx<NA>(a, b)] +=
+              a == b ? __popcll(Xa[a] & Y[a]) : __popcll((Xa[a] & Y[b]) | (Xa[b] & Y[a]));
+        }
+      }
+    }
+    if (sh.y < sh.z) {
+#pragma unroll
+      for (int k = 0; k < NT; ++k) acc[k] >>= 1;
+    }
+    // pairs with the last species: H_a - 2 U(a, a) - sum_{b != a} U(a, b), H_a the shell-s degree sum
+    // of the sites of species a; U(K-1, K-1) from the shell's pair count
+    uint32_t ue[NA];
+    uint32_t rest = sh.w;
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      ue[a] = 0u;
+      if (a >= static_cast<int>(km1)) break;
+      uint32_t h = 0u;
+      for (uint32_t beta = 0; beta < m; ++beta) h += deg[s * m + beta] * __popcll(X[(beta * km1 + a) * kBlock]);
+      uint32_t u = h - 2u * acc[lat_idx<NA>(a, a)];
+#pragma unroll
+      for (int b = 0; b < NA; ++b) {
+        if (b >= static_cast<int>(km1)) break;
+        if (b != a) u -= acc[b < a ? lat_idx<NA>(b, a) : lat_idx<NA>(a, b)];
+      }
+      ue[a] = u;
+      rest -= u;
+#pragma unroll
+      for (int b = a; b < NA; ++b) {
+        if (b >= static_cast<int>(km1)) break;
+        rest -= acc[lat_idx<NA>(a, b)];
+      }
+    }
+    const uint32_t uee = rest;
+#pragma unroll
+    for (int xi = 0; xi < KM; ++xi) {
+      if (xi >= static_cast<int>(K)) break;
+      const int xc = xi < NA ? xi : 0;
+      const uint32_t d = (s * K + xi) * K + xi;
+      const uint32_t nd = static_cast<uint32_t>(xi) == km1 ? uee : (xi < NA ? acc[lat_idx<NA>(xc, xc)] : 0u);
+      const T sig = F::sub(T(1), F::mul(F::cvt(nd), f[d]));
+      T diff = F::sub(sig, tg[d]);
+      diff = diff > T(0) ? diff : -diff;
+      obj = F::add(obj, F::mul(w[d], diff));
+#pragma unroll
+      for (int eta = xi + 1; eta < KM; ++eta) {
+        if (eta >= static_cast<int>(K)) break;
+        const int ec = eta < NA ? eta : 0;
+        const uint32_t u = (s * K + xi) * K + eta;
+        const uint32_t nb = static_cast<uint32_t>(eta) == km1 ? (xi < NA ? ue[xc] : 0u)
+                                                              : (eta < NA ? acc[lat_idx<NA>(xc, ec)] : 0u);
+        const T sg = F::sub(T(1), F::mul(F::cvt(nb), f[u]));
+        T df = F::sub(sg, tg[u]);
+        df = df > T(0) ? df : -df;
+        obj = F::add(obj, F::mul(w[u], df));
+      }
+    }
+  }
+  return obj;
+}
+
+template <class T>
+__device__ __forceinline__ T lat_part(uint8_t* smem, const PartDesc& P, int t) {
+  switch (P.lat_km) {
+    case 2:
+      lat_planes<2>(smem, P, t);
+      return lat_objective<2, T>(smem, P, t);
+    case 4:
+      lat_planes<4>(smem, P, t);
+      return lat_objective<4, T>(smem, P, t);
+    default:
+      lat_planes<8>(smem, P, t);
+      return lat_objective<8, T>(smem, P, t);
+  }
+}
+
+// The general tile loop with lattice counting. In trace mode the pair-stream count runs as well: its
+// ordered bonds go to the trace, and an objective that differs from the lattice path's is counted in
+// counters[kMismatch] (the host reports it as an error).
+template <class T, bool SYS>
+__device__ __forceinline__ void run_tile_lat(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                             WarpState& ws) {
+  using F = FP<T>;
+  const int t = threadIdx.x;
+  const uint64_t base = tile.count / kBlock, rem = tile.count % kBlock;
+  const uint64_t my_count = base + (static_cast<uint64_t>(t) < rem ? 1 : 0);
+  const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
+  const uint64_t max_count = base + (rem ? 1 : 0);
+  const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
+  for (uint32_t p = 0; p < J.n_parts; ++p) init_column(smem, J.parts[p], t);
+  uint32_t wlo = 0, wn = 0;
+  if (SYS) {
+    const PartDesc& P = J.parts[0];
+    const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
+    wlo = win[0];
+    wn = win[1] - win[0];
+    if (my_count > 0)
+      unrank_window(part_base(smem, P) + P.col_off + 4 * t, P, wlo, wn, tile.start + my_off, J.total);
+  }
+  T thr_g = load_threshold<T>(J);
+  for (uint64_t it = 0; it < max_count; ++it) {
+    const bool active = it < my_count;
+    T total = T(0);
+    if (active) {
+      for (uint32_t p = 0; p < J.n_parts; ++p) {
+        const PartDesc& P = J.parts[p];
+        if (!SYS) {
+          if (it > 0) init_column(smem, P, t);
+          shuffle_part(smem, P, t, 0u, tile.start + my_off + it, p, k0, k1);
+        }
+        const T o = lat_part<T>(smem, P, t);
+        if (J.trace) {
+          if (J.kw == 1)
+            count_part<1>(smem, J.blob, P, t);
+          else
+            count_part<2>(smem, J.blob, P, t);
+          const T g = objective_part<T>(smem, P, t);
+          if (!(g == o)) atomicAdd(&J.counters[kMismatch], 1ull);
+        }
+        total = p == 0 ? o : F::add(total, o);
+      }
+    }
+    thr_g = load_threshold<T>(J);
+    const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
+    const bool pass = active && static_cast<double>(total) <= bound;
+    const uint64_t id = tile.start + my_off + it;
+    handle_candidates<T>(J, ctab, ws, pass, total, thr_g, id, t);
+    if (J.trace && active) write_trace<T>(J, smem, id - J.trace_base, total, id, t);
+    if (SYS && active && it + 1 < my_count)
+      next_permutation(part_base(smem, J.parts[0]) + J.parts[0].col_off + 4 * t, wlo, wn);
+  }
+}
+
 // ------------------------------------------------------------------------------ persistent kernel
 constexpr unsigned long long kNoTile = ~0ull;
 
@@ -972,6 +1224,15 @@ __device__ __forceinline__ void dispatch_mask(const JobDesc& sj, uint8_t* smem, 
 }
 
 template <bool SYS>
+__device__ __forceinline__ void dispatch_lattice(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                                 WarpState& ws) {
+  if (sj.prec == 1)
+    run_tile_lat<double, SYS>(sj, smem, ctab, tile, ws);
+  else
+    run_tile_lat<float, SYS>(sj, smem, ctab, tile, ws);
+}
+
+template <bool SYS>
 __device__ __forceinline__ void dispatch_general(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                                  WarpState& ws) {
   if (sj.prec == 1) {
@@ -987,7 +1248,9 @@ __device__ __forceinline__ void dispatch_general(const JobDesc& sj, uint8_t* sme
   }
 }
 
-template <bool SYS, bool GENERAL, bool MASK>
+// Each kernel holds some of the paths (see kernels.h); the host launches a job only in a kernel that
+// holds its path (a bit-mask job may also run the general path: its columns and stream exist too).
+template <bool SYS, bool GENERAL, bool MASK, bool LAT>
 __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                               WarpState& ws) {
   if constexpr (MASK) {
@@ -996,7 +1259,13 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
       return;
     }
   }
-  if constexpr (GENERAL) {  // also correct for bit-mask jobs: their columns and stream exist too
+  if constexpr (LAT) {
+    if (sj.lat) {
+      dispatch_lattice<SYS>(sj, smem, ctab, tile, ws);
+      return;
+    }
+  }
+  if constexpr (GENERAL) {
     dispatch_general<SYS>(sj, smem, ctab, tile, ws);
   }
 }
@@ -1006,7 +1275,7 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
 // whenever its next tile belongs to another job. In live mode every tile ends with a level flush and
 // a decrement of the job's tile count; the CTA that finishes a job's last tile publishes the job's
 // generation in done[slot] (host-mapped memory).
-template <bool GENERAL, bool MASK>
+template <bool GENERAL, bool MASK, bool LAT>
 __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
                                             uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
                                             unsigned long long* status, volatile uint32_t* done) {
@@ -1096,9 +1365,9 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
       ws.reset(sj, smem);
     }
     if (sj.mode == 1)
-      dispatch_tile<true, GENERAL, MASK>(sj, smem, ctab, tile, ws);
+      dispatch_tile<true, GENERAL, MASK, LAT>(sj, smem, ctab, tile, ws);
     else
-      dispatch_tile<false, GENERAL, MASK>(sj, smem, ctab, tile, ws);
+      dispatch_tile<false, GENERAL, MASK, LAT>(sj, smem, ctab, tile, ws);
     __syncthreads();  // every thread is done with this tile before s_tile changes
     if (live) {
       flush_levels(ctab, sj);

@@ -1,0 +1,16 @@
+// sqsg_engine_lat: the persistent engine holding the lattice path (bonds from translated bit planes of
+// a supercell, see run_tile_lat). Its per-lane state (species-pair counters, translated and current
+// planes for up to eight species) needs more than 128 registers, so the kernel allows 2 CTAs per SM
+// at up to 255 registers instead of spilling.
+#include "engine_device.cuh"
+#include "kernels.h"
+
+namespace sqsg {
+
+__global__ void __launch_bounds__(kBlock, kMinBlocksLat)
+    sqsg_engine_lat(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                    const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
+  engine_body<false, false, true>(jobs, tiles, n_tiles, q, cancel, status, done);
+}
+
+}  // namespace sqsg

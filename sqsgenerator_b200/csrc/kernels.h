@@ -20,6 +20,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksWide)
     sqsg_engine_wide(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                      const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
 
+// sqsg_engine_lat — the lattice path (supercells whose pairs are whole translation classes).
+__global__ void __launch_bounds__(kBlock, kMinBlocksLat)
+    sqsg_engine_lat(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                    const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
+
 // Rebuilds the full records (selection order) of n candidates of one job; counts objective mismatches.
 __global__ void __launch_bounds__(kBlock)
     sqsg_materialize(const JobDesc* __restrict__ job, const Cand* __restrict__ cands, uint32_t n,

@@ -128,6 +128,148 @@ static uint64_t window_permutations(const sqsg_sublattice& sl, PartDesc& pd) {
   return total;
 }
 
+// Lattice-path tables of one part, from its supercell hint (sqsg_sublattice::lattice): valid only
+// when the sites are a bijection onto (unit-cell site, cell) and every pair belongs to a translation
+// class {(beta, c), (beta2, c + d)} that the pair list holds completely — once per cell, or once per
+// pair of cells for a class that is its own reverse (beta == beta2, 2d = 0).
+struct LatticeTables {
+  uint32_t m = 0, A = 0, B = 0, C = 0, cells = 0, chunks = 0;
+  unsigned long long full = 0;
+  std::vector<uint32_t> site_off;  // m x 4*chunks column offsets (cells past the grid repeat cell 0)
+  std::vector<uint32_t> ent;       // beta | beta2 << 4 | translation << 8
+  std::vector<uint32_t> shell;     // per shell: first class, first self-reverse class, end, pairs
+  std::vector<LatTr> tr;
+  std::vector<uint32_t> deg;       // S x m
+};
+
+static bool lattice_tables(const sqsg_sublattice& sl, LatticeTables& L) {
+  if (!sl.lattice) return false;
+  const uint32_t N = sl.n_sites, S = sl.n_shells;
+  const uint32_t A = sl.cells[0], B = sl.cells[1], C = sl.cells[2], m = sl.n_basis;
+  if (A == 0 || B == 0 || C == 0 || m == 0 || m > 15) return false;
+  const uint64_t cells = static_cast<uint64_t>(A) * B * C;
+  if (cells > 64 || cells * m != N) return false;
+  std::vector<uint32_t> beta(N), cx(N), cy(N), cz(N), site_at(N, ~0u);
+  for (uint32_t x = 0; x < N; ++x) {
+    const uint32_t* h = sl.lattice + 4 * static_cast<size_t>(x);
+    if (h[0] >= m || h[1] >= A || h[2] >= B || h[3] >= C) return false;
+    beta[x] = h[0];
+    cx[x] = h[1];
+    cy[x] = h[2];
+    cz[x] = h[3];
+    const uint32_t q = h[0] * static_cast<uint32_t>(cells) + h[1] + A * (h[2] + B * h[3]);
+    if (site_at[q] != ~0u) return false;
+    site_at[q] = x;
+  }
+  // class key: shell, beta, beta2, displacement (dx + 64 * (dy + 64 * dz)) of the second site
+  auto key_of = [](uint32_t s, uint32_t b1, uint32_t b2, uint32_t dx, uint32_t dy, uint32_t dz) {
+    return (static_cast<unsigned long long>((s << 8) | (b1 << 4) | b2) << 18) | (dx + 64u * (dy + 64u * dz));
+  };
+  std::vector<std::pair<unsigned long long, uint32_t>> member(sl.n_pairs);  // (class key, cell id in class)
+  std::vector<uint8_t> self_rev(sl.n_pairs);
+  for (uint32_t e = 0; e < sl.n_pairs; ++e) {
+    const uint32_t i = sl.pairs[3 * e], j = sl.pairs[3 * e + 1], s = sl.pairs[3 * e + 2];
+    const uint32_t dx = (cx[j] + A - cx[i]) % A, dy = (cy[j] + B - cy[i]) % B, dz = (cz[j] + C - cz[i]) % C;
+    const unsigned long long k1 = key_of(s, beta[i], beta[j], dx, dy, dz);
+    const unsigned long long k2 = key_of(s, beta[j], beta[i], (A - dx) % A, (B - dy) % B, (C - dz) % C);
+    const uint32_t ci = cx[i] + A * (cy[i] + B * cz[i]), cj = cx[j] + A * (cy[j] + B * cz[j]);
+    if (k1 == k2) {
+      member[e] = {k1, std::min(ci, cj)};
+      self_rev[e] = 1;
+    } else {
+      member[e] = k1 < k2 ? std::make_pair(k1, ci) : std::make_pair(k2, cj);
+    }
+  }
+  std::vector<uint32_t> order(sl.n_pairs);
+  for (uint32_t e = 0; e < sl.n_pairs; ++e) order[e] = e;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return member[a] < member[b]; });
+  struct Class {
+    unsigned long long key;
+    bool self;
+    uint32_t count;
+  };
+  std::vector<Class> classes;
+  for (size_t k = 0; k < order.size(); ++k) {
+    const auto& mk = member[order[k]];
+    if (k > 0 && member[order[k - 1]] == mk) return false;  // the same pair twice
+    if (classes.empty() || classes.back().key != mk.first)
+      classes.push_back(Class{mk.first, self_rev[order[k]] != 0, 0});
+    classes.back().count++;
+  }
+  for (auto& c : classes)
+    if (c.count != (c.self ? cells / 2 : cells)) return false;  // an incomplete class
+  L.m = m;
+  L.A = A;
+  L.B = B;
+  L.C = C;
+  L.cells = static_cast<uint32_t>(cells);
+  L.chunks = (L.cells + 3) / 4;
+  L.full = cells == 64 ? ~0ull : ((1ull << cells) - 1ull);
+  L.site_off.assign(static_cast<size_t>(m) * 4 * L.chunks, 0);
+  for (uint32_t b = 0; b < m; ++b)
+    for (uint32_t c = 0; c < 4 * L.chunks; ++c)
+      L.site_off[b * 4 * L.chunks + c] = host_site_off(site_at[b * L.cells + (c < L.cells ? c : 0)]);
+  // translations: the second site's planes move by -d onto the first site's cells
+  std::map<uint32_t, uint32_t> tr_index;
+  auto translation = [&](uint32_t dpack) -> uint32_t {
+    const uint32_t dx = dpack % 64, dy = (dpack / 64) % 64, dz = dpack / 4096;
+    const uint32_t tx = (A - dx) % A, ty = (B - dy) % B, tz = (C - dz) % C;
+    const uint32_t tkey = tx + 64u * (ty + 64u * tz);
+    auto it = tr_index.find(tkey);
+    if (it != tr_index.end()) return it->second;
+    LatTr t{};
+    t.sx = tx;
+    t.sxr = A - tx;
+    t.sy = A * ty;
+    t.syr = A * B - A * ty;
+    t.sz = A * B * tz;
+    t.szr = L.cells - A * B * tz;
+    for (uint32_t c = 0; c < L.cells; ++c) {
+      const uint32_t x = c % A, y = (c / A) % B;
+      if (x >= tx)
+        t.mxh |= 1ull << c;
+      else
+        t.mxl |= 1ull << c;
+      if (y >= ty)
+        t.myh |= 1ull << c;
+      else
+        t.myl |= 1ull << c;
+    }
+    const uint32_t idx = static_cast<uint32_t>(L.tr.size());
+    L.tr.push_back(t);
+    tr_index[tkey] = idx;
+    return idx;
+  };
+  L.shell.assign(4 * static_cast<size_t>(S), 0);
+  L.deg.assign(static_cast<size_t>(S) * m, 0);
+  for (uint32_t s = 0; s < S; ++s) {
+    std::vector<std::pair<uint64_t, uint32_t>> normal, self;  // (sort key, entry)
+    uint32_t pairs = 0;
+    for (auto& c : classes) {
+      const uint32_t cs = static_cast<uint32_t>(c.key >> 26);
+      if (cs != s) continue;
+      const uint32_t b1 = static_cast<uint32_t>(c.key >> 22) & 0xfu, b2 = static_cast<uint32_t>(c.key >> 18) & 0xfu;
+      const uint32_t t = translation(static_cast<uint32_t>(c.key & 0x3ffffull));
+      const uint32_t en = b1 | (b2 << 4) | (t << 8);
+      // classes sharing (beta2, translation) are adjacent: their translated planes are computed once
+      const uint64_t sk = (static_cast<uint64_t>(en >> 4) << 4) | b1;
+      (c.self ? self : normal).emplace_back(sk, en);
+      pairs += c.count;
+      L.deg[s * m + b1] += 1;
+      if (!c.self) L.deg[s * m + b2] += 1;
+    }
+    std::sort(normal.begin(), normal.end());
+    std::sort(self.begin(), self.end());
+    L.shell[4 * s] = static_cast<uint32_t>(L.ent.size());
+    for (auto& x : normal) L.ent.push_back(x.second);
+    L.shell[4 * s + 1] = static_cast<uint32_t>(L.ent.size());
+    for (auto& x : self) L.ent.push_back(x.second);
+    L.shell[4 * s + 2] = static_cast<uint32_t>(L.ent.size());
+    L.shell[4 * s + 3] = pairs;
+  }
+  return L.tr.size() < (1u << 24);
+}
+
 PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   PreparedJob pj;
   if (job.prec != SQSG_PREC_SINGLE && job.prec != SQSG_PREC_DOUBLE) throw std::invalid_argument("invalid prec");
@@ -159,14 +301,17 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   d.keep = static_cast<uint32_t>(job.keep);
   d.kw = 1;
 
-  size_t blob_size = 0, smem = 0;
+  size_t blob_size = 0, smem = 0, engine_end = 0;
   size_t rec = 16, tsp = 0, tbd = 0;
   std::vector<std::vector<uint32_t>> streams(job.n_sublattices);
   std::vector<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>> k2_data;
   std::vector<std::vector<uint32_t>> k2_nbp_data;
+  // validation, pair streams and lattice tables of every part first: the path is chosen per job
+  std::vector<LatticeTables> lat(job.n_sublattices);
+  bool job_lat = option(kOptForceGeneral) == 0;
+  bool will_k2 = false;
   for (uint32_t p = 0; p < job.n_sublattices; ++p) {
     const sqsg_sublattice& sl = job.sublattices[p];
-    PartDesc& P = d.parts[p];
     if (sl.n_sites == 0) throw std::invalid_argument("empty structure");
     if (sl.n_species == 0 || sl.n_shells == 0) throw std::out_of_range("no coordination shells selected");
     if (sl.n_species > static_cast<uint32_t>(kMaxSpecies))
@@ -185,19 +330,31 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     }
     if (pj.systematic && sl.n_windows != 1)
       throw std::invalid_argument("In \"systematic\" iteration mode only one sublattice is allowed");
+    streams[p] = build_stream(sl);  // validates the pair list
+    job_lat = job_lat && lattice_tables(sl, lat[p]) && sl.n_species >= 2;
+    if (job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64 && sl.n_shells <= kK2MaxShells &&
+        job.keep < 32 && option(kOptForceGeneral) == 0) {
+      bool has0 = false, has1 = false;  // systematic: the window must hold both species
+      for (uint32_t x = sl.windows[0]; x < sl.windows[1]; ++x) (sl.species[x] ? has1 : has0) = true;
+      will_k2 = !pj.systematic || (has0 && has1);
+    }
+  }
+  job_lat = job_lat && !will_k2;
+  d.lat = job_lat ? 1u : 0u;
+  for (uint32_t p = 0; p < job.n_sublattices; ++p) {
+    const sqsg_sublattice& sl = job.sublattices[p];
+    PartDesc& P = d.parts[p];
     P.n_sites = sl.n_sites;
     P.n_species = sl.n_species;
     P.n_shells = sl.n_shells;
     P.n_windows = sl.n_windows;
     P.hw = (sl.n_species + 1) / 2;
     if (sl.n_species > 4) d.kw = 2;
-    streams[p] = build_stream(sl);
     P.stream_words = static_cast<uint32_t>(streams[p].size());
     P.stream_narrow = narrow_stream(sl.n_sites) ? 1u : 0u;
     const size_t skk = static_cast<size_t>(sl.n_shells) * sl.n_species * sl.n_species;
     // binary fast path data: per (shell, site) mask of the neighbours j > i (bit N-1-j)
-    const bool k2 = job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64 && sl.n_shells <= kK2MaxShells &&
-                    job.keep < 32 && option(kOptForceGeneral) == 0;
+    const bool k2 = will_k2;
     std::vector<uint32_t> k2_entries, k2_shells, k2_nbp;
     if (k2) {
       const uint32_t N = sl.n_sites;
@@ -294,11 +451,32 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
       k2_data.emplace_back();
       k2_nbp_data.emplace_back();
     }
+    const LatticeTables& LT = lat[p];
+    size_t planes = 0;  // lattice path: per-lane plane bytes
+    if (job_lat) {
+      P.lat_km = sl.n_species <= 2 ? 2u : (sl.n_species <= 4 ? 4u : 8u);
+      P.lat_basis = LT.m;
+      P.lat_cells = LT.cells;
+      P.lat_chunks = LT.chunks;
+      P.lat_full = LT.full;
+      P.lat_site_off = static_cast<uint32_t>(off);
+      off = align_up(off + 4 * LT.site_off.size(), 16);
+      P.lat_ent_off = static_cast<uint32_t>(off);
+      off = align_up(off + 4 * LT.ent.size(), 16);
+      P.lat_shell_off = static_cast<uint32_t>(off);
+      off = align_up(off + 4 * LT.shell.size(), 16);
+      P.lat_tr_off = static_cast<uint32_t>(off);
+      off = align_up(off + sizeof(LatTr) * LT.tr.size(), 16);
+      P.lat_deg_off = static_cast<uint32_t>(off);
+      off = align_up(off + 4 * LT.deg.size(), 16);
+      planes = static_cast<size_t>(LT.m) * (sl.n_species - 1) * 8 * kBlock;
+    }
     P.stream_off = static_cast<uint32_t>(off);
     const size_t with_stream = align_up(off + 4ull * streams[p].size(), 16);
     const size_t lanes = (static_cast<size_t>((sl.n_sites + 3) / 4) +
                           static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw) * kBlock * 4;
-    const bool staged = !k2 && job.n_sublattices == 1 &&
+    // the lattice path reads the stream only for traces and rebuilt records: never staged
+    const bool staged = !k2 && !job_lat && job.n_sublattices == 1 &&
                         ctas_per_sm(job.device, with_stream + lanes) >= ctas_per_sm(job.device, off + lanes);
     P.stream_global = staged ? 0u : 1u;
     P.static_bytes = static_cast<uint32_t>(staged ? with_stream : off);
@@ -309,7 +487,13 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     P.smem_off = static_cast<uint32_t>(smem);
     P.col_off = static_cast<uint32_t>(off);
     off += static_cast<size_t>((sl.n_sites + 3) / 4) * kBlock * 4;
+    if (job_lat) {
+      off = align_up(off, 16);
+      P.lat_planes_off = static_cast<uint32_t>(off);
+      off += planes;
+    }
     P.hist_off = static_cast<uint32_t>(off);
+    engine_end = smem + off;  // the lattice path needs no histogram (but traces and rebuilt records do)
     off += static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw * kBlock * 4;
     smem += align_up(off, 16);
     // candidate record layout
@@ -338,11 +522,12 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
   d.record_bytes = static_cast<uint32_t>(align_up(rec, 16));
   pj.record_bytes = d.record_bytes;
   d.smem_full = static_cast<uint32_t>(smem);
+  if (job_lat && trace_capacity == 0) smem = align_up(engine_end, 16);  // drop the last part's histogram
   // keep >= 32: each warp's best list (keep+1 entries, rounded up to whole rows of 32) lives in shared
   // memory after the parts; smaller keep uses one register per lane
   if (job.keep >= 32) {
     d.big_len = static_cast<uint32_t>(align_up(job.keep + 1, 32));
-    d.big_off = static_cast<uint32_t>(align_up(smem, 16));
+    d.big_off = static_cast<uint32_t>(align_up(d.smem_full, 16));
     smem = d.big_off + static_cast<size_t>(kBlock / 32) * d.big_len * sizeof(double);
   }
   d.smem_bytes = static_cast<uint32_t>(smem);
@@ -375,6 +560,14 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     if (!k2d.second.empty()) std::memcpy(base + P.k2_shell_off, k2d.second.data(), 4 * k2d.second.size());
     if (!k2_nbp_data[p].empty())
       std::memcpy(base + P.k2_nbp_off, k2_nbp_data[p].data(), 4 * k2_nbp_data[p].size());
+    if (d.lat) {
+      const LatticeTables& LT = lat[p];
+      std::memcpy(base + P.lat_site_off, LT.site_off.data(), 4 * LT.site_off.size());
+      std::memcpy(base + P.lat_ent_off, LT.ent.data(), 4 * LT.ent.size());
+      std::memcpy(base + P.lat_shell_off, LT.shell.data(), 4 * LT.shell.size());
+      std::memcpy(base + P.lat_tr_off, LT.tr.data(), sizeof(LatTr) * LT.tr.size());
+      std::memcpy(base + P.lat_deg_off, LT.deg.data(), 4 * LT.deg.size());
+    }
   }
   // binary systematic path: binomials C(m, j) for m <= window size, j <= ones in the window, kept in
   // global memory after the staged sections (read through the L1 by the per-thread unrank)

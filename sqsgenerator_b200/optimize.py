@@ -64,6 +64,26 @@ def prepare(config: SqsConfiguration) -> list[OptimizationData]:
             st = applied.sliced(sl.sites)
             parts.append((st, st, np.arange(len(st), dtype=np.uint32),
                           np.array([[0, len(st)]], dtype=np.uint32), [sl]))
+    # supercell hint: supercell site k of a x b x c copies of n0 unit-cell sites is
+    # k = ((i * b + j) * c + l) * n0 + s (the supercell loop order, core/structure.h:335-366)
+    a, b, c = (int(v) for v in config.supercell)
+    n0 = len(config.structure_config)
+
+    def supercell_coords(indices):
+        idx = np.asarray(indices, dtype=np.int64)
+        s_, cell = idx % n0, idx // n0
+        l_ = cell % c
+        j_ = (cell // c) % b
+        i_ = cell // (b * c)
+        _, basis = np.unique(s_, return_inverse=True)
+        return np.stack([basis, i_, j_, l_], axis=1).astype(np.uint32)
+
+    hints = []
+    if config.sublattice_mode == SublatticeMode.interact:
+        hints.append(supercell_coords(parts[0][2]))
+    else:
+        for sl in config.composition:
+            hints.append(supercell_coords(sl.sites))
     for k, (st, sst, order, windows, sls) in enumerate(parts):
         radii = config.shell_radii[k]
         weights = config.shell_weights[k]
@@ -80,7 +100,8 @@ def prepare(config: SqsConfiguration) -> list[OptimizationData]:
             prefactors=np.ascontiguousarray(config.prefactors[k], dtype=T),
             pair_weights=_scaled_pair_weights(config.pair_weights[k], weights, K, T),
             target=np.ascontiguousarray(config.target_objective[k], dtype=T),
-            shell_radii=np.asarray(radii), shell_weights=dict(weights), sublattices=sls))
+            shell_radii=np.asarray(radii), shell_weights=dict(weights), sublattices=sls,
+            lattice=hints[k], cells=(a, b, c)))
     return out
 
 
@@ -97,8 +118,10 @@ class _JobBuffers:
 
 
 def build_job(config: SqsConfiguration, data: list[OptimizationData], device: int = 0,
-              callback=None, cancel=None):
-    """The flat ``sqsg_job`` for a configuration (C ABI struct + buffers to keep alive)."""
+              callback=None, cancel=None, lattice_hint: bool = True):
+    """The flat ``sqsg_job`` for a configuration (C ABI struct + buffers to keep alive). With
+    ``lattice_hint`` the supercell coordinates of the sites are passed on (the library checks them and
+    may count bonds with translated bit planes; the result is the same either way)."""
     bufs = _JobBuffers()
     T = dtype_of(config.prec)
     subs = (_native.SqsgSublattice * len(data))()
@@ -115,6 +138,10 @@ def build_job(config: SqsConfiguration, data: list[OptimizationData], device: in
         s.prefactors = bufs.add(d.prefactors.astype(T))
         s.pair_weights = bufs.add(d.pair_weights.astype(T))
         s.target = bufs.add(d.target.astype(T))
+        if lattice_hint and d.lattice is not None:
+            s.lattice = bufs.add(np.ascontiguousarray(d.lattice, dtype=np.uint32).reshape(-1))
+            s.cells[0], s.cells[1], s.cells[2] = (int(v) for v in d.cells)
+            s.n_basis = int(d.lattice[:, 0].max()) + 1
     bufs.keep.append(subs)
     job = _native.SqsgJob()
     job.prec = int(config.prec)

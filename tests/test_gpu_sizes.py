@@ -4,8 +4,8 @@ Every configuration the device evaluates in these runs is traced and checked aga
 ordered bond counts (core/optimization.h:74-77) bit for bit and the objective (optimization.h:79-103)
 bit for bit in the run's precision. Each test also asserts which path the library chose
 (sqsg_plan_job), so that the general pair-stream path in each of its forms (narrow stream staged in
-shared memory, narrow stream read through L1, wide stream for cells above 512 sites) and the
-bit-mask path are each covered.
+shared memory, narrow stream read through L1, wide stream for cells above 512 sites), the bit-mask
+path and the lattice path are each covered, and the paths are checked against each other.
 """
 import collections
 import ctypes as C
@@ -65,33 +65,89 @@ def config4(prec="double", iterations=3000):
                                 composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}])
 
 
+PATHS = {"lattice": {}, "general": {"force_general": 1}}
+
+
+@pytest.mark.parametrize("path", sorted(PATHS))
 @pytest.mark.parametrize("prec", ["double", "single"])
-def test_config3_quinary_256_sites(prec):
+def test_config3_quinary_256_sites(prec, path):
+    """In trace mode the lattice path also runs the pair stream: the traced bonds are the pair
+    stream's, and any configuration whose lattice objective differs is an error of the call."""
     cfg = config3(prec)
-    p = plan_of(cfg)
-    assert p["parts"][0]["path"] == "general"
-    assert p["parts"][0]["stream_narrow"] and p["parts"][0]["stream_staged"]
-    c, d, sp, ob, ids = traced(cfg, 3000, prec)
+    with N.options(**PATHS[path]):
+        p = plan_of(cfg)
+        assert p["parts"][0]["path"] == path
+        if path == "general":
+            assert p["parts"][0]["stream_narrow"] and p["parts"][0]["stream_staged"]
+        c, d, sp, ob, ids = traced(cfg, 3000, prec)
     assert len(d[0].species_packed) == 256 and len(d[0].pairs) == 5376
     assert collections.Counter(sp[0].tolist()) == collections.Counter(d[0].species_packed.tolist())
 
 
+@pytest.mark.parametrize("path", sorted(PATHS))
 @pytest.mark.parametrize("prec", ["double", "single"])
-def test_config4_rocksalt_split_216_sites(prec):
+def test_config4_rocksalt_split_216_sites(prec, path):
     cfg = config4(prec)
-    p = plan_of(cfg)
-    assert [x["path"] for x in p["parts"]] == ["general", "general"]
-    assert not p["parts"][0]["stream_staged"] and not p["parts"][1]["stream_staged"]
-    c, d, sp, ob, ids = traced(cfg, 3000, prec)
+    with N.options(**PATHS[path]):
+        p = plan_of(cfg)
+        assert [x["path"] for x in p["parts"]] == [path, path]
+        assert not p["parts"][0]["stream_staged"] and not p["parts"][1]["stream_staged"]
+        c, d, sp, ob, ids = traced(cfg, 3000, prec)
     assert [len(x.species_packed) for x in d] == [108, 108]
     assert [len(x.pairs) for x in d] == [972, 972]
+
+
+LATTICE_CASES = {
+    "config3": lambda: config3("double", iterations=200000),
+    "config4": lambda: config4("single", iterations=300000),
+    "fcc32_ternary": lambda: cases.fcc32("double", composition={"Ti": 11, "Al": 11, "Nb": 10}, iterations=300000,
+                                         seed=4),
+    "fcc32_systematic_ternary": lambda: cases.fcc32("double", composition={"Ti": 2, "Al": 3, "Nb": 27},
+                                                    iteration_mode="systematic", seed=None, iterations=None, keep=6,
+                                                    pair_weights=None),
+    "perovskite_333": lambda: dict(prec="double", structure=dict(
+        lattice=(np.eye(3) * 4.0).tolist(), coords=[[0, 0, 0], [0.5, 0.5, 0.5], [0.5, 0.5, 0], [0.5, 0, 0.5],
+                                                    [0, 0.5, 0.5]], species=[1] * 5, supercell=[3, 3, 3]),
+        composition={"Ti": 45, "Al": 45, "Nb": 45}, shell_weights={"1": 1.0, "2": 0.5}, iterations=100000, seed=11,
+        thread_config=1, keep=7),
+    "rocksalt_interact": lambda: dict(cases.rocksalt_split("double", cells=(3, 3, 3), iterations=100000, seed=2,
+                                                           composition=[{"sites": "Na", "Ti": 54, "Al": 54},
+                                                                        {"sites": "Cl", "N": 96, "B": 12}]),
+                                      sublattice_mode="interact", shell_weights={"1": 1.0, "2": 0.5}),
+    "bcc_4x4x2_quaternary": lambda: dict(prec="single", structure=dict(
+        lattice=(np.eye(3) * 2.87).tolist(), coords=[[0, 0, 0], [0.5, 0.5, 0.5]], species=[1] * 2,
+        supercell=[4, 4, 2]), composition={"Ti": 16, "Al": 16, "Nb": 16, "V": 16},
+        shell_weights={"1": 1.0, "2": 0.5, "3": 0.25}, iterations=200000, seed=21, thread_config=1, keep=9),
+}
+
+
+@pytest.mark.parametrize("name", sorted(LATTICE_CASES))
+def test_lattice_and_general_paths_agree(name):
+    """The same job on the lattice path and on the pair-stream path: the same result set (objectives,
+    ids, species, SRO) and the same exact objective levels."""
+    cfg = LATTICE_CASES[name]()
+    plan = plan_of(cfg)
+    assert [x["path"] for x in plan["parts"]] == ["lattice"] * len(plan["parts"])
+    a = _full_records(cfg)
+    with N.options(force_general=1):
+        assert plan_of(cfg)["parts"][0]["path"] == "general"
+        b = _full_records(cfg)
+    assert a[0] > 0 and a == b
+
+
+@pytest.mark.parametrize("name", ["fcc32_ternary", "perovskite_333", "bcc_4x4x2_quaternary", "rocksalt_interact"])
+def test_lattice_trace_against_oracle(name):
+    cfg = dict(LATTICE_CASES[name]())
+    cfg["iterations"] = 4000
+    assert plan_of(cfg)["parts"][0]["path"] == "lattice"
+    traced(cfg, 4000, cfg["prec"])
 
 
 def test_narrow_stream_read_through_l1_fcc500():
     """fcc 5x5x5 (500 sites), three species, four shells (12/6/24/12 neighbours): staging the stream
     would cost a CTA per SM, so it is read from the job blob through L1."""
     cfg = fcc((5, 5, 5), {"Ti": 167, "Al": 167, "Nb": 166}, 4, iterations=1500)
-    p = plan_of(cfg)
+    p = plan_of(cfg)  # 125 cells: more than the lattice path's 64
     assert p["parts"][0]["path"] == "general"
     assert p["parts"][0]["stream_narrow"] and not p["parts"][0]["stream_staged"]
     c, d, sp, ob, ids = traced(cfg, 1500, "double")
@@ -101,7 +157,7 @@ def test_narrow_stream_read_through_l1_fcc500():
 def test_wide_stream_above_512_sites_fcc864():
     """fcc 6x6x6 (864 sites): column offsets above 16 bits take the wide stream form."""
     cfg = fcc((6, 6, 6), {"Ti": 432, "Al": 432}, 2, iterations=1000)
-    p = plan_of(cfg)
+    p = plan_of(cfg)  # 216 cells: general path
     assert p["parts"][0]["path"] == "general" and not p["parts"][0]["stream_narrow"]
     c, d, sp, ob, ids = traced(cfg, 1000, "double")
     assert len(d[0].species_packed) == 864
@@ -121,6 +177,28 @@ def test_bitmask_and_general_paths_agree_fcc32(prec):
     assert np.array_equal(ids_a[order_a], ids_b[order_b])
     assert np.array_equal(sp_a[order_a], sp_b[order_b])
     assert ob_a[order_a].tobytes() == ob_b[order_b].tobytes()
+
+
+def _full_records(cfg):
+    c = S.parse_config(cfg)
+    d = S.prepare(c)
+    job, bufs = build_job(c, d)
+    run = C.c_void_p()
+    N.check(N.lib().sqsg_optimize(C.byref(job), C.byref(run)))
+    try:
+        n = int(N.lib().sqsg_run_count(run))
+        T = np.float64 if int(c.prec) == 1 else np.float32
+        nsp = sum(len(x.species_packed) for x in d)
+        nsro = sum(x.prefactors.size for x in d)
+        obj = np.zeros(max(n, 1), T)
+        sp = np.zeros(max(n, 1) * nsp, np.uint8)
+        sro = np.zeros(max(n, 1) * nsro, T)
+        ids = np.zeros(max(n, 1), np.uint64)
+        N.check(N.lib().sqsg_run_copy(run, 0, n, N.ptr(obj), None, N.ptr(sp), N.ptr(sro), N.ptr(ids)))
+        return (n, obj[:n].tobytes(), sp[: n * nsp].tobytes(), sro[: n * nsro].tobytes(), ids[:n].tobytes(),
+                tuple(cases.run_levels(run)))
+    finally:
+        N.lib().sqsg_run_free(run)
 
 
 def _records(cfg):
@@ -178,6 +256,9 @@ def test_staging_wait_runs_out_and_the_context_stays_usable():
 
 def test_plan_reports_occupancy_on_the_device():
     p = plan_of(config3())
+    assert p["kernel"] == "sqsg_engine_lat" and p["ctas_per_sm"] >= 1
+    with N.options(force_general=1):
+        p = plan_of(config3())
     assert p["kernel"] == "sqsg_engine_wide" and p["ctas_per_sm"] >= 1
     p = plan_of(cases.fcc32("double"))
     assert p["kernel"] == "sqsg_engine_mask" and p["ctas_per_sm"] >= 1

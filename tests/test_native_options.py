@@ -24,11 +24,48 @@ def test_plan_paths_without_a_device():
     p = plan_of(cases.fcc32("double"))
     assert p["kernel"] == "sqsg_engine_mask" and p["parts"][0]["path"] == "bitmask"
     p = plan_of(cases.quinary("double", cells=(4, 4, 4)))
-    assert p["kernel"] == "sqsg_engine_wide" and p["parts"][0]["path"] == "general"
-    assert p["parts"][0]["stream_narrow"]
+    assert p["kernel"] == "sqsg_engine_lat" and p["parts"][0]["path"] == "lattice"
     p = plan_of(cases.rocksalt_split("double", cells=(3, 3, 3)))
-    assert [x["path"] for x in p["parts"]] == ["general", "general"]
-    assert not any(x["stream_staged"] for x in p["parts"])  # split jobs read the stream through L1
+    assert p["kernel"] == "sqsg_engine_lat" and [x["path"] for x in p["parts"]] == ["lattice", "lattice"]
+    with N.options(force_general=1):
+        p = plan_of(cases.quinary("double", cells=(4, 4, 4)))
+        assert p["kernel"] == "sqsg_engine_wide" and p["parts"][0]["path"] == "general"
+        assert p["parts"][0]["stream_narrow"]
+        p = plan_of(cases.rocksalt_split("double", cells=(3, 3, 3)))
+        assert [x["path"] for x in p["parts"]] == ["general", "general"]
+        assert not any(x["stream_staged"] for x in p["parts"])  # split jobs read the stream through L1
+
+
+def _job(cfg, **kw):
+    c = S.parse_config(cfg)
+    d = S.prepare(c)
+    return c, d, build_job(c, d, **kw)
+
+
+def test_lattice_hint_is_checked():
+    """The supercell hint only selects the lattice path when it is consistent with the pair list."""
+    cfg = cases.quinary("double", cells=(3, 3, 3))
+    c, d, (job, bufs) = _job(cfg, lattice_hint=False)
+    assert N.plan(job)["parts"][0]["path"] == "general"
+    # a hint that swaps two sites' cells: some translation classes become incomplete
+    bad = d[0].lattice.copy()
+    bad[[0, 5], 1:] = bad[[5, 0], 1:]
+    d[0].lattice = bad
+    job, bufs = build_job(c, d)
+    assert N.plan(job)["parts"][0]["path"] == "general"
+    # a cell index out of range is rejected too
+    c, d, _ = _job(cfg)
+    d[0].lattice = d[0].lattice.copy()
+    d[0].lattice[3, 2] = 99
+    job, bufs = build_job(c, d)
+    assert N.plan(job)["parts"][0]["path"] == "general"
+
+
+def test_lattice_hint_of_more_than_64_cells_is_not_used():
+    cfg = cases.fcc32("double", composition={"Ti": 250, "Al": 250}, iterations=1000)
+    cfg["structure"]["supercell"] = [5, 5, 5]
+    c, d, (job, bufs) = _job(cfg)
+    assert N.plan(job)["parts"][0]["path"] == "general"
 
 
 def test_force_general_option():
