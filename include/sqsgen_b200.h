@@ -203,6 +203,17 @@ sqsg_status sqsg_run_levels(const sqsg_run* run, uint32_t* n, double* values, ui
 /* candidates: records the device appended; truncated: 1 when the record set hit its capacity;
  * levels_exact: 0 when the level table overflowed (then only the records define the result). */
 sqsg_status sqsg_run_info(const sqsg_run* run, uint64_t* candidates, int32_t* truncated, int32_t* levels_exact);
+/* Host-side time of the stages of the call that produced the run, in nanoseconds (*n: in =
+ * capacity, out = SQSG_STAGE_COUNT): job preparation and tiling; uploads; the engine kernel (CUDA
+ * events); the host's wait for it (kernel time plus launch and queueing); counters and objective
+ * levels downloaded and assessed; result-set selection (device selection, record rebuilding and the
+ * copy into host memory); and the whole call. Stages of the served form are not recorded (zeros).
+ * No reference counterpart. */
+enum {
+  SQSG_STAGE_PREPARE = 0, SQSG_STAGE_UPLOAD = 1, SQSG_STAGE_KERNEL = 2, SQSG_STAGE_WAIT = 3,
+  SQSG_STAGE_LEVELS = 4, SQSG_STAGE_SELECT = 5, SQSG_STAGE_TOTAL = 6, SQSG_STAGE_COUNT = 7
+};
+sqsg_status sqsg_run_stages(const sqsg_run* run, uint64_t* ns, uint32_t* n);
 /* Bytes the call copied host->device (job blob, tiles, descriptors) and device->host (records,
  * level table, counters). */
 sqsg_status sqsg_run_transfer(const sqsg_run* run, uint64_t* h2d_bytes, uint64_t* d2h_bytes);

@@ -36,7 +36,7 @@ EXPORTED = (
     "sqsg_optimize_trace", "sqsg_optimize_batch", "sqsg_run_levels", "sqsg_run_info",
     "sqsg_microbench", "sqsg_run_transfer", "sqsg_optimize_levels_noalloc",
     "sqsg_server_create", "sqsg_server_submit", "sqsg_server_wait", "sqsg_server_stats", "sqsg_server_destroy",
-    "sqsg_server_running", "sqsg_set_option", "sqsg_get_option", "sqsg_plan_job",
+    "sqsg_server_running", "sqsg_set_option", "sqsg_get_option", "sqsg_plan_job", "sqsg_run_stages",
 )
 
 PATH_NAMES = {0: "general", 1: "bitmask", 2: "lattice"}
@@ -174,6 +174,7 @@ def lib():
         L.sqsg_run_levels.argtypes = [vp, C.POINTER(u32), vp, vp, vp]
         L.sqsg_run_info.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.sqsg_run_transfer.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
+        L.sqsg_run_stages.argtypes = [vp, vp, C.POINTER(u32)]
         L.sqsg_optimize_levels_noalloc.argtypes = [C.POINTER(SqsgJob), vp, C.POINTER(u32), vp, vp, vp,
                                                    C.POINTER(SqsgStatistics), C.c_char_p, C.c_size_t]
         L.sqsg_server_create.argtypes = [C.POINTER(SqsgServerOptions), C.POINTER(vp)]
@@ -250,6 +251,17 @@ def plan(job) -> dict:
              for k in range(p.n_parts)]
     return dict(kernel=p.kernel.decode(), smem_bytes=int(p.smem_bytes), ctas_per_sm=int(p.ctas_per_sm),
                 record_bytes=int(p.record_bytes), parts=parts)
+
+
+STAGE_NAMES = ("prepare", "upload", "kernel", "wait", "levels", "select", "total")
+
+
+def run_stages(run) -> dict:
+    """Host time (seconds) per stage of the sqsg_optimize call that produced `run`."""
+    ns = np.zeros(len(STAGE_NAMES), np.uint64)
+    n = C.c_uint32(len(STAGE_NAMES))
+    check(lib().sqsg_run_stages(run, ptr(ns), C.byref(n)))
+    return {name: float(ns[k]) * 1e-9 for k, name in enumerate(STAGE_NAMES[: n.value])}
 
 
 def device_count() -> int:

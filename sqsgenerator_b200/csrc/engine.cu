@@ -237,6 +237,7 @@ struct Run {
   bool truncated = false, levels_exact = true;
   uint64_t candidates = 0;
   uint64_t h2d_bytes = 0, d2h_bytes = 0;
+  uint64_t stage_ns[SQSG_STAGE_COUNT] = {};  // host-side time per stage of the call (sqsg_run_stages)
 };
 
 // The reference accepts a configuration when its objective is <= the search threshold, which only
@@ -662,6 +663,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     }
     const EngineKernel kernel = kernel_of(kind);
     const uint32_t grid = launch_grid(device, smem, tiles.size(), kernel);
+    const uint64_t t_launch = now_ns();
     CUDA_CHECK(cudaEventRecord(ws->ev_start, ws->stream));
     if (!tiles.empty()) {
       kernel<<<grid, kBlock, smem, ws->stream>>>(
@@ -724,6 +726,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     float ms = 0.f;
     CUDA_CHECK(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
     loop_ms_total += ms;
+    const uint64_t t_done = now_ns();
     std::vector<unsigned long long> cnt(nj * kNumCounters);
     CUDA_CHECK(cudaMemcpy(cnt.data(), counters, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     unsigned long long status = 0;
@@ -768,6 +771,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     if (rerun && trace) continue;  // a traced job is one job: run it again whole
 
     const uint64_t t_loop = now_ns();
+    const uint64_t t_attempt = t_launch - t_setup;  // uploads (and tiles) of this attempt
     runs.assign(nj, Run{});
     std::vector<size_t> again;  // overflowed jobs of a batch run again alone, the rest finish now
     for (size_t j = 0; j < nj; ++j) {
@@ -839,6 +843,17 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       if (trace->id) CUDA_CHECK(cudaMemcpy(trace->id, ws->trace_id.p, n * 8, cudaMemcpyDeviceToHost));
     }
     const uint64_t t_end = now_ns();
+    for (size_t j = 0; j < nj; ++j) {
+      uint64_t* st = runs[j].stage_ns;
+      if (st[SQSG_STAGE_TOTAL]) continue;  // a job that ran again alone keeps its own profile
+      st[SQSG_STAGE_PREPARE] = pjs[j].prepare_ns + (t_setup - t0);
+      st[SQSG_STAGE_UPLOAD] = t_attempt;
+      st[SQSG_STAGE_KERNEL] = static_cast<uint64_t>(loop_ms_total * 1e6);
+      st[SQSG_STAGE_WAIT] = t_done - t_launch;
+      st[SQSG_STAGE_LEVELS] = t_loop - t_done;
+      st[SQSG_STAGE_SELECT] = t_end - t_loop;
+      st[SQSG_STAGE_TOTAL] = pjs[j].prepare_ns + (t_end - t0);
+    }
     std::vector<bool> rerun_job(nj, false);
     for (size_t j : again) rerun_job[j] = true;
     for (size_t j = 0; j < nj; ++j) {
@@ -1466,7 +1481,9 @@ static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, co
     std::vector<const sqsg_job*> srcs;
     for (uint32_t j = 0; j < n; ++j) {
       if (jobs[j].device != device) throw std::invalid_argument("a batch runs on one device");
+      const uint64_t tp = now_ns();
       pjs.push_back(prepare(jobs[j], trace ? trace->capacity : 0));
+      pjs.back().prepare_ns = now_ns() - tp;
       srcs.push_back(&jobs[j]);
     }
     if (n == 1 || trace) {
@@ -1626,6 +1643,17 @@ sqsg_status sqsg_run_levels(const sqsg_run* run, uint32_t* n, double* values, ui
       if (counts) counts[k] = r.level_count[k];
       if (checksums) checksums[k] = r.level_checksum[k];
     }
+  });
+}
+
+sqsg_status sqsg_run_stages(const sqsg_run* run, uint64_t* ns, uint32_t* n) {
+  return guarded([&] {
+    if (!run || !n) throw std::invalid_argument("null pointer");
+    const uint32_t cap = *n;
+    *n = SQSG_STAGE_COUNT;
+    if (cap < SQSG_STAGE_COUNT) throw std::length_error("stage capacity too small");
+    if (ns)
+      for (int k = 0; k < SQSG_STAGE_COUNT; ++k) ns[k] = run->r.stage_ns[k];
   });
 }
 

@@ -33,6 +33,7 @@ struct PreparedJob {
   uint64_t max_results = 0;     // caller's record capacity (0 = default)
   uint64_t range_first = 0, range_count = 0;  // share of the configuration space to evaluate
   // a re-run of an overflowed job: record capacity, starting threshold, passes already made
+  uint64_t prepare_ns = 0;      // host time of prepare()
   uint64_t rerun_capacity = 0;
   double rerun_threshold = 0.0;
   int passes = 0;
