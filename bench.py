@@ -57,6 +57,11 @@ def workload_config(name: str):
                                     composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}]), (
             "rocksalt 3x3x3 (216 sites) split: Ti54Al54 cations and N96B12 anions optimised together, 2 shells per "
             "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations, float64")
+    if name == "split_single":
+        return cases.rocksalt_split("single", cells=(3, 3, 3), iterations=500_000_000, seed=1,
+                                    composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}]), (
+            "rocksalt 3x3x3 (216 sites) split: Ti54Al54 cations and N96B12 anions optimised together, 2 shells per "
+            "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations, float32")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -116,6 +121,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
+        self.util = []  # NVML utilization.gpu samples (percent of time a kernel ran)
         self.nvml = None
         self.proc = None
         self.path = None
@@ -139,6 +145,7 @@ class ClockSampler:
                 nv.nvmlDeviceGetCurrentClocksThrottleReasons
             self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
                               float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)), int(get_reasons(h))))
+            self.util.append(float(nv.nvmlDeviceGetUtilizationRates(h).gpu))
         except Exception:  # noqa: BLE001 — a failed read is a missing sample
             pass
 
@@ -193,8 +200,11 @@ class ClockSampler:
         mx = max(r[1] for r in self.rows)
         reasons = sorted({n for r in self.rows for n, b in self.REASON_BITS.items() if r[2] & b})
         loaded = [v for v in sm if v > 0.5 * mx] or sm
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "samples": len(self.rows),
-                "source": "nvml" if self.nvml else "nvidia-smi", "reasons": reasons}
+        out = {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "samples": len(self.rows),
+               "source": "nvml" if self.nvml else "nvidia-smi", "reasons": reasons}
+        if self.util:
+            out["util_mean"] = statistics.mean(self.util)
+        return out
 
 
 def cpu_sample(seconds: float, keep: int, workload: str = "systematic"):
@@ -222,14 +232,15 @@ def cpu_sample(seconds: float, keep: int, workload: str = "systematic"):
     cfg, _ = workload_config(workload)
     c = S.parse_config(cfg)
     d = S.prepare(c)
-    mode = "split" if workload == "split" else "interact"
+    mode = "split" if workload.startswith("split") else "interact"
+    prec = "double" if int(c.prec) == 1 else "single"
     probe = 20_000
     t = time.perf_counter()
-    oracle.optimize(d, iterations=probe, keep=c.keep, threads=threads, sublattice_mode=mode)
+    oracle.optimize(d, prec=prec, iterations=probe, keep=c.keep, threads=threads, sublattice_mode=mode)
     rate = probe / (time.perf_counter() - t)
     count = max(probe, int(rate * seconds))
     t = time.perf_counter()
-    _, st = oracle.optimize(d, iterations=count, keep=c.keep, threads=threads, sublattice_mode=mode)
+    _, st = oracle.optimize(d, prec=prec, iterations=count, keep=c.keep, threads=threads, sublattice_mode=mode)
     dt = time.perf_counter() - t
     return count, dt, threads, (
         f"{count} random configurations through the restated reference optimizer loop (rapidrand shuffler shared by "
@@ -259,14 +270,161 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args):
-    import numpy as np
+def check_records(d, prec: str, recs) -> dict:
+    """Checker of the cpu_baseline leg: the objective of each sampled record recomputed by the oracle
+    (restated reference count_bonds + compute_objective, parts summed left to right) must equal the
+    device's bit for bit."""
+    import oracle
+
+    T = np.float64 if prec == "double" else np.float32
+    ok = 0
+    for species, obj in recs:
+        tot, off = None, 0
+        for part in d:
+            n = len(part.species_packed)
+            o, _ = oracle.evaluate(part, species[off:off + n], prec)
+            off += n
+            tot = o if tot is None else T(tot + o)
+        ok += int(np.asarray(tot, T).tobytes() == np.asarray(obj, T).tobytes())
+    return {"records_checked": len(recs), "records_bit_exact": ok}
+
+
+def measure(workload: str, steps: int, warmup: int, device: int, world: int, rank: int, max_results: int,
+            limit: int = 0) -> dict:
+    """One workload through sqsg_optimize (sqsg_optimize_batch for the 64 chains of the quinary
+    workload): `warmup` untimed steps, then `steps` timed steps with an L2 flush before each."""
     import torch
 
     import cases as _cases
     import sqsgenerator_b200 as S
     from sqsgenerator_b200 import _native as N
     from sqsgenerator_b200.optimize import build_job
+    from sqsgenerator_b200.shard import shard_range
+
+    cfg, desc = workload_config(workload)
+    c = S.parse_config(cfg)
+    d = S.prepare(c)
+    n_jobs = 64 if workload.startswith("quinary") else 1
+    per_job = c.iterations if not limit else min(limit, c.iterations)
+    first, count = shard_range(per_job, world, rank)
+    jobs = (N.SqsgJob * n_jobs)()
+    keep_alive = []
+    for k in range(n_jobs):
+        ck = S.parse_config(dict(cfg, seed=k)) if n_jobs > 1 else c
+        job, bufs = build_job(ck, d, device=device)
+        job.range_first, job.range_count, job.max_results = first, count, max_results
+        jobs[k] = job
+        keep_alive.append(bufs)
+    L = N.lib()
+    P_total = sum(len(x.pairs) for x in d)
+    nsp = sum(len(x.species_packed) for x in d)
+    nsro = sum(x.prefactors.size for x in d)
+    T = np.float64 if int(c.prec) == 1 else np.float32
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+
+    def step():
+        runs = (C.c_void_p * n_jobs)()
+        t0 = time.perf_counter()
+        if n_jobs == 1:
+            N.check(L.sqsg_optimize(C.byref(jobs[0]), C.cast(runs, C.POINTER(C.c_void_p))))
+        else:
+            N.check(L.sqsg_optimize_batch(jobs, n_jobs, C.cast(runs, C.POINTER(C.c_void_p))))
+        results, sample = 0, []
+        t_copy = time.perf_counter()
+        for k in range(n_jobs):
+            run = runs[k]
+            n = int(L.sqsg_run_count(run))
+            obj = np.empty(max(n, 1), T)
+            sp = np.empty(max(n, 1) * nsp, np.uint8)
+            sro = np.empty(max(n, 1) * nsro, T)
+            ids = np.empty(max(n, 1), np.uint64)
+            N.check(L.sqsg_run_copy(run, 0, n, N.ptr(obj), None, N.ptr(sp), N.ptr(sro), N.ptr(ids)))
+            results += n
+            if k == 0:
+                rows = sp[: n * nsp].reshape(n, nsp)
+                pick = np.unique(np.linspace(0, max(n - 1, 0), num=min(n, 64)).astype(np.int64)) if n else []
+                sample = [(rows[i].copy(), obj[i]) for i in pick]
+        wall = time.perf_counter() - t0
+        copy_s = time.perf_counter() - t_copy
+        finished = h2d = d2h = 0
+        for k in range(n_jobs):
+            st = N.SqsgStatistics()
+            N.check(L.sqsg_run_statistics(runs[k], C.byref(st)))
+            finished += int(st.finished)
+            a, b = C.c_uint64(), C.c_uint64()
+            N.check(L.sqsg_run_transfer(runs[k], C.byref(a), C.byref(b)))
+            h2d += a.value
+            d2h += b.value
+            if k == 0:
+                loop = st.timings_ns[2] * 1e-9
+        stages = N.run_stages(runs[0])
+        stages["copy_to_caller"] = copy_s
+        levels = _cases.run_levels(runs[0])
+        info_c, info_t, info_e = C.c_uint64(), C.c_int32(), C.c_int32()
+        N.check(L.sqsg_run_info(runs[0], C.byref(info_c), C.byref(info_t), C.byref(info_e)))
+        for k in range(n_jobs):
+            L.sqsg_run_free(runs[k])
+        return dict(wall=wall, loop=loop, finished=finished, results=results, h2d=h2d, d2h=d2h, levels=levels,
+                    sample=sample, stages=stages, truncated=bool(info_t.value))
+
+    for _ in range(warmup):
+        step()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    out = []
+    with ClockSampler(device) as clk:
+        for _ in range(steps):
+            flush.fill_(1)  # L2 flush between timed steps (256 MiB > 126 MB L2)
+            torch.cuda.synchronize()
+            out.append(step())
+        torch.cuda.synchronize()
+    plan = N.plan(jobs[0])
+    return dict(workload=workload, desc=desc, config=c, data=d, n_jobs=n_jobs, total=per_job * n_jobs,
+                P_total=P_total, nsp=nsp, steps=steps, out=out, clocks=clk.summary(), plan=plan,
+                loop=sum(o["loop"] for o in out), wall=sum(o["wall"] for o in out),
+                finished=sum(o["finished"] for o in out))
+
+
+def roofline_of(res: dict, smem_bw: float, int_rate: float, world: int = 1) -> dict:
+    """Fixed algorithmic work per configuration: 2*P shared-memory species bytes (P pairs), 3*P integer
+    operations; divided by the kernel's CUDA-event time per launch and by the in-run peaks."""
+    launch_s = res["loop"] / res["steps"]
+    configs_per_launch = res["finished"] / res["steps"] / world
+    P = res["P_total"]
+    achieved = 2 * P * configs_per_launch / launch_s / 1e9
+    prof = os.path.join(ROOT, "profiles", f"sqsg_engine_{res['workload']}.json")
+    traffic, traffic_case = None, None
+    if os.path.exists(prof):
+        pj = json.load(open(prof))
+        traffic, traffic_case = pj.get("dram_bytes_per_launch"), pj.get("case")
+    return {"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
+            "frac": achieved / (smem_bw / 1e9), "traffic": traffic, "traffic_case": traffic_case,
+            "peak_source": "measured in this run: conflict-free LDS.32 microbenchmark (sqsg_microbench kind 0)",
+            "algorithmic": f"2*P = {2 * P} B of shared-memory species reads per configuration (P = {P} pairs)",
+            "int32_frac": (3 * P * configs_per_launch / launch_s) / int_rate, "int32_peak_ops": int_rate,
+            "kernel": res["plan"]["kernel"], "paths": [p["path"] for p in res["plan"]["parts"]],
+            "ctas_per_sm": res["plan"]["ctas_per_sm"]}
+
+
+def extra_line(res: dict, smem_bw: float, int_rate: float, cpu: dict | None, parity: dict | None) -> dict:
+    last = res["out"][-1]
+    return {"workload": res["desc"], "value": res["finished"] / res["loop"], "unit": "configs/s",
+            "steps": res["steps"], "ms_per_step": res["loop"] / res["steps"] * 1e3,
+            "configs_per_step": res["finished"] // res["steps"],
+            "e2e": {"value": res["finished"] / res["wall"], "unit": "configs/s", "h2d_bytes_per_step": last["h2d"],
+                    "d2h_bytes_per_step": last["d2h"], "ms_per_step": res["wall"] / res["steps"] * 1e3,
+                    "host_stages_s": last["stages"]},
+            "roofline": roofline_of(res, smem_bw, int_rate), "clocks": res["clocks"], "cpu_baseline": cpu,
+            "parity": parity, "results": {"records_per_step": last["results"], "truncated": last["truncated"],
+                                          "best_levels": last["levels"][:3]}}
+
+
+def run_b200(args):
+    import torch
+
+    from sqsgenerator_b200 import _native as N
+    from sqsgenerator_b200.shard import merge_levels
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -280,88 +438,8 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     device = local
     torch.cuda.set_device(device)
-    cfg, desc = workload_config(args.workload)
-    c = S.parse_config(cfg)
-    d = S.prepare(c)
-    n_jobs = 64 if args.workload == "quinary" else 1
-    per_job = c.iterations if not args.limit else min(args.limit, c.iterations)
-    total = per_job * n_jobs
-    # one GPU's share: contiguous ranges of the configuration space (jobs keep their own seeds)
-    from sqsgenerator_b200.shard import merge_levels, shard_range
-
-    first, count = shard_range(per_job, world, rank)
-    jobs = (N.SqsgJob * n_jobs)()
-    keep_alive = []
-    for k in range(n_jobs):
-        if n_jobs > 1:
-            cfg_k = dict(cfg, seed=k)
-            ck = S.parse_config(cfg_k)
-        else:
-            ck = c
-        job, bufs = build_job(ck, d, device=device)
-        job.range_first = first
-        job.range_count = count
-        job.max_results = args.max_results
-        jobs[k] = job
-        keep_alive.append(bufs)
-    L = N.lib()
-    P_total = sum(len(x.pairs) for x in d)
-    nsp = sum(len(x.species_packed) for x in d)
-    nsro = sum(x.prefactors.size for x in d)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
-
-    def step():
-        runs = (C.c_void_p * n_jobs)()
-        t0 = time.perf_counter()
-        if n_jobs == 1:
-            N.check(L.sqsg_optimize(C.byref(jobs[0]), C.cast(runs, C.POINTER(C.c_void_p))))
-        else:
-            N.check(L.sqsg_optimize_batch(jobs, n_jobs, C.cast(runs, C.POINTER(C.c_void_p))))
-        results = 0
-        for k in range(n_jobs):
-            run = runs[k]
-            n = int(L.sqsg_run_count(run))
-            obj = np.empty(max(n, 1), np.float64)
-            sp = np.empty(max(n, 1) * nsp, np.uint8)
-            sro = np.empty(max(n, 1) * nsro, np.float64)
-            ids = np.empty(max(n, 1), np.uint64)
-            N.check(L.sqsg_run_copy(run, 0, n, N.ptr(obj), None, N.ptr(sp), N.ptr(sro), N.ptr(ids)))
-            results += n
-        wall = time.perf_counter() - t0
-        finished = 0
-        h2d = d2h = 0
-        for k in range(n_jobs):
-            st = N.SqsgStatistics()
-            N.check(L.sqsg_run_statistics(runs[k], C.byref(st)))
-            finished += int(st.finished)
-            a, b = C.c_uint64(), C.c_uint64()
-            N.check(L.sqsg_run_transfer(runs[k], C.byref(a), C.byref(b)))
-            h2d += a.value
-            d2h += b.value
-            if k == 0:
-                loop = st.timings_ns[2] * 1e-9
-        levels = _cases.run_levels(runs[0])
-        for k in range(n_jobs):
-            L.sqsg_run_free(runs[k])
-        return dict(wall=wall, loop=loop, finished=finished, results=results, h2d=h2d, d2h=d2h, levels=levels)
-
-    for _ in range(args.warmup):
-        step()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    out = []
-    with ClockSampler(device) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1)  # L2 flush between timed steps (256 MiB > 126 MB L2)
-            torch.cuda.synchronize()
-            out.append(step())
-        torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    loop = sum(o["loop"] for o in out)
-    wall = sum(o["wall"] for o in out)
-    finished = sum(o["finished"] for o in out)
+    res = measure(args.workload, args.steps, args.warmup, device, world, rank, args.max_results, args.limit)
+    loop, wall, finished = res["loop"], res["wall"], res["finished"]
     if world > 1:
         t = torch.tensor([loop, wall], dtype=torch.float64, device=f"cuda:{device}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -370,53 +448,65 @@ def run_b200(args):
         torch.distributed.all_reduce(f)
         finished = int(f.item())
         gathered = [None] * world
-        torch.distributed.all_gather_object(gathered, out[-1]["levels"])
+        torch.distributed.all_gather_object(gathered, res["out"][-1]["levels"])
     else:
-        gathered = [out[-1]["levels"]]
+        gathered = [res["out"][-1]["levels"]]
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
         return
+    c = res["config"]
     levels = merge_levels(gathered, c.keep)  # exact: counts and checksum halves add up
     parity = None
     golden_path = os.path.join(ROOT, "tests", "golden", "fcc32_systematic_levels.json")
     if args.workload == "systematic" and not args.limit and os.path.exists(golden_path):
         g = json.load(open(golden_path))["double"]
         parity = {"levels_match_oracle": levels == [(x["objective"], x["count"], x["checksum"]) for x in g],
-                  "best_objective": levels[0][0], "optimal_configurations": levels[0][1]}
-    value = finished / loop
-    e2e = finished / wall
+                  "best_objective": levels[0][0], "optimal_configurations": levels[0][1],
+                  "source": "tests/golden/fcc32_systematic_levels.json (the oracle's exhaustive enumeration)"}
     smem_bw, _ = N.microbench(0, device)
     int_rate, _ = N.microbench(1, device)
-    launch_s = loop / args.steps
-    configs_per_launch = finished / args.steps / world
-    alg_bytes = 2 * P_total * configs_per_launch
-    achieved = alg_bytes / launch_s / 1e9
-    prof = os.path.join(ROOT, "profiles", f"sqsg_engine_{args.workload}.json")
-    traffic = None
-    if os.path.exists(prof):
-        traffic = json.load(open(prof)).get("dram_bytes_per_launch")
-    roofline = {"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
-                "frac": achieved / (smem_bw / 1e9), "traffic": traffic,
-                "peak_source": "measured in this run: conflict-free LDS.32 microbenchmark (sqsg_microbench kind 0)",
-                "algorithmic": f"2*P = {2 * P_total} B of shared-memory species reads per configuration",
-                "int32_frac": (3 * P_total * configs_per_launch / launch_s) / int_rate,
-                "int32_peak_ops": int_rate}
+    res_w = dict(res, loop=loop, wall=wall, finished=finished)
+    roofline = roofline_of(res_w, smem_bw, int_rate, world)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         n, dt, threads, sample = cpu_sample(args.cpu_seconds, c.keep, args.workload)
         cpu = {"value": n / dt, "unit": "configs/s", "cores": threads, "kind": "port", "sample": sample}
-    line = {"metric": METRIC, "value": value, "unit": "configs/s", "n_gpus": world, "steps": args.steps,
+    last = res["out"][-1]
+    line = {"metric": METRIC, "value": finished / loop, "unit": "configs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": loop / args.steps * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "configs_per_step": total, "sites": nsp, "pairs": P_total, "jobs": n_jobs,
-                       "l2": "flushed between timed steps (256 MiB device write)",
-                       "max_results": args.max_results,
+            "config": {"workload": res["desc"], "configs_per_step": res["total"], "sites": res["nsp"],
+                       "pairs": res["P_total"], "jobs": res["n_jobs"],
+                       "l2": "flushed between timed steps (256 MiB device write)", "max_results": args.max_results,
                        "parallelism": f"configuration space split into {world} contiguous ranges"},
-            "e2e": {"value": e2e, "unit": "configs/s", "h2d_bytes_per_step": out[-1]["h2d"],
-                    "d2h_bytes_per_step": out[-1]["d2h"], "ms_per_step": wall / args.steps * 1e3},
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": args.steps,
-            "results": {"records_per_step": out[-1]["results"], "levels": levels[:3]}, "parity": parity}
+            "e2e": {"value": finished / wall, "unit": "configs/s", "h2d_bytes_per_step": last["h2d"],
+                    "d2h_bytes_per_step": last["d2h"], "ms_per_step": wall / args.steps * 1e3,
+                    "host_stages_s": last["stages"]},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": res["clocks"], "gpu_launches": args.steps,
+            "results": {"records_per_step": last["results"], "truncated": last["truncated"],
+                        "truncation_note": "records are capped at max_results per step; the exact objective "
+                                           "levels (counts and id checksums) cover the whole space",
+                        "levels": levels[:3]},
+            "parity": parity}
+    if world == 1 and args.extras:
+        extras = {}
+        for name, steps in (("random", 20), ("quinary", 2), ("split", 2), ("split_single", 2)):
+            r = measure(name, steps, 1, device, 1, 0, 0)
+            cpu_x, par = None, None
+            if not args.no_cpu_baseline:
+                n, dt, threads, sample = cpu_sample(args.cpu_seconds / 2, r["config"].keep, name)
+                cpu_x = {"value": n / dt, "unit": "configs/s", "cores": threads, "kind": "port", "sample": sample}
+                prec = "double" if int(r["config"].prec) == 1 else "single"
+                par = check_records(r["data"], prec, r["out"][-1]["sample"])
+            extras[name] = extra_line(r, smem_bw, int_rate, cpu_x, par)
+            line["gpu_launches"] += r["steps"] * (1 + 1)  # engine + rebuilt records per step
+        import copy
+
+        served_args = copy.copy(args)
+        served_args.warmup = 1
+        extras["served"] = served_measure(served_args, device, 1, 0, smem_bw)
+        line["extras"] = extras
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -434,12 +524,39 @@ def _run_digest(L, N, run, cases_mod):
                 finished=int(st.finished), latency_ns=int(st.timings_ns[0]))
 
 
-def run_served(args):
+def cpu_served_sample(prepared, seconds: float) -> dict:
+    """cpu_baseline leg of the served stream: its jobs in arrival order through the restated reference
+    loop (oracle) on all host cores, each cut to a bounded budget, until `seconds` have passed."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    done = 0
+    jobs = 0
+    t0 = time.perf_counter()
+    for _, c, d, _ in prepared:
+        if time.perf_counter() - t0 > seconds:
+            break
+        if int(c.iteration_mode) == 1:
+            n = min(int(c.iterations), 200_000)
+            oracle.systematic_levels(d[0], keep=c.keep, threads=threads, first=0, count=n)
+        else:
+            n = min(int(c.iterations), 20_000)
+            oracle.optimize(d, iterations=n, keep=c.keep, threads=threads, sublattice_mode="interact")
+        done += n
+        jobs += 1
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "configs/s", "cores": threads, "kind": "port",
+            "sample": f"the first {jobs} jobs of the stream in arrival order, each cut to at most 20,000 random "
+                      "configurations (200,000 ranks for systematic jobs), through the restated reference optimizer "
+                      f"loop on {threads} threads"}
+
+
+def served_measure(args, device: int, world: int, rank: int, smem_bw: float | None = None) -> dict | None:
     """The served mixed-job stream on one GPU: the same Poisson stream of jobs through (1) the plain path, one
     sqsg_optimize call at a time in arrival order (a FIFO queue in front of the GPU), (2) the continuous-batching
     server (sqsg_server_*), and (3) one offline sqsg_optimize_batch call over all jobs. Host precompute (parsing
     and geometry) is done before the timed region for every arm; job preparation, upload, kernels, result
-    download and selection are inside it."""
+    download and selection are inside it. Returns the result line (rank 0) or None."""
     import torch
 
     import cases as _cases
@@ -447,18 +564,6 @@ def run_served(args):
     from sqsgenerator_b200 import _native as N
     from sqsgenerator_b200.optimize import build_job
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
-    device = local
-    torch.cuda.set_device(device)
     L = N.lib()
     stream = mixed_jobs(args.jobs, seed=2026, rate=args.rate)[rank::world]  # each GPU serves its share
     prepared = []
@@ -470,7 +575,7 @@ def run_served(args):
 
     def plain(items):
         t0 = time.perf_counter()
-        lat, digests = [], []
+        lat, digests, kernel_s, host_s = [], [], 0.0, 0.0
         for arr, c, d, _ in items:
             now = time.perf_counter() - t0
             if now < arr:
@@ -480,8 +585,11 @@ def run_served(args):
             N.check(L.sqsg_optimize(C.byref(job), C.byref(run)))
             lat.append(time.perf_counter() - t0 - arr)
             digests.append(_run_digest(L, N, run, _cases))
+            st = N.run_stages(run)
+            kernel_s += st["kernel"]
+            host_s += st["total"] - st["wait"]
             L.sqsg_run_free(run)
-        return time.perf_counter() - t0, lat, digests
+        return time.perf_counter() - t0, lat, digests, kernel_s, host_s
 
     def served(items):
         srv = S.Server(device)
@@ -539,9 +647,12 @@ def run_served(args):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     with ClockSampler(device) as clk:
-        p_span, p_lat, p_dig = plain(prepared)
-        s_span, s_lat, s_dig, s_stats = served(prepared)
-        b_span, b_dig = batched(prepared)
+        with ClockSampler(device) as clk_p:
+            p_span, p_lat, p_dig, p_kernel, p_host = plain(prepared)
+        with ClockSampler(device) as clk_s:
+            s_span, s_lat, s_dig, s_stats = served(prepared)
+        with ClockSampler(device) as clk_b:
+            b_span, b_dig = batched(prepared)
     configs = sum(x["finished"] for x in p_dig)
     pair_evals = sum(x["finished"] * P for x, (_, _, _, P) in zip(p_dig, prepared))
     same = sum(1 for a, b in zip(p_dig, s_dig) if (a["levels"], a["ids"], a["obj"]) == (b["levels"], b["ids"], b["obj"]))
@@ -563,14 +674,14 @@ def run_served(args):
         n_jobs = len(prepared)
     p_span, s_span, b_span = spans
     if rank != 0:
-        if world > 1:
-            torch.distributed.destroy_process_group()
-        return
-    smem_bw, _ = N.microbench(0, device)
+        return None
+    if smem_bw is None:
+        smem_bw, _ = N.microbench(0, device)
+    cpu = None if args.no_cpu_baseline or world > 1 else cpu_served_sample(prepared, args.cpu_seconds)
     q = lambda v, p: float(np.percentile(np.asarray(v), p)) * 1e3  # noqa: E731
     value = configs / s_span
     achieved = 2 * pair_evals / s_span / 1e9
-    line = {"metric": METRIC, "value": value, "unit": "configs/s", "n_gpus": world, "steps": 1,
+    return {"metric": METRIC, "value": value, "unit": "configs/s", "n_gpus": world, "steps": 1,
             "warmup": args.warmup, "ms_per_step": s_span * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"served mixed-job stream: {n_jobs} jobs, Poisson arrivals at {args.rate}/s "
@@ -579,19 +690,45 @@ def run_served(args):
                        "jobs": n_jobs, "configs": configs, "pair_evaluations": pair_evals,
                        "l2": "not flushed: every job's data is uploaded from host memory inside the timed region"},
             "served": {"configs_per_s": value, "makespan_s": s_span, "p50_ms": q(s_lat, 50), "p99_ms": q(s_lat, 99),
-                       "launches": s_stats["launches"]},
+                       "launches": s_stats["launches"], "gpu_util_mean": clk_s.summary().get("util_mean")},
             "plain": {"configs_per_s": configs / p_span, "makespan_s": p_span, "p50_ms": q(p_lat, 50),
-                      "p99_ms": q(p_lat, 99)},
+                      "p99_ms": q(p_lat, 99), "gpu_util_mean": clk_p.summary().get("util_mean"),
+                      "kernel_s_sum": p_kernel, "host_s_sum": p_host},
             "batched": {"configs_per_s": configs / b_span, "makespan_s": b_span,
+                        "gpu_util_mean": clk_b.summary().get("util_mean"),
                         "note": "one sqsg_optimize_batch call over all jobs, no arrivals"},
+            "served_over_plain": p_span / s_span,
+            "bound": {"kernel_s_sum_alone": p_kernel,
+                      "plain_over_kernel_sum": p_span / p_kernel if p_kernel else None,
+                      "note": "kernel_s_sum_alone is the summed engine-kernel time of the jobs run one at a time; "
+                              "a served makespan cannot fall much below it when large jobs fill the GPU alone, so "
+                              "plain_over_kernel_sum bounds served/plain for this mix"},
             "parity": {"served_identical_to_plain": same, "batched_identical_to_plain": same_b, "jobs": n_jobs},
             "e2e": {"value": value, "unit": "configs/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
             "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
                          "frac": achieved / (smem_bw / 1e9), "traffic": None,
                          "algorithmic": "2*P bytes of shared-memory species reads per configuration, summed over jobs",
                          "peak_source": "measured in this run: conflict-free LDS.32 microbenchmark"},
-            "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": s_stats["launches"]}
-    print(json.dumps(line), flush=True)
+            "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": s_stats["launches"]}
+
+
+def run_served(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    line = served_measure(args, local, world, rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
 
@@ -603,12 +740,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="systematic",
-                    choices=["systematic", "random", "quinary", "split", "served"])
+                    choices=["systematic", "random", "quinary", "split", "split_single", "served"])
     ap.add_argument("--jobs", type=int, default=200, help="served: jobs in the stream")
     ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate, jobs/s")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="only the headline workload (by default the run adds the random, quinary, split and served "
+                         "workloads, once each, on one GPU)")
     ap.add_argument("--limit", type=int, default=0, help="evaluate only the first LIMIT ranks (profiling)")
     ap.add_argument("--max-results", type=int, default=1 << 16,
                     help="record capacity per step; the exact objective levels do not depend on it")
