@@ -189,3 +189,39 @@ def test_structure_bytes_round_trip():
     np.testing.assert_array_equal(back.lattice, s.lattice)
     np.testing.assert_array_equal(back.frac_coords, s.frac_coords)
     assert back.species == s.species and back.pbc == tuple(s.pbc)
+
+
+def _nlohmann_include():
+    import glob
+    import sys as _sys
+
+    for root in {_sys.prefix, os.path.dirname(os.path.dirname(np.__file__))}:
+        for hit in glob.glob(os.path.join(root, "**", "nlohmann", "json.hpp"), recursive=True):
+            return os.path.dirname(os.path.dirname(hit))
+    return None
+
+
+@pytest.mark.parametrize("settings", ["interact_double", "interact_single", "split_double", "split_single"])
+def test_pack_reads_with_nlohmann_from_msgpack(settings, tmp_path):
+    """The bytes of pack.bytes() decode with nlohmann::json::from_msgpack (the call the reference's loader
+    uses, python/extension/sqsgen.cpp:38-56) and read with the reference's keys and value types
+    (tests/pack_reader.cpp follows include/sqsgen/io/json.h:120-287)."""
+    inc = _nlohmann_include()
+    if inc is None:
+        pytest.skip("nlohmann/json.hpp is not installed on this machine")
+    exe = tmp_path / "pack_reader"
+    src = os.path.join(os.path.dirname(__file__), "pack_reader.cpp")
+    import subprocess
+
+    subprocess.run(["g++", "-std=c++20", "-O1", "-I", inc, src, "-o", str(exe)], check=True)
+    mode, prec = settings.split("_")
+    cfg = cases.settings_16(prec) if mode == "interact" else cases.rocksalt_split(prec, iterations=1000)
+    pack = _synthetic_pack(cfg, n=25)
+    path = tmp_path / "pack.msgpack"
+    path.write_bytes(pack.bytes())
+    out = subprocess.run([str(exe), str(path), prec], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    n_results, n_sro = (int(x) for x in out.stdout.split()[1::2])
+    assert n_results == pack.num_results()
+    per = sum(d.prefactors.size for d in S.prepare(pack.config))
+    assert n_sro == n_results * per
