@@ -651,7 +651,7 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
         total = p == 0 ? o : F::add(total, o);
       }
     }
-    if ((it & 15) == 0) thr_g = load_threshold<T>(J);
+    thr_g = load_threshold<T>(J);  // one L2 load per configuration: small next to its pair loop
     const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
     const bool pass = active && static_cast<double>(total) <= bound;
     const uint64_t id = tile.start + my_off + it;
