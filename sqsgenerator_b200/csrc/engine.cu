@@ -362,12 +362,15 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
 
 // Candidate sets at least this large are selected on the device.
 constexpr uint64_t kDeviceSelectMin = 32768;
-// Candidate capacity of a job that leaves max_results at 0 (64 MiB of candidates; a job whose
-// buffer overflows runs again with a buffer sized from its exact level counts).
-constexpr uint64_t kDefaultCandidates = 1u << 22;
-// Device memory a re-run may give a job's candidates when the first pass overflowed (random runs over
-// small configuration spaces revisit configurations and store every visit at or below T*).
-constexpr uint64_t kRerunRecordBytes = 16ull << 30;
+// Candidate capacity of a job that leaves max_results at 0 (16 MiB of candidates; a job whose
+// buffer overflows runs again with a buffer sized from its exact level counts, within rerun_limit).
+constexpr uint64_t kDefaultCandidates = 1u << 20;
+// Size of the full records (rebuilt on the device and copied out) that a re-run may produce when the
+// first pass overflowed its candidate buffer (random runs over small configuration spaces revisit
+// configurations and store every visit at or below T*). A job whose result set is larger keeps the
+// records of its first pass (truncated; the objective levels stay exact).
+constexpr uint64_t kRerunRecordBytes = 4ull << 30;
+static uint64_t rerun_limit(const PreparedJob& pj) { return kRerunRecordBytes / pj.record_bytes; }
 
 static RecordLayout record_layout(const PreparedJob& pj) {
   RecordLayout L;
@@ -760,7 +763,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
         d2h_bytes += n * sizeof(Cand);
       }
       const bool may_rerun = !pjs[j].max_results && pjs[j].passes + attempt < 2;
-      outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, kRerunRecordBytes / sizeof(Cand));
+      outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, rerun_limit(pjs[j]));
       if (outc[j].rerun) {
         capacity[j] = outc[j].rerun_capacity;
         fixed_threshold[j] = true;
@@ -1153,7 +1156,9 @@ static void finalizer_loop(ServerState* Sp) {
     const unsigned long long* cnt = c.cnt.data();
     const uint64_t n = std::min<uint64_t>(cnt[kCandidates], J.capacity);
     const uint64_t arena_records =
-        (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) / sizeof(Cand);
+        std::min<uint64_t>(rerun_limit(J.pj),
+                           (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) /
+                               sizeof(Cand));
     Run r;
     std::string error;
     Outcome o;
