@@ -235,6 +235,8 @@ sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t ca
  *   "stage_wait_ns"      > 0   bound of the device's wait for a job's staged data (default 2e9).
  *   "debug_skip_staging" 0/1   debug: the device expects the staged data but no copy is issued, so
  *                              that the bounded wait runs out and the call returns SQSG_ERR_TIMEOUT.
+ *   "use_tuning"         0/1   1 (default): jobs take the measured launch choices of their bucket
+ *                              (sqsg_autotune, shipped table); 0: the fixed rules.
  * Unknown names give SQSG_ERR_INVALID_ARGUMENT. */
 sqsg_status sqsg_set_option(const char* name, int64_t value);
 sqsg_status sqsg_get_option(const char* name, int64_t* value);
@@ -255,11 +257,34 @@ typedef struct {
   uint32_t record_bytes;  /* bytes per candidate record in device memory */
   char kernel[32];        /* the engine kernel a sqsg_optimize call launches */
   sqsg_part_plan parts[8];
+  uint64_t bucket;        /* the job's bucket in the tuning table (see sqsg_autotune) */
+  int32_t tuned;          /* 1 when the launch follows a measured tuning entry */
+  uint32_t reserved2;
 } sqsg_plan;
 
 /* How sqsg_optimize would run the job: per optimised structure the evaluation path, and the launch
  * shape. Validates the job like sqsg_optimize; needs no device (ctas_per_sm is then 0). */
 sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan);
+
+/* Launch choices of one job bucket (sqsg_autotune). */
+typedef struct {
+  int32_t path;           /* SQSG_PATH_* */
+  int32_t stream_staged;  /* general path: 1 pair stream staged in shared memory, 0 read through L1 */
+  uint32_t ctas_per_sm;   /* CTAs per SM of the launch (0: as many as fit) */
+  uint32_t tile_cap;      /* configurations per thread and tile, at most */
+  double configs_per_s;   /* measured engine rate (kernel time) */
+} sqsg_tuning;
+
+/* Autotuner (no reference counterpart; the reference's only scheduling knob is the chunk size,
+ * include/sqsgen/io/config/combined.h:122-136). Times short prefixes of the job on its device for each
+ * launch choice that applies to it — evaluation path (lattice or pair stream), pair-stream staging,
+ * CTAs per SM, tile size — within about `seconds`, and records the fastest for the job's bucket (its
+ * precision, mode, parts, species, shells, and the powers of two of its sites and pairs). Later jobs of
+ * the same bucket in this process take the recorded choices (option "use_tuning", default 1); the
+ * library also ships a table measured on a B200. Results never depend on the choices. *best: the
+ * chosen; tried (optional, capacity *n_tried, out = count): every choice measured. */
+sqsg_status sqsg_autotune(const sqsg_job* job, double seconds, sqsg_tuning* best, sqsg_tuning* tried,
+                          uint32_t* n_tried);
 
 /* Peak-rate microbenchmarks used as roofline denominators (no reference counterpart).
  * kind 0: shared-memory load bandwidth (bytes/s); kind 1: 32-bit integer lane operations per second. */

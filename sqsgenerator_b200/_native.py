@@ -36,7 +36,7 @@ EXPORTED = (
     "sqsg_optimize_trace", "sqsg_optimize_batch", "sqsg_run_levels", "sqsg_run_info",
     "sqsg_microbench", "sqsg_run_transfer", "sqsg_optimize_levels_noalloc",
     "sqsg_server_create", "sqsg_server_submit", "sqsg_server_wait", "sqsg_server_stats", "sqsg_server_destroy",
-    "sqsg_server_running", "sqsg_set_option", "sqsg_get_option", "sqsg_plan_job", "sqsg_run_stages",
+    "sqsg_server_running", "sqsg_set_option", "sqsg_get_option", "sqsg_plan_job", "sqsg_run_stages", "sqsg_autotune",
 )
 
 PATH_NAMES = {0: "general", 1: "bitmask", 2: "lattice"}
@@ -114,7 +114,13 @@ class SqsgPartPlan(C.Structure):
 
 class SqsgPlan(C.Structure):
     _fields_ = [("n_parts", C.c_uint32), ("smem_bytes", C.c_uint32), ("ctas_per_sm", C.c_uint32),
-                ("record_bytes", C.c_uint32), ("kernel", C.c_char * 32), ("parts", SqsgPartPlan * 8)]
+                ("record_bytes", C.c_uint32), ("kernel", C.c_char * 32), ("parts", SqsgPartPlan * 8),
+                ("bucket", C.c_uint64), ("tuned", C.c_int32), ("reserved2", C.c_uint32)]
+
+
+class SqsgTuning(C.Structure):
+    _fields_ = [("path", C.c_int32), ("stream_staged", C.c_int32), ("ctas_per_sm", C.c_uint32),
+                ("tile_cap", C.c_uint32), ("configs_per_s", C.c_double)]
 
 
 class SqsgServerOptions(C.Structure):
@@ -175,6 +181,8 @@ def lib():
         L.sqsg_run_info.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.sqsg_run_transfer.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
         L.sqsg_run_stages.argtypes = [vp, vp, C.POINTER(u32)]
+        L.sqsg_autotune.argtypes = [C.POINTER(SqsgJob), dbl, C.POINTER(SqsgTuning), C.POINTER(SqsgTuning),
+                                    C.POINTER(u32)]
         L.sqsg_optimize_levels_noalloc.argtypes = [C.POINTER(SqsgJob), vp, C.POINTER(u32), vp, vp, vp,
                                                    C.POINTER(SqsgStatistics), C.c_char_p, C.c_size_t]
         L.sqsg_server_create.argtypes = [C.POINTER(SqsgServerOptions), C.POINTER(vp)]
@@ -250,7 +258,19 @@ def plan(job) -> dict:
                   stream_narrow=bool(p.parts[k].stream_narrow), stream_staged=bool(p.parts[k].stream_staged))
              for k in range(p.n_parts)]
     return dict(kernel=p.kernel.decode(), smem_bytes=int(p.smem_bytes), ctas_per_sm=int(p.ctas_per_sm),
-                record_bytes=int(p.record_bytes), parts=parts)
+                record_bytes=int(p.record_bytes), parts=parts, bucket=int(p.bucket), tuned=bool(p.tuned))
+
+
+def autotune(job, seconds: float = 2.0) -> tuple[dict, list[dict]]:
+    """sqsg_autotune of a native job: (chosen, every choice measured)."""
+    best = SqsgTuning()
+    tried = (SqsgTuning * 64)()
+    n = C.c_uint32(64)
+    check(lib().sqsg_autotune(C.byref(job), float(seconds), C.byref(best), tried, C.byref(n)))
+    conv = lambda t: dict(path=PATH_NAMES.get(t.path, str(t.path)), stream_staged=int(t.stream_staged),  # noqa: E731
+                          ctas_per_sm=int(t.ctas_per_sm), tile_cap=int(t.tile_cap),
+                          configs_per_s=float(t.configs_per_s))
+    return conv(best), [conv(tried[k]) for k in range(min(n.value, 64))]
 
 
 STAGE_NAMES = ("prepare", "upload", "kernel", "wait", "levels", "select", "total")

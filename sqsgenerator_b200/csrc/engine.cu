@@ -39,8 +39,9 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 
 // ------------------------------------------------------------------------------------------------
 // Process-wide options
-static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}};
-static const char* const kOptionNames[kOptCount] = {"force_general", "stage_wait_ns", "debug_skip_staging"};
+static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}, {1}};
+static const char* const kOptionNames[kOptCount] = {"force_general", "stage_wait_ns", "debug_skip_staging",
+                                                    "use_tuning"};
 
 long long option(Option o) { return g_options[o].load(std::memory_order_relaxed); }
 
@@ -193,11 +194,12 @@ static void configure_kernel(size_t smem) {
   }
 }
 
-static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel kernel) {
+static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel kernel, uint32_t ctas = 0) {
   configure_kernel(smem);
   int per_sm = 0;
   CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem));
   if (per_sm <= 0) throw unsupported_error("the job needs more shared memory than one SM offers");
+  if (ctas > 0) per_sm = std::min<int>(per_sm, static_cast<int>(ctas));
   size_t grid = static_cast<size_t>(per_sm) * device_sm_count(dev);
   return static_cast<uint32_t>(std::max<size_t>(1, std::min(grid, n_tiles)));
 }
@@ -594,7 +596,8 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     }
   }
   std::vector<Tile> tiles;
-  for (size_t j = 0; j < nj; ++j) make_tiles(pjs[j], static_cast<uint32_t>(j), tiles);
+  for (size_t j = 0; j < nj; ++j)
+    make_tiles(pjs[j], static_cast<uint32_t>(j), tiles, pjs[j].tuning.tile_cap ? pjs[j].tuning.tile_cap : 1u << 16);
 
   const uint64_t t_setup = now_ns();
   float loop_ms_total = 0.f;
@@ -665,7 +668,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       kind = kKindWide;
     }
     const EngineKernel kernel = kernel_of(kind);
-    const uint32_t grid = launch_grid(device, smem, tiles.size(), kernel);
+    const uint32_t grid = launch_grid(device, smem, tiles.size(), kernel, nj == 1 ? pjs[0].tuning.ctas : 0u);
     const uint64_t t_launch = now_ns();
     CUDA_CHECK(cudaEventRecord(ws->ev_start, ws->stream));
     if (!tiles.empty()) {
@@ -1553,6 +1556,9 @@ sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
     plan->n_parts = d.n_parts;
     plan->smem_bytes = d.smem_bytes;
     plan->record_bytes = d.record_bytes;
+    plan->bucket = bucket_key(*job);
+    Tuning t;
+    plan->tuned = option(kOptUseTuning) && tuning_lookup(plan->bucket, t) ? 1 : 0;
     const bool bitmask = d.k2 != 0;
     const int kind = kind_of(d);
     std::snprintf(plan->kernel, sizeof(plan->kernel), "%s", kernel_name(kind));
@@ -1573,6 +1579,101 @@ sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
       }
     } else {
       cudaGetLastError();
+    }
+  });
+}
+
+sqsg_status sqsg_autotune(const sqsg_job* job, double seconds, sqsg_tuning* best, sqsg_tuning* tried,
+                          uint32_t* n_tried) {
+  return guarded([&] {
+    if (!job || !best) throw std::invalid_argument("null pointer");
+    if (!(seconds > 0)) throw std::out_of_range("seconds must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      throw cuda_error("no CUDA device is available (the autotuner measures on the device)");
+    }
+    const int device = job->device;
+    if (device < 0 || device >= ndev) throw std::invalid_argument("invalid device ordinal");
+    CUDA_CHECK(cudaSetDevice(device));
+    sqsg_job probe = *job;
+    probe.callback = nullptr;
+    probe.cancel = nullptr;
+    probe.max_results = 4096;  // the records are not what is timed
+    const Tuning rules{};
+    const PreparedJob base = prepare(probe, 0, &rules);
+    const uint64_t total = base.range_count;
+    if (total == 0) throw std::out_of_range("the job has no configurations to time");
+    // the choices that apply to this job
+    std::vector<std::pair<int, int>> paths;  // (path, stage)
+    if (base.desc.lat) paths.push_back({SQSG_PATH_LATTICE, -1});
+    if (base.desc.k2) paths.push_back({SQSG_PATH_BITMASK, -1});
+    if (!base.desc.k2 && job->n_sublattices == 1) {
+      paths.push_back({SQSG_PATH_GENERAL, 0});
+      paths.push_back({SQSG_PATH_GENERAL, 1});
+    } else if (!base.desc.k2) {
+      paths.push_back({SQSG_PATH_GENERAL, 0});
+    }
+    std::vector<Tuning> cands;
+    std::vector<int> cand_path;
+    for (auto [path, stage] : paths) {
+      Tuning t;
+      t.path = path == SQSG_PATH_GENERAL ? SQSG_PATH_GENERAL : -1;
+      t.stage = stage;
+      const PreparedJob pj = prepare(probe, 0, &t);
+      int per_sm = 0;
+      configure_kernel(pj.desc.smem_bytes);
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_of(kind_of(pj.desc)), kBlock,
+                                                               pj.desc.smem_bytes));
+      if (per_sm <= 0) continue;
+      std::vector<uint32_t> ctas{0u};
+      if (per_sm > 1) ctas.push_back(static_cast<uint32_t>(per_sm - 1));
+      for (uint32_t c : ctas)
+        for (uint32_t cap : {1024u, 8192u, 65536u}) {
+          Tuning x = t;
+          x.ctas = c;
+          x.tile_cap = cap;
+          cands.push_back(x);
+          cand_path.push_back(path);
+        }
+    }
+    auto timed = [&](const Tuning& t, uint64_t count) {
+      probe.range_first = job->range_first;
+      probe.range_count = count;
+      std::vector<PreparedJob> pjs;
+      pjs.push_back(prepare(probe, 0, &t));
+      std::vector<const sqsg_job*> srcs{&probe};
+      std::vector<Run> runs;
+      execute(pjs, srcs, device, runs, nullptr);
+      const double s = static_cast<double>(runs[0].stats.timings_ns[SQSG_TIMING_LOOP]) * 1e-9;
+      return s > 0 ? static_cast<double>(runs[0].stats.finished) / s : 0.0;
+    };
+    // calibration with the rules (the first run also warms up), then equal shares of the budget
+    const uint64_t c0 = std::min<uint64_t>(total, 1u << 22);
+    timed(rules, c0);
+    const double r0 = std::max(1.0, timed(rules, c0));
+    const double share = seconds / (2.0 * std::max<size_t>(1, cands.size()));
+    const uint64_t count = std::min<uint64_t>(total, std::max<uint64_t>(1u << 16, static_cast<uint64_t>(r0 * share)));
+    std::vector<double> rate(cands.size());
+    size_t bi = 0;
+    for (size_t k = 0; k < cands.size(); ++k) {
+      rate[k] = std::max(timed(cands[k], count), timed(cands[k], count));
+      if (rate[k] > rate[bi]) bi = k;
+    }
+    if (cands.empty()) throw unsupported_error("no launch choice fits this job on the device");
+    tuning_store(bucket_key(*job), cands[bi]);
+    auto fill = [&](size_t k, sqsg_tuning& o) {
+      o.path = cand_path[k];
+      o.stream_staged = cands[k].stage;
+      o.ctas_per_sm = cands[k].ctas;
+      o.tile_cap = cands[k].tile_cap;
+      o.configs_per_s = rate[k];
+    };
+    fill(bi, *best);
+    if (n_tried) {
+      const uint32_t cap = tried ? *n_tried : 0;
+      *n_tried = static_cast<uint32_t>(cands.size());
+      for (size_t k = 0; k < cands.size() && k < cap; ++k) fill(k, tried[k]);
     }
   });
 }

@@ -270,8 +270,79 @@ static bool lattice_tables(const sqsg_sublattice& sl, LatticeTables& L) {
   return L.tr.size() < (1u << 24);
 }
 
-PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
+// ------------------------------------------------------------------------------------------------
+// Tuning table
+struct TableEntry {
+  uint64_t key;
+  int path, stage;
+  uint32_t ctas, tile_cap;
+};
+static const TableEntry kShippedTable[] = {
+#include "tuning_table.inc"
+    {0, -1, -1, 0, 0}};
+
+static std::mutex g_tuning_mutex;
+static std::map<uint64_t, Tuning>& tuning_cache() {
+  static auto* m = new std::map<uint64_t, Tuning>();  // never destroyed: used until exit
+  return *m;
+}
+
+static uint32_t ceil_log2(uint64_t v) {
+  uint32_t b = 0;
+  while ((1ull << b) < v && b < 63) ++b;
+  return b;
+}
+
+uint64_t bucket_key(const sqsg_job& job) {
+  uint64_t n = 0, p = 0;
+  uint32_t kmax = 0, smax = 0, hint = 0;
+  for (uint32_t k = 0; k < job.n_sublattices && job.sublattices; ++k) {
+    const sqsg_sublattice& sl = job.sublattices[k];
+    n += sl.n_sites;
+    p += sl.n_pairs;
+    kmax = std::max(kmax, sl.n_species);
+    smax = std::max(smax, sl.n_shells);
+    hint |= sl.lattice ? 1u : 0u;
+  }
+  uint64_t key = static_cast<uint64_t>(job.prec & 1);
+  key = (key << 1) | static_cast<uint64_t>(job.iteration_mode & 1);
+  key = (key << 4) | std::min<uint32_t>(job.n_sublattices, 15);
+  key = (key << 4) | std::min<uint32_t>(kmax, 15);
+  key = (key << 8) | std::min<uint32_t>(smax, 255);
+  key = (key << 6) | ceil_log2(n);
+  key = (key << 6) | ceil_log2(p);
+  key = (key << 1) | hint;
+  return key + 1;  // 0 ends the shipped table
+}
+
+bool tuning_lookup(uint64_t key, Tuning& out) {
+  {
+    std::lock_guard<std::mutex> l(g_tuning_mutex);
+    auto it = tuning_cache().find(key);
+    if (it != tuning_cache().end()) {
+      out = it->second;
+      return true;
+    }
+  }
+  for (const TableEntry& e : kShippedTable)
+    if (e.key == key) {
+      out = Tuning{e.path, e.stage, e.ctas, e.tile_cap};
+      return true;
+    }
+  return false;
+}
+
+void tuning_store(uint64_t key, const Tuning& t) {
+  std::lock_guard<std::mutex> l(g_tuning_mutex);
+  tuning_cache()[key] = t;
+}
+
+PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* tuning) {
   PreparedJob pj;
+  if (tuning)
+    pj.tuning = *tuning;
+  else if (option(kOptUseTuning))
+    tuning_lookup(bucket_key(job), pj.tuning);
   if (job.prec != SQSG_PREC_SINGLE && job.prec != SQSG_PREC_DOUBLE) throw std::invalid_argument("invalid prec");
   if (job.iteration_mode != SQSG_ITERATION_RANDOM && job.iteration_mode != SQSG_ITERATION_SYSTEMATIC)
     throw std::invalid_argument("invalid iteration mode");
@@ -339,7 +410,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
       will_k2 = !pj.systematic || (has0 && has1);
     }
   }
-  job_lat = job_lat && !will_k2;
+  job_lat = job_lat && !will_k2 && pj.tuning.path != SQSG_PATH_GENERAL;
   d.lat = job_lat ? 1u : 0u;
   for (uint32_t p = 0; p < job.n_sublattices; ++p) {
     const sqsg_sublattice& sl = job.sublattices[p];
@@ -476,8 +547,10 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity) {
     const size_t lanes = (static_cast<size_t>((sl.n_sites + 3) / 4) +
                           static_cast<size_t>(sl.n_shells) * sl.n_species * P.hw) * kBlock * 4;
     // the lattice path reads the stream only for traces and rebuilt records: never staged
-    const bool staged = !k2 && !job_lat && job.n_sublattices == 1 &&
-                        ctas_per_sm(job.device, with_stream + lanes) >= ctas_per_sm(job.device, off + lanes);
+    bool staged = !k2 && !job_lat && job.n_sublattices == 1 &&
+                  ctas_per_sm(job.device, with_stream + lanes) >= ctas_per_sm(job.device, off + lanes);
+    if (!k2 && !job_lat && job.n_sublattices == 1 && pj.tuning.stage >= 0)  // a measured choice
+      staged = pj.tuning.stage == 1 && ctas_per_sm(job.device, with_stream + lanes) >= 1;
     P.stream_global = staged ? 0u : 1u;
     P.static_bytes = static_cast<uint32_t>(staged ? with_stream : off);
     P.blob_off = static_cast<uint32_t>(blob_size);

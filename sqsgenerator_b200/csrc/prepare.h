@@ -14,6 +14,24 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // Byte offset of site x in a lane's species column (words of four sites interleaved across lanes).
 inline uint32_t host_site_off(uint32_t x) { return (x >> 2) * (kBlock * 4) + (x & 3); }
 
+// Launch choices of one job. Unset fields follow the fixed rules: the lattice path when the supercell
+// hint holds, the pair stream staged in shared memory unless that costs a CTA per SM, as many CTAs per
+// SM as fit, tiles of at most 65,536 configurations per thread. sqsg_autotune measures the choices
+// for a job's bucket (job shape) and records the fastest; the shipped table holds measured entries.
+struct Tuning {
+  int path = -1;          // -1: rules; SQSG_PATH_GENERAL: the pair stream even when the lattice path applies
+  int stage = -1;         // general path: -1 rules, 0 stream read through L1, 1 staged in shared memory
+  uint32_t ctas = 0;      // CTAs per SM of a single-job launch (0: as many as fit)
+  uint32_t tile_cap = 0;  // configurations per thread and tile, at most (0: 65,536)
+};
+
+// The bucket of a job's shape: precision, mode, parts, largest K and S, log2 of its sites and pairs,
+// and whether it carries a supercell hint.
+uint64_t bucket_key(const sqsg_job& job);
+// The tuning for a bucket: measured in this process (sqsg_autotune), else the shipped table.
+bool tuning_lookup(uint64_t key, Tuning& out);
+void tuning_store(uint64_t key, const Tuning& t);
+
 struct PartMeta {
   uint32_t N, K, S;
 };
@@ -34,6 +52,7 @@ struct PreparedJob {
   uint64_t range_first = 0, range_count = 0;  // share of the configuration space to evaluate
   // a re-run of an overflowed job: record capacity, starting threshold, passes already made
   uint64_t prepare_ns = 0;      // host time of prepare()
+  Tuning tuning;                // launch choices (see Tuning)
   uint64_t rerun_capacity = 0;
   double rerun_threshold = 0.0;
   int passes = 0;
@@ -43,7 +62,8 @@ struct PreparedJob {
 constexpr size_t kMaxJobTiles = 1u << 24;
 
 // Validates the job and lays out its descriptor and blob (trace_capacity > 0: trace layout too).
-PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity);
+// `tuning` (optional) overrides the table lookup for this job.
+PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* tuning = nullptr);
 // Appends the job's tiles (guided sizes, at most max_per_thread configurations per thread).
 void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles, uint64_t max_per_thread = 1u << 16);
 // CTAs of the general-path kernel that fit on one SM of `device` with `dynamic_smem` bytes each.

@@ -18,6 +18,7 @@ enum Option : int {
   kOptForceGeneral = 0,     // 1: every job takes the general pair-stream path
   kOptStageWaitNs = 1,      // bound of the device's staging wait in nanoseconds
   kOptDebugSkipStaging = 2, // debug: issue no staging copy, so that the bounded wait runs out
+  kOptUseTuning = 3,        // 1: jobs take the measured launch choices of their bucket (tuning table)
   kOptCount
 };
 long long option(Option o);

@@ -262,3 +262,20 @@ def test_plan_reports_occupancy_on_the_device():
     assert p["kernel"] == "sqsg_engine_wide" and p["ctas_per_sm"] >= 1
     p = plan_of(cases.fcc32("double"))
     assert p["kernel"] == "sqsg_engine_mask" and p["ctas_per_sm"] >= 1
+
+
+def test_autotune_records_a_choice_and_results_do_not_change():
+    """sqsg_autotune measures the launch choices of a job's bucket and records the fastest; a job of
+    that bucket then follows it (sqsg_plan_job says so), with the same result set as under the rules."""
+    cfg = LATTICE_CASES["fcc32_ternary"]()
+    c = S.parse_config(cfg)
+    d = S.prepare(c)
+    job, bufs = build_job(c, d)
+    with N.options(use_tuning=0):
+        ref = _full_records(cfg)
+        assert not N.plan(job)["tuned"]
+    best, tried = N.autotune(job, 0.5)
+    assert tried and best["configs_per_s"] == max(t["configs_per_s"] for t in tried)
+    assert {t["path"] for t in tried} == {"lattice", "general"}
+    assert N.plan(job)["tuned"]
+    assert _full_records(cfg) == ref

@@ -129,3 +129,15 @@ def test_dynamic_smem_tracker_is_per_device(tmp_path):
                     "-o", str(exe), "-pthread"], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.strip() == "ok", (out.returncode, out.stdout, out.stderr)
+
+
+def test_tuning_option_and_bucket():
+    c, d, (job, bufs) = _job(cases.quinary("double", cells=(4, 4, 4)))
+    p = N.plan(job)
+    assert p["bucket"] > 0 and p["bucket"] == N.plan(job)["bucket"]
+    assert N.get_option("use_tuning") == 1
+    with N.options(use_tuning=0):
+        assert not N.plan(job)["tuned"]
+    # another shape, another bucket
+    c2, d2, (job2, bufs2) = _job(cases.quinary("double", cells=(3, 3, 3)))
+    assert N.plan(job2)["bucket"] != p["bucket"]
