@@ -167,21 +167,6 @@ static int device_sm_count(int dev) {
   return n;
 }
 
-using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, const volatile int32_t*,
-                              unsigned long long*, volatile uint32_t*);
-
-// The general path runs in sqsg_engine_wide (128 registers); a launch whose jobs all take the binary
-// bit-mask path runs in sqsg_engine_mask (96 registers, 5 CTAs per SM).
-// Kernel kinds: each job runs in the kernel that holds its path.
-enum KernelKind : int { kKindMask = 0, kKindWide = 1, kKindLat = 2 };
-static int kind_of(const JobDesc& d) { return d.k2 ? kKindMask : (d.lat ? kKindLat : kKindWide); }
-static EngineKernel kernel_of(int kind) {
-  return kind == kKindMask ? sqsg_engine_mask : (kind == kKindLat ? sqsg_engine_lat : sqsg_engine_wide);
-}
-static const char* kernel_name(int kind) {
-  return kind == kKindMask ? "sqsg_engine_mask" : (kind == kKindLat ? "sqsg_engine_lat" : "sqsg_engine_wide");
-}
-
 // The dynamic shared-memory attribute is per device: it is raised on the current device (every
 // caller has made the job's device current).
 static void configure_kernel(size_t smem) {
@@ -739,10 +724,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     CUDA_CHECK(cudaMemcpy(&status, ws->status.p, sizeof(status), cudaMemcpyDeviceToHost));
     if (status == kErrStageTimeout) throw timeout_error("shared-memory staging wait timed out on the device");
     if (status != 0) throw cuda_error("device error code " + std::to_string(status));
-    for (size_t j = 0; j < nj; ++j)
-      if (cnt[j * kNumCounters + kMismatch])
-        throw cuda_error("internal error: " + std::to_string(cnt[j * kNumCounters + kMismatch]) +
-                         " lattice-path objectives differ from the pair-stream path's");
+    for (size_t j = 0; j < nj; ++j) check_job_counters(cnt.data() + j * kNumCounters);
     // Every job's counters and level table come back; a job whose record buffer overflowed is re-run
     // (see assess) when the caller left the capacity to the library. Records come back only when
     // the level table overflowed (the levels are then rebuilt from them on the host) or the set is
@@ -1167,6 +1149,7 @@ static void finalizer_loop(ServerState* Sp) {
     Outcome o;
     uint64_t fin_d2h = c.records.size() * sizeof(Cand);
     try {
+      check_job_counters(cnt);
       o = assess(J.pj, cnt, c.levels, c.records, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
       if (!o.rerun) {
         r.prec = J.pj.prec;

@@ -1266,8 +1266,13 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
     }
   }
   if constexpr (GENERAL) {
-    dispatch_general<SYS>(sj, smem, ctab, tile, ws);
+    if (!sj.lat || sj.trace) {  // a lattice job's shared memory holds the general layout only in traces
+      dispatch_general<SYS>(sj, smem, ctab, tile, ws);
+      return;
+    }
   }
+  // no path of this kernel fits the job: nothing is evaluated and the job is flagged
+  if (threadIdx.x == 0) atomicMax(&sj.counters[kError], static_cast<unsigned long long>(kErrBadJob));
 }
 
 // Tiles are taken from q with one atomic per tile. A CTA stages a job's read-only data (cubes,

@@ -3,8 +3,11 @@
 #pragma once
 
 #include <cstdint>
+#include <stdexcept>
+#include <string>
 
 #include "engine.cuh"
+#include "sqsg_internal.h"
 
 namespace sqsg {
 
@@ -29,5 +32,32 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksLat)
 __global__ void __launch_bounds__(kBlock)
     sqsg_materialize(const JobDesc* __restrict__ job, const Cand* __restrict__ cands, uint32_t n,
                      uint8_t* __restrict__ out, unsigned long long* bad);
+
+using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, const volatile int32_t*,
+                              unsigned long long*, volatile uint32_t*);
+
+// Kernel kinds: each job runs in the kernel that holds its path. A bit-mask job (k2) runs in
+// sqsg_engine_mask, a lattice job in sqsg_engine_lat, every other job in sqsg_engine_wide (which may
+// also take bit-mask jobs: their columns and pair stream exist too). A job given to a kernel without
+// its path is skipped on the device and flagged kErrBadJob in its counters.
+enum KernelKind : int { kKindMask = 0, kKindWide = 1, kKindLat = 2 };
+inline int kind_of(const JobDesc& d) { return d.k2 ? kKindMask : (d.lat ? kKindLat : kKindWide); }
+inline EngineKernel kernel_of(int kind) {
+  return kind == kKindMask ? sqsg_engine_mask : (kind == kKindLat ? sqsg_engine_lat : sqsg_engine_wide);
+}
+inline const char* kernel_name(int kind) {
+  return kind == kKindMask ? "sqsg_engine_mask" : (kind == kKindLat ? "sqsg_engine_lat" : "sqsg_engine_wide");
+}
+
+// Throws for the device-side errors a job's counters carry: a staging timeout, a job launched in a
+// kernel without its path, and lattice objectives that differ from the pair-stream path's (traces).
+inline void check_job_counters(const unsigned long long* cnt) {
+  if (cnt[kError] == kErrStageTimeout) throw timeout_error("shared-memory staging wait timed out on the device");
+  if (cnt[kError] == kErrBadJob) throw std::logic_error("internal error: a job was launched in a kernel without its path");
+  if (cnt[kError]) throw cuda_error("device error code " + std::to_string(cnt[kError]));
+  if (cnt[kMismatch])
+    throw cuda_error("internal error: " + std::to_string(cnt[kMismatch]) +
+                     " lattice-path objectives differ from the pair-stream path's");
+}
 
 }  // namespace sqsg

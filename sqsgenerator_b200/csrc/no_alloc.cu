@@ -133,7 +133,7 @@ static Err run(const sqsg_job& job, void* stream, uint32_t* n_levels, double* va
   JobDesc d = pj.desc;
   const size_t n_tiles = tiles.size();
   // the kernel sqsg_optimize would launch for this job
-  const auto kernel = d.k2 ? sqsg_engine_mask : sqsg_engine_wide;
+  const EngineKernel kernel = kernel_of(kind_of(d));
   int optin = 0;
   NA_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, job.device), "attribute query");
   cudaFuncAttributes attr{};
@@ -150,55 +150,73 @@ static Err run(const sqsg_job& job, void* stream, uint32_t* n_levels, double* va
   d.counters = reinterpret_cast<unsigned long long*>(dev + kCountersOff);
   d.levels = reinterpret_cast<LevelSlot*>(dev + kLevelsOff);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // the array keeps the previous call's contents: reset counters, queue, status and level table
-  unsigned long long init[kNumCounters] = {0};
-  const double maxv = pj.prec == SQSG_PREC_DOUBLE ? std::numeric_limits<double>::max()
-                                                   : static_cast<double>(std::numeric_limits<float>::max());
-  init[kThreshold] = ord_bits(maxv);
-  init[kBest] = ord_bits(std::numeric_limits<double>::infinity());
-  NA_CUDA(cudaMemcpyAsync(dev + kDescOff, &d, sizeof(d), cudaMemcpyHostToDevice, s), "descriptor upload");
-  NA_CUDA(cudaMemcpyAsync(dev + kCountersOff, init, sizeof(init), cudaMemcpyHostToDevice, s), "counter upload");
-  NA_CUDA(cudaMemsetAsync(dev + kQueueOff, 0, sizeof(QueueCtl), s), "queue reset");
-  NA_CUDA(cudaMemsetAsync(dev + kStatusOff, 0, 8, s), "status reset");
-  NA_CUDA(cudaMemsetAsync(dev + kLevelsOff, 0, kLevelSlots * sizeof(LevelSlot), s), "level reset");
-  if (!pj.blob.empty())
-    NA_CUDA(cudaMemcpyAsync(dev + kBlobOff, pj.blob.data(), pj.blob.size(), cudaMemcpyHostToDevice, s), "blob upload");
-  if (n_tiles)
-    NA_CUDA(cudaMemcpyAsync(dev + kTilesOff, tiles.data(), n_tiles * sizeof(Tile), cudaMemcpyHostToDevice, s),
-            "tile upload");
   int per_sm = 0, sms = 0;
   NA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, d.smem_bytes), "occupancy");
   NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, job.device), "attribute query");
   if (per_sm <= 0) NA_FAIL(SQSG_ERR_UNSUPPORTED, "the job does not fit on one SM");
-  const auto t0 = std::chrono::steady_clock::now();
-  // Once the kernel is launched it uses the shared array until it ends: every return from here on
-  // first waits for the stream, so that the next call never resets the array under a running kernel.
-  struct StreamGuard {
-    cudaStream_t s;
-    bool armed = false;
-    ~StreamGuard() {
-      if (armed) cudaStreamSynchronize(s);
-    }
-  } guard{s};
-  if (n_tiles) {
-    const size_t grid = std::max<size_t>(1, std::min<size_t>(n_tiles, static_cast<size_t>(per_sm) * sms));
-    kernel<<<static_cast<uint32_t>(grid), kBlock, d.smem_bytes, s>>>(
-        reinterpret_cast<const JobDesc*>(dev + kDescOff), reinterpret_cast<const Tile*>(dev + kTilesOff),
-        static_cast<uint32_t>(n_tiles), reinterpret_cast<QueueCtl*>(dev + kQueueOff), nullptr,
-        reinterpret_cast<unsigned long long*>(dev + kStatusOff), nullptr);
-    guard.armed = true;
-    NA_CUDA(cudaGetLastError(), "engine launch failed");
-  }
+  const double maxv = pj.prec == SQSG_PREC_DOUBLE ? std::numeric_limits<double>::max()
+                                                   : static_cast<double>(std::numeric_limits<float>::max());
   static LevelSlot lv[kLevelSlots];  // static: guarded by g_mutex, keeps 96 KiB off the caller's stack
-  unsigned long long cnt[kNumCounters], status = 0;
-  NA_CUDA(cudaMemcpyAsync(lv, dev + kLevelsOff, sizeof(lv), cudaMemcpyDeviceToHost, s), "level download");
-  NA_CUDA(cudaMemcpyAsync(cnt, dev + kCountersOff, sizeof(cnt), cudaMemcpyDeviceToHost, s), "counter download");
-  NA_CUDA(cudaMemcpyAsync(&status, dev + kStatusOff, 8, cudaMemcpyDeviceToHost, s), "status download");
-  NA_CUDA(cudaStreamSynchronize(s), "engine run failed");
-  guard.armed = false;
+  unsigned long long cnt[kNumCounters];
+  // One pass over every tile: the array keeps the previous pass's contents, so counters, queue,
+  // status and level table are reset first; `threshold` is the ordered key the table starts from.
+  auto pass = [&](unsigned long long threshold) -> Err {
+    unsigned long long init[kNumCounters] = {0};
+    init[kThreshold] = threshold;
+    init[kBest] = ord_bits(std::numeric_limits<double>::infinity());
+    NA_CUDA(cudaMemcpyAsync(dev + kDescOff, &d, sizeof(d), cudaMemcpyHostToDevice, s), "descriptor upload");
+    NA_CUDA(cudaMemcpyAsync(dev + kCountersOff, init, sizeof(init), cudaMemcpyHostToDevice, s), "counter upload");
+    NA_CUDA(cudaMemsetAsync(dev + kQueueOff, 0, sizeof(QueueCtl), s), "queue reset");
+    NA_CUDA(cudaMemsetAsync(dev + kStatusOff, 0, 8, s), "status reset");
+    NA_CUDA(cudaMemsetAsync(dev + kLevelsOff, 0, kLevelSlots * sizeof(LevelSlot), s), "level reset");
+    if (!pj.blob.empty())
+      NA_CUDA(cudaMemcpyAsync(dev + kBlobOff, pj.blob.data(), pj.blob.size(), cudaMemcpyHostToDevice, s),
+              "blob upload");
+    if (n_tiles)
+      NA_CUDA(cudaMemcpyAsync(dev + kTilesOff, tiles.data(), n_tiles * sizeof(Tile), cudaMemcpyHostToDevice, s),
+              "tile upload");
+    // Once the kernel is launched it uses the shared array until it ends: every return from here on
+    // first waits for the stream, so that the next pass or call never resets the array under it.
+    struct StreamGuard {
+      cudaStream_t s;
+      bool armed = false;
+      ~StreamGuard() {
+        if (armed) cudaStreamSynchronize(s);
+      }
+    } guard{s};
+    if (n_tiles) {
+      const size_t grid = std::max<size_t>(1, std::min<size_t>(n_tiles, static_cast<size_t>(per_sm) * sms));
+      kernel<<<static_cast<uint32_t>(grid), kBlock, d.smem_bytes, s>>>(
+          reinterpret_cast<const JobDesc*>(dev + kDescOff), reinterpret_cast<const Tile*>(dev + kTilesOff),
+          static_cast<uint32_t>(n_tiles), reinterpret_cast<QueueCtl*>(dev + kQueueOff), nullptr,
+          reinterpret_cast<unsigned long long*>(dev + kStatusOff), nullptr);
+      guard.armed = true;
+      NA_CUDA(cudaGetLastError(), "engine launch failed");
+    }
+    unsigned long long status = 0;
+    NA_CUDA(cudaMemcpyAsync(lv, dev + kLevelsOff, sizeof(lv), cudaMemcpyDeviceToHost, s), "level download");
+    NA_CUDA(cudaMemcpyAsync(cnt, dev + kCountersOff, sizeof(cnt), cudaMemcpyDeviceToHost, s), "counter download");
+    NA_CUDA(cudaMemcpyAsync(&status, dev + kStatusOff, 8, cudaMemcpyDeviceToHost, s), "status download");
+    NA_CUDA(cudaStreamSynchronize(s), "engine run failed");
+    guard.armed = false;
+    if (status == kErrStageTimeout) NA_FAIL(SQSG_ERR_TIMEOUT, "shared-memory staging wait timed out on the device");
+    if (status) NA_FAIL(SQSG_ERR_CUDA, "device error");
+    const sqsg_status cs = guarded([&] { check_job_counters(cnt); });
+    if (cs != SQSG_OK) {
+      char msg[512];
+      sqsg_last_error(msg, sizeof(msg));
+      NA_FAIL(cs, msg);
+    }
+    return ok();
+  };
+  const auto t0 = std::chrono::steady_clock::now();
+  NA_TRY(pass(ord_bits(maxv)));
+  // While the search threshold is still high, the table takes every new objective and can overflow
+  // (small keep+1 against many distinct objectives early on). The final threshold bounds the
+  // (keep+1)-th best distinct objective from above, and the configurations are the same on every
+  // pass, so one more pass from that threshold gives the exact levels.
+  if (cnt[kLevelOverflow]) NA_TRY(pass(cnt[kThreshold]));
   const auto t1 = std::chrono::steady_clock::now();
-  if (status == kErrStageTimeout) NA_FAIL(SQSG_ERR_TIMEOUT, "shared-memory staging wait timed out on the device");
-  if (status) NA_FAIL(SQSG_ERR_CUDA, "device error");
   // the keep+1 smallest objective keys, by insertion into a fixed array (guarded by g_mutex)
   const uint32_t want = static_cast<uint32_t>(job.keep + 1);
   static LevelSlot best[kMaxKeep + 1];
