@@ -298,7 +298,10 @@ sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds)
  * Outputs: the keep+1 best objectives with exact counts and id checksums (*n_levels: in = capacity,
  * out = count) — the values sqsg_run_levels gives for the same job — and, of the statistics, finished,
  * best_objective and the total/loop timings; best_rank is set to UINT64_MAX (not reported: no
- * configuration records are kept). Limits: staged job data <= 3 MiB, <= 16448 tiles; no callback or
+ * configuration records are kept). A job with more distinct objectives than the 4096-slot level table
+ * takes before the search threshold settles runs again from a tighter threshold (at most 8 passes;
+ * SQSG_ERR_CAPACITY if the table still overflows); the timings cover every pass.
+ * Limits: staged job data <= 3 MiB, <= 16448 tiles; no callback or
  * cancellation; `stream` may be NULL (legacy default stream). The first call on a device looks up the
  * array's device address, so make it before any stream capture. Calls share the array: each call
  * resets what must start at zero, calls from one process are serialised by a lock, and a call returns

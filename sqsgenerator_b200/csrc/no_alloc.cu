@@ -13,6 +13,7 @@
 // the values sqsg_run_levels reports for the same job — and the run statistics, but no configuration
 // records (those need device buffers sized by the result set).
 //
+// A job whose level table overflows runs again from a tighter threshold (at most kMaxPasses passes).
 // Limits: the staged job data must fit kBlobBytes and the tile list kMaxTiles (errors otherwise);
 // no progress callback and no cancellation.
 
@@ -210,12 +211,32 @@ static Err run(const sqsg_job& job, void* stream, uint32_t* n_levels, double* va
     return ok();
   };
   const auto t0 = std::chrono::steady_clock::now();
-  NA_TRY(pass(ord_bits(maxv)));
-  // While the search threshold is still high, the table takes every new objective and can overflow
-  // (small keep+1 against many distinct objectives early on). The final threshold bounds the
-  // (keep+1)-th best distinct objective from above, and the configurations are the same on every
-  // pass, so one more pass from that threshold gives the exact levels.
-  if (cnt[kLevelOverflow]) NA_TRY(pass(cnt[kThreshold]));
+  // While the search threshold is still high the table takes every new objective, and it overflows
+  // when a job has more distinct objectives than slots before the warps' best lists fill (keep+1
+  // distinct values per warp). Every pass evaluates the same configurations, so a pass that starts
+  // from a threshold at or above the (keep+1)-th best distinct objective yields the exact levels. Two
+  // such bounds come out of an overflowed pass: the final device threshold, and the (keep+1)-th
+  // smallest key the table did take (those keys are objectives of the job). The next pass starts
+  // from the smaller one; each pass keeps about (keep+1)/kLevelSlots of the objectives below the
+  // previous bound, so a few passes suffice.
+  constexpr int kMaxPasses = 8;
+  unsigned long long threshold = ord_bits(maxv);
+  for (int p = 0;; ++p) {
+    NA_TRY(pass(threshold));
+    if (!cnt[kLevelOverflow]) break;
+    if (p + 1 == kMaxPasses) break;  // reported as an overflow below
+    static unsigned long long keys[kLevelSlots];
+    uint32_t nk = 0;
+    for (int k = 0; k < kLevelSlots; ++k)
+      if (lv[k].key) keys[nk++] = lv[k].key;
+    unsigned long long next = cnt[kThreshold];
+    if (nk > job.keep) {
+      std::nth_element(keys, keys + job.keep, keys + nk);
+      next = std::min(next, keys[job.keep]);
+    }
+    if (next >= threshold) break;  // no tighter bound: reported as an overflow below
+    threshold = next;
+  }
   const auto t1 = std::chrono::steady_clock::now();
   // the keep+1 smallest objective keys, by insertion into a fixed array (guarded by g_mutex)
   const uint32_t want = static_cast<uint32_t>(job.keep + 1);
