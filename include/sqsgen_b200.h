@@ -237,6 +237,15 @@ sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t ca
  *                              that the bounded wait runs out and the call returns SQSG_ERR_TIMEOUT.
  *   "use_tuning"         0/1   1 (default): jobs take the measured launch choices of their bucket
  *                              (sqsg_autotune, shipped table); 0: the fixed rules.
+ *   "default_candidates" > 0   candidate capacity (16-byte entries) of a job that leaves max_results
+ *                              at 0 (default 2^20); a job that overflows it runs again (below).
+ *   "rerun_record_bytes" > 0   bytes of full records that the re-run of an overflowed job may produce
+ *                              (default 4 GiB). The re-run stores every evaluation at or below the
+ *                              final (keep+1)-th best objective T*; when those are too many, a random
+ *                              job whose configurations have exact keys (the arrangements of its
+ *                              species multisets number at most 2^40) stores each distinct
+ *                              configuration once, with its smallest id. Otherwise the result set is
+ *                              truncated (sqsg_run_info) and the objective levels stay exact.
  * Unknown names give SQSG_ERR_INVALID_ARGUMENT. */
 sqsg_status sqsg_set_option(const char* name, int64_t value);
 sqsg_status sqsg_get_option(const char* name, int64_t* value);

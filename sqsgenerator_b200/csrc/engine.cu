@@ -39,9 +39,10 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 
 // ------------------------------------------------------------------------------------------------
 // Process-wide options
-static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}, {1}};
+static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}, {1},
+                                                      {1ll << 20}, {4ll << 30}};
 static const char* const kOptionNames[kOptCount] = {"force_general", "stage_wait_ns", "debug_skip_staging",
-                                                    "use_tuning"};
+                                                    "use_tuning", "default_candidates", "rerun_record_bytes"};
 
 long long option(Option o) { return g_options[o].load(std::memory_order_relaxed); }
 
@@ -349,15 +350,18 @@ static void select_results(const PreparedJob& pj, const std::vector<uint8_t>& re
 
 // Candidate sets at least this large are selected on the device.
 constexpr uint64_t kDeviceSelectMin = 32768;
-// Candidate capacity of a job that leaves max_results at 0 (16 MiB of candidates; a job whose
-// buffer overflows runs again with a buffer sized from its exact level counts, within rerun_limit).
-constexpr uint64_t kDefaultCandidates = 1u << 20;
+// Candidate capacity of a job that leaves max_results at 0 (option "default_candidates", 2^20 = 16 MiB
+// of candidates by default; a job whose buffer overflows runs again with a buffer sized from its
+// exact level counts, within rerun_limit).
+static uint64_t default_candidates() { return static_cast<uint64_t>(option(kOptDefaultCandidates)); }
 // Size of the full records (rebuilt on the device and copied out) that a re-run may produce when the
-// first pass overflowed its candidate buffer (random runs over small configuration spaces revisit
-// configurations and store every visit at or below T*). A job whose result set is larger keeps the
-// records of its first pass (truncated; the objective levels stay exact).
-constexpr uint64_t kRerunRecordBytes = 4ull << 30;
-static uint64_t rerun_limit(const PreparedJob& pj) { return kRerunRecordBytes / pj.record_bytes; }
+// first pass overflowed its candidate buffer (option "rerun_record_bytes", 4 GiB by default). Random
+// runs over small configuration spaces revisit configurations; their re-run keeps each distinct one
+// once when its keys are exact. A job whose result set is larger keeps the records of its first pass
+// (truncated; the objective levels stay exact).
+static uint64_t rerun_limit(const PreparedJob& pj) {
+  return static_cast<uint64_t>(option(kOptRerunRecordBytes)) / pj.record_bytes;
+}
 
 static RecordLayout record_layout(const PreparedJob& pj) {
   RecordLayout L;
@@ -385,9 +389,14 @@ static RecordLayout record_layout(const PreparedJob& pj) {
 //  - A record buffer that overflowed asks for a re-run (same tiles, same Philox counters, same
 //    evaluations) whose threshold starts at T* (exact levels: the buffer is sized from their counts)
 //    or at the (keep+1)-th distinct objective of the stored records, an upper bound of T*.
+//  - When the evaluations at or below T* are too many for any buffer but the random job's
+//    configurations have exact keys, the re-run stores each distinct configuration once (with its
+//    smallest id) in a table sized from min(evaluations, arrangements): in random mode repeats make
+//    up most of a small configuration space.
 struct Outcome {
   bool rerun = false;
   uint64_t rerun_capacity = 0;
+  uint64_t rerun_slots = 0;  // > 0: a deduplicating re-run with a table of this many slots
   double rerun_threshold = 0.0;
   bool levels_exact = false;
   double tstar = std::numeric_limits<double>::infinity();
@@ -437,6 +446,16 @@ static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, cons
       o.rerun = true;
       o.rerun_capacity = std::max<uint64_t>(need + 64, 1024);
       o.rerun_threshold = o.tstar;
+    } else if (full && may_rerun && pj.dedup_ok) {
+      const uint64_t distinct = std::min<uint64_t>(need, pj.dedup_space);
+      uint64_t slots = 1024;
+      while (slots < 2 * distinct) slots <<= 1;  // load factor at most 1/2
+      if (distinct + 64 + slots * sizeof(DedupSlot) / sizeof(Cand) <= max_capacity) {
+        o.rerun = true;
+        o.rerun_capacity = std::max<uint64_t>(distinct + 64, 1024);
+        o.rerun_slots = slots;
+        o.rerun_threshold = o.tstar;
+      }
     }
     return o;
   }
@@ -562,7 +581,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
   const size_t smem_limit = max_dynamic_smem(device);
   size_t smem = 0, blob_total = 0;
   std::vector<size_t> blob_off(nj), rec_off(nj);
-  std::vector<uint64_t> capacity(nj);
+  std::vector<uint64_t> capacity(nj), slots(nj, 0);
   std::vector<double> start_threshold(nj, 0.0);
   std::vector<bool> fixed_threshold(nj, false);
   size_t rec_total = 0;
@@ -573,9 +592,10 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     smem = std::max<size_t>(smem, pjs[j].desc.smem_bytes);
     blob_off[j] = blob_total;
     blob_total = align_up(blob_total + pjs[j].blob.size(), 256);
-    capacity[j] = pjs[j].max_results ? pjs[j].max_results : kDefaultCandidates;
+    capacity[j] = pjs[j].max_results ? pjs[j].max_results : default_candidates();
     if (pjs[j].rerun_capacity) {
       capacity[j] = pjs[j].rerun_capacity;
+      slots[j] = pjs[j].rerun_slots;
       fixed_threshold[j] = true;
       start_threshold[j] = pjs[j].rerun_threshold;
     }
@@ -588,9 +608,9 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
   float loop_ms_total = 0.f;
   for (int attempt = 0; attempt < 4; ++attempt) {
     rec_total = 0;
-    for (size_t j = 0; j < nj; ++j) {
+    for (size_t j = 0; j < nj; ++j) {  // candidates, then the distinct-configuration table (if any)
       rec_off[j] = rec_total;
-      rec_total = align_up(rec_total + capacity[j] * sizeof(Cand), 256);
+      rec_total = align_up(align_up(rec_total + capacity[j] * sizeof(Cand), 256) + slots[j] * sizeof(DedupSlot), 256);
     }
     ws->blob.ensure(std::max<size_t>(blob_total, 256));
     ws->records.ensure(std::max<size_t>(rec_total, 256));
@@ -608,6 +628,12 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       d.blob = static_cast<const uint8_t*>(ws->blob.p) + blob_off[j];
       d.records = static_cast<uint8_t*>(ws->records.p) + rec_off[j];
       d.capacity = capacity[j];
+      if (slots[j]) {
+        d.dedup = reinterpret_cast<DedupSlot*>(static_cast<uint8_t*>(ws->records.p) +
+                                               align_up(rec_off[j] + capacity[j] * sizeof(Cand), 256));
+        d.dedup_mask = slots[j] - 1;
+        CUDA_CHECK(cudaMemsetAsync(d.dedup, 0xff, slots[j] * sizeof(DedupSlot), ws->stream));
+      }
       d.counters = counters + j * kNumCounters;
       d.levels = static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots;
       const double maxv = pjs[j].prec == 1 ? std::numeric_limits<double>::max()
@@ -725,6 +751,12 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     if (status == kErrStageTimeout) throw timeout_error("shared-memory staging wait timed out on the device");
     if (status != 0) throw cuda_error("device error code " + std::to_string(status));
     for (size_t j = 0; j < nj; ++j) check_job_counters(cnt.data() + j * kNumCounters);
+    // deduplicating re-runs: the table's distinct configurations become the job's candidates
+    for (size_t j = 0; j < nj; ++j)
+      if (slots[j])
+        cnt[j * kNumCounters + kCandidates] =
+            compact_dedup(ws->select, ws->stream, descs[j].dedup, slots[j],
+                          reinterpret_cast<Cand*>(static_cast<uint8_t*>(ws->records.p) + rec_off[j]), capacity[j]);
     // Every job's counters and level table come back; a job whose record buffer overflowed is re-run
     // (see assess) when the caller left the capacity to the library. Records come back only when
     // the level table overflowed (the levels are then rebuilt from them on the host) or the set is
@@ -751,6 +783,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       outc[j] = assess(pjs[j], cj, lv, recs[j], n, capacity[j], may_rerun, rerun_limit(pjs[j]));
       if (outc[j].rerun) {
         capacity[j] = outc[j].rerun_capacity;
+        slots[j] = outc[j].rerun_slots;
         fixed_threshold[j] = true;
         start_threshold[j] = outc[j].rerun_threshold;
         rerun = true;
@@ -804,6 +837,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
       for (size_t j : again) {
         PreparedJob pj = pjs[j];
         pj.rerun_capacity = capacity[j];
+        pj.rerun_slots = slots[j];
         pj.rerun_threshold = start_threshold[j];
         pj.passes += attempt + 1;
         sub.push_back(std::move(pj));
@@ -878,6 +912,7 @@ struct RingSpec {
 constexpr RingSpec kRingSpec[kBuckets] = {{kKindMask, 5}, {kKindWide, 4}, {kKindWide, 3}, {kKindWide, 2},
                                           {kKindWide, 1}, {kKindLat, 2},  {kKindLat, 1}};
 constexpr int kMaxSm = 256;
+constexpr size_t kOnesBytes = 1u << 20;  // pinned 0xff source of distinct-configuration table resets
 constexpr uint64_t kRingCap = 1u << 20;
 constexpr uint32_t kIdlePolls = 250;          // ~0.5 ms of empty polls before a CTA leaves its ring
 constexpr int kLaunchSlots = 32;              // concurrent launches per ring
@@ -897,6 +932,7 @@ struct ServerJob {
   uint64_t pairs = 0;         // pair evaluations per configuration
   size_t arena_off = 0, arena_bytes = 0, blob_bytes = 0;
   uint64_t capacity = 0;
+  uint64_t slots = 0;         // > 0: deduplicating re-run (distinct-configuration table after the records)
   bool user_capacity = false;
   int attempt = 0;
   bool fixed_threshold = false;
@@ -945,6 +981,7 @@ struct ServerState {
   uint64_t last_partition = 0;
   uint32_t* h_yield = nullptr;  // pinned sources of yield writes
   uint8_t* h_zero = nullptr;    // pinned zeros: level tables are cleared by copy, not by a kernel
+  uint8_t* h_ones = nullptr;    // pinned 0xff bytes (kOnesBytes): empty distinct-configuration tables
   uint32_t* h_done = nullptr;
   uint32_t* d_done = nullptr;
   std::vector<std::unique_ptr<ServerJob>> slots;
@@ -1016,7 +1053,8 @@ static void arena_free(ServerState& S, size_t off, size_t bytes) {
 }
 
 static size_t job_footprint(const ServerJob& J) {
-  return align_up(J.pj.blob.size(), 256) + align_up(J.capacity * sizeof(Cand), 256);
+  return align_up(J.pj.blob.size(), 256) + align_up(J.capacity * sizeof(Cand), 256) +
+         align_up(J.slots * sizeof(DedupSlot), 256);
 }
 
 // Admits the oldest pending job if a slot, ring space and arena memory are free: uploads its data,
@@ -1065,6 +1103,14 @@ static bool try_admit(ServerState& S) {
   CUDA_CHECK(cudaMemcpyAsync(d.counters, init.data(), init.size() * 8, cudaMemcpyHostToDevice, S.copy));
   // copies only: a memset kernel would wait for SMs held by the running persistent kernels
   CUDA_CHECK(cudaMemcpyAsync(d.levels, S.h_zero, kLevelSlots * sizeof(LevelSlot), cudaMemcpyHostToDevice, S.copy));
+  if (J.slots) {  // the distinct-configuration table starts empty (all bits set), also by copies
+    d.dedup = reinterpret_cast<DedupSlot*>(d.records + align_up(J.capacity * sizeof(Cand), 256));
+    d.dedup_mask = J.slots - 1;
+    const size_t bytes = J.slots * sizeof(DedupSlot);
+    for (size_t off = 0; off < bytes; off += kOnesBytes)
+      CUDA_CHECK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(d.dedup) + off, S.h_ones,
+                                 std::min<size_t>(kOnesBytes, bytes - off), cudaMemcpyHostToDevice, S.copy));
+  }
   CUDA_CHECK(cudaMemcpyAsync(S.d_jobs + slot, &d, sizeof(d), cudaMemcpyHostToDevice, S.copy));
   J.dev_desc = d;
   const uint64_t n = J.tiles.size();
@@ -1138,6 +1184,15 @@ static void finalizer_loop(ServerState* Sp) {
     const uint64_t arena_bytes = S.opt.arena_bytes;
     lock.unlock();
     ServerJob& J = *c.job;
+    std::string error;
+    if (J.slots && stream) {  // a deduplicating re-run: its distinct configurations are the candidates
+      try {
+        c.cnt[kCandidates] = compact_dedup(scratch, stream, J.dev_desc.dedup, J.slots,
+                                           reinterpret_cast<Cand*>(S.arena + J.arena_off + J.blob_bytes), J.capacity);
+      } catch (std::exception const& ex) {
+        error = ex.what();
+      }
+    }
     const unsigned long long* cnt = c.cnt.data();
     const uint64_t n = std::min<uint64_t>(cnt[kCandidates], J.capacity);
     const uint64_t arena_records =
@@ -1145,10 +1200,10 @@ static void finalizer_loop(ServerState* Sp) {
                            (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) /
                                sizeof(Cand));
     Run r;
-    std::string error;
     Outcome o;
     uint64_t fin_d2h = c.records.size() * sizeof(Cand);
     try {
+      if (!error.empty()) throw cuda_error(error);
       check_job_counters(cnt);
       o = assess(J.pj, cnt, c.levels, c.records, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
       if (!o.rerun) {
@@ -1191,6 +1246,7 @@ static void finalizer_loop(ServerState* Sp) {
       S.cv_done.notify_all();
     } else if (o.rerun) {
       J.capacity = o.rerun_capacity;
+      J.slots = o.rerun_slots;
       J.fixed_threshold = true;
       J.start_threshold = o.rerun_threshold;
       J.attempt++;
@@ -1516,7 +1572,8 @@ sqsg_status sqsg_set_option(const char* name, int64_t value) {
   return guarded([&] {
     const int k = option_index(name);
     if (k < 0) throw std::invalid_argument(std::string("unknown option: ") + (name ? name : "(null)"));
-    if (k == kOptStageWaitNs && value <= 0) throw std::out_of_range("stage_wait_ns must be positive");
+    if ((k == kOptStageWaitNs || k == kOptDefaultCandidates || k == kOptRerunRecordBytes) && value <= 0)
+      throw std::out_of_range(std::string(kOptionNames[k]) + " must be positive");
     g_options[k].store(value);
   });
 }
@@ -1802,6 +1859,8 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_yield), kBuckets * sizeof(uint32_t), cudaHostAllocDefault));
     CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_zero), kLevelSlots * sizeof(LevelSlot), cudaHostAllocDefault));
     std::memset(S.h_zero, 0, kLevelSlots * sizeof(LevelSlot));
+    CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&S.h_ones), kOnesBytes, cudaHostAllocDefault));
+    std::memset(S.h_ones, 0xff, kOnesBytes);
     CUDA_CHECK(cudaDeviceGetAttribute(&S.n_sm, cudaDevAttrMultiProcessorCount, S.device));
     if (S.n_sm > kMaxSm || S.n_sm <= kReservedSm) throw unsupported_error("unsupported SM count for the server");
     CUDA_CHECK(cudaMalloc(&S.d_owner, kMaxSm));
@@ -2013,6 +2072,7 @@ sqsg_status sqsg_server_destroy(sqsg_server* server) {
   if (S.h_ctl) cudaFreeHost(S.h_ctl);
   if (S.h_yield) cudaFreeHost(S.h_yield);
   if (S.h_zero) cudaFreeHost(S.h_zero);
+  if (S.h_ones) cudaFreeHost(S.h_ones);
   if (S.d_owner) cudaFree(S.d_owner);
   if (S.h_owner) cudaFreeHost(S.h_owner);
   if (S.h_done) cudaFreeHost(S.h_done);

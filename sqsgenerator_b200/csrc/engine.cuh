@@ -91,6 +91,19 @@ struct Cand {
   unsigned long long id;
 };
 
+// Distinct-configuration table of a random-mode re-run (JobDesc.dedup_slots > 0): open addressing on
+// an exact configuration key (the multiset-permutation rank of the species, or the species bit mask
+// of a binary bit-mask job), holding the smallest configuration id that produced the key and its
+// objective. Empty slots have key == kDedupEmpty and id == ~0.
+struct DedupSlot {
+  unsigned long long key;
+  unsigned long long id;
+  double objective;
+};
+constexpr unsigned long long kDedupEmpty = ~0ull;
+constexpr int kDedupProbes = 4096;
+constexpr unsigned long long kDedupMaxSpace = 1ull << 40;  // rank arithmetic stays inside 64 bits
+
 // One distinct objective value seen at or below the search threshold, with the number of
 // evaluations that produced it and two order-independent 32-bit sums of hashes of their ids.
 struct LevelSlot {
@@ -145,6 +158,11 @@ struct PartDesc {
   uint32_t lat_deg_off;   // staged: u32 shell-s neighbours of each unit-cell site, S x m
   uint32_t lat_planes_off;// shared-memory-only: per lane m x (K-1) one-hot planes (u64, interleaved by lane)
   unsigned long long lat_full;  // the cells' bits
+  // configuration keys of a deduplicating re-run: species counts of the part (all its sites), the
+  // number of their distinct arrangements, and the product of the earlier parts' numbers
+  uint32_t dd_counts[kMaxSpecies];
+  unsigned long long dd_space;
+  unsigned long long dd_stride;
 };
 
 // A translation of the cell grid (bit c = x + A*(y + B*z)) by (dx, dy, dz), as rotations inside rows
@@ -186,6 +204,8 @@ struct JobDesc {
   uint64_t wait_ns;       // bound of the staging wait (%globaltimer nanoseconds)
   uint32_t debug;         // DebugFlag bits
   uint32_t reserved_dbg;
+  DedupSlot* dedup;       // random-mode re-run: distinct-configuration table (null: candidates are appended)
+  uint64_t dedup_mask;    // table slots - 1 (a power of two)
   PartDesc parts[kMaxParts];
 };
 

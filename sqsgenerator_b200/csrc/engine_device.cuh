@@ -492,9 +492,54 @@ __device__ __forceinline__ void write_trace(const JobDesc& J, uint8_t* smem, uin
 
 // ACC (bit-mask path): kept configurations go to the warp's level accumulators while the list is
 // unchanged; otherwise (and always with a shared-memory list) straight to the CTA table.
-template <class T, bool ACC = false>
+// ------------------------------------------------------------------------------ distinct configurations
+// Exact key of the lane's configuration: per part, the rank of its species arrangement among all
+// arrangements of the part's multiset (sites in order; arrangements that put a smaller species at the
+// first differing site rank lower), combined over the parts in mixed radix. The host only enables
+// keys when the product of the parts' arrangement counts is at most kDedupMaxSpace, so every
+// intermediate M * c below stays under 2^48. The division M * c / n is exact: it is the number of
+// arrangements of the remaining sites that start with species c's index.
+static __device__ __noinline__ unsigned long long column_key(uint8_t* smem, const JobDesc& J, int t) {
+  unsigned long long key = 0ull;
+  for (uint32_t p = 0; p < J.n_parts; ++p) {
+    const PartDesc& P = J.parts[p];
+    const uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
+    uint32_t c[kMaxSpecies];
+    for (uint32_t k = 0; k < kMaxSpecies; ++k) c[k] = P.dd_counts[k];
+    unsigned long long M = P.dd_space, r = 0ull;
+    uint32_t n = P.n_sites;
+    for (uint32_t x = 0; x < P.n_sites; ++x, --n) {
+      const uint32_t sp = col[site_off(x)] >> 3;
+      for (uint32_t k = 0; k < sp; ++k) r += M * c[k] / n;
+      M = M * c[sp] / n;
+      --c[sp];
+    }
+    key += r * P.dd_stride;
+  }
+  return key;
+}
+
+// Records (key, id, objective) in the job's distinct-configuration table: the first lane to bring a
+// key claims a slot, and every lane with that key lowers the slot's id to the smallest. A key that
+// finds no slot within kDedupProbes marks the record set incomplete (counters[kRecordsFull]).
+static __device__ __noinline__ void dedup_insert(const JobDesc& J, unsigned long long key, unsigned long long id,
+                                                 double objective) {
+  unsigned long long h = mix64(key) & J.dedup_mask;
+  for (int probe = 0; probe < kDedupProbes; ++probe, h = (h + 1) & J.dedup_mask) {
+    DedupSlot& slot = J.dedup[h];
+    const unsigned long long prev = atomicCAS(&slot.key, kDedupEmpty, key);
+    if (prev == kDedupEmpty || prev == key) {
+      atomicMin(&slot.id, id);
+      slot.objective = objective;  // the same value from every lane with this key
+      return;
+    }
+  }
+  J.counters[kRecordsFull] = 1ull;
+}
+
+template <class T, bool ACC = false, class KeyF>
 __device__ __forceinline__ void handle_candidates(const JobDesc& J, LevelSlot* ctab, WarpState& ws, bool pass, T total,
-                                                  T thr_g, uint64_t id, int t) {
+                                                  T thr_g, uint64_t id, int t, const KeyF& keyf) {
   const int lane = t & 31;
   unsigned m = __ballot_sync(0xffffffffu, pass);
   if (!m) return;
@@ -581,6 +626,10 @@ __device__ __forceinline__ void handle_candidates(const JobDesc& J, LevelSlot* c
       pending &= ~gm;
     }
   }
+  if (J.dedup) {  // a deduplicating re-run: each distinct configuration once, with its smallest id
+    if (keep_it) dedup_insert(J, keyf(), id, v_mine);
+    return;
+  }
   // Once the record buffer is full, appends stop (the level table stays exact) and the contended
   // candidate counter is left alone.
   unsigned long long base = 0;
@@ -655,7 +704,7 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
     const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
     const bool pass = active && static_cast<double>(total) <= bound;
     const uint64_t id = tile.start + my_off + it;
-    handle_candidates<T>(J, ctab, ws, pass, total, thr_g, id, t);
+    handle_candidates<T>(J, ctab, ws, pass, total, thr_g, id, t, [&] { return column_key(smem, J, t); });
     if (J.trace && active) write_trace<T>(J, smem, id - J.trace_base, total, id, t);
     if (systematic && active && it + 1 < my_count)
       next_permutation(part_base(smem, J.parts[0]) + J.parts[0].col_off + 4 * t, wlo, wn);
@@ -897,7 +946,8 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
     const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
     const bool pass = active && static_cast<double>(total) <= bound;
     const uint64_t id = tile.start + my_off + it;
-    handle_candidates<T, true>(J, ctab, ws, pass, total, thr_g, id, t);
+    handle_candidates<T, true>(J, ctab, ws, pass, total, thr_g, id, t,
+                               [&] { return static_cast<unsigned long long>(v); });
     if (J.trace && active) {
       k2_materialize<V, W>(smem, P, t, v);
       write_trace<T>(J, smem, id - J.trace_base, total, id, t);
@@ -1157,7 +1207,7 @@ __device__ __forceinline__ void run_tile_lat(const JobDesc& J, uint8_t* smem, Le
     const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
     const bool pass = active && static_cast<double>(total) <= bound;
     const uint64_t id = tile.start + my_off + it;
-    handle_candidates<T>(J, ctab, ws, pass, total, thr_g, id, t);
+    handle_candidates<T>(J, ctab, ws, pass, total, thr_g, id, t, [&] { return column_key(smem, J, t); });
     if (J.trace && active) write_trace<T>(J, smem, id - J.trace_base, total, id, t);
     if (SYS && active && it + 1 < my_count)
       next_permutation(part_base(smem, J.parts[0]) + J.parts[0].col_off + 4 * t, wlo, wn);

@@ -586,6 +586,33 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       d.k2 = sl.n_sites <= 32 ? 1 : 2;
   }
   if (!pj.systematic) pj.total = job.iterations;
+  // Random mode: exact configuration keys for a deduplicating re-run (see column_key), when the
+  // product of the parts' arrangement counts stays within kDedupMaxSpace.
+  if (!pj.systematic && trace_capacity == 0) {
+    unsigned __int128 prod = 1;
+    bool ok = true;
+    for (uint32_t p = 0; p < job.n_sublattices && ok; ++p) {
+      const sqsg_sublattice& sl = job.sublattices[p];
+      PartDesc& P = d.parts[p];
+      uint32_t counts[kMaxSpecies] = {};
+      for (uint32_t x = 0; x < sl.n_sites; ++x) counts[sl.species[x]]++;
+      unsigned __int128 m = 1;  // multinomial(n; counts) as a product of binomials, exact at every step
+      uint64_t seen = 0;
+      for (uint32_t k = 0; k < sl.n_species && ok; ++k)
+        for (uint32_t i = 1; i <= counts[k] && ok; ++i) {
+          m = m * (++seen) / i;
+          ok = m <= kDedupMaxSpace;
+        }
+      if (!ok) break;
+      for (uint32_t k = 0; k < kMaxSpecies; ++k) P.dd_counts[k] = counts[k];
+      P.dd_space = static_cast<unsigned long long>(m);
+      P.dd_stride = static_cast<unsigned long long>(prod);
+      prod *= m;
+      ok = prod <= kDedupMaxSpace;
+    }
+    pj.dedup_ok = ok;
+    pj.dedup_space = ok ? static_cast<uint64_t>(prod) : 0;
+  }
   d.total = pj.total;
   if (job.range_first > pj.total) throw std::out_of_range("range_first beyond the configuration space");
   pj.range_first = job.range_first;

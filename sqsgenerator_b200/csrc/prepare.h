@@ -55,7 +55,12 @@ struct PreparedJob {
   Tuning tuning;                // launch choices (see Tuning)
   uint64_t rerun_capacity = 0;
   double rerun_threshold = 0.0;
+  uint64_t rerun_slots = 0;     // > 0: the re-run collects distinct configurations in a table of this size
   int passes = 0;
+  // random mode: configurations have exact keys (the parts' arrangement counts multiply to at most
+  // kDedupMaxSpace = dedup_space), so a re-run may deduplicate on the device
+  bool dedup_ok = false;
+  uint64_t dedup_space = 0;
 };
 
 // A job may have at most this many tiles (about 1.4e14 configurations at full-size tiles).

@@ -324,6 +324,40 @@ uint64_t materialize(SelectScratch& S, cudaStream_t st, const Materializer& mat,
   return bad;
 }
 
+namespace {
+
+__global__ void k_compact_dedup(const DedupSlot* __restrict__ tab, uint64_t slots, Cand* __restrict__ out, uint64_t cap,
+                                unsigned long long* __restrict__ count) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < slots;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const DedupSlot e = tab[i];
+    if (e.key == kDedupEmpty) continue;
+    const unsigned long long k = atomicAdd(count, 1ull);
+    if (k < cap) out[k] = Cand{e.objective, e.id};
+  }
+}
+
+}  // namespace
+
+uint64_t compact_dedup(SelectScratch& S, cudaStream_t st, const DedupSlot* table, uint64_t slots, Cand* out,
+                       uint64_t cap) {
+  if (S.stream != st) {
+    S.release();
+    S.stream = st;
+  }
+  auto* count = static_cast<unsigned long long*>(S.get(20, 8));
+  SEL_CHECK(cudaMemsetAsync(count, 0, 8, st));
+  const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(blocks(slots, 256), 148u * 16u));
+  if (slots) {
+    k_compact_dedup<<<grid, 256, 0, st>>>(table, slots, out, cap, count);
+    SEL_CHECK(cudaGetLastError());
+  }
+  unsigned long long n = 0;
+  SEL_CHECK(cudaMemcpyAsync(&n, count, 8, cudaMemcpyDeviceToHost, st));
+  SEL_CHECK(cudaStreamSynchronize(st));
+  return n;
+}
+
 bool select_on_device(SelectScratch& S, cudaStream_t st, const RecordLayout& lay, const Cand* d_cands, uint64_t n64,
                       const std::vector<double>& levels, bool dedup, int64_t max_per_objective, uint64_t id_limit,
                       const Materializer& mat, SelectedSet& out) {

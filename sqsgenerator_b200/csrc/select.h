@@ -68,7 +68,7 @@ struct SelectedSet {
 
 // Grow-only device scratch for select_on_device, bound to the stream it was last used on.
 struct SelectScratch {
-  static constexpr int kSlots = 20;
+  static constexpr int kSlots = 21;
   void* buf[kSlots] = {};
   size_t size[kSlots] = {};
   cudaStream_t stream = nullptr;
@@ -91,6 +91,12 @@ struct Materializer {
 // after waiting for the stream. Scratch slots 16 and 17 of S hold the descriptor and the counter.
 uint64_t materialize(SelectScratch& S, cudaStream_t stream, const Materializer& mat, const Cand* d_cands, uint32_t m,
                      uint8_t* d_out);
+
+// Gathers the occupied slots of a distinct-configuration table (a deduplicating re-run) into
+// candidates at `out` (at most cap, in no particular order) and returns how many slots were occupied,
+// after waiting for the stream. Scratch slot 20 of S holds the counter.
+uint64_t compact_dedup(SelectScratch& S, cudaStream_t stream, const DedupSlot* table, uint64_t slots, Cand* out,
+                       uint64_t cap);
 
 // Selects, from n device-resident candidates, those whose objective equals one of `levels` (the
 // keep+1 smallest distinct objectives, exact), orders them by (objective, id), rebuilds their full

@@ -19,6 +19,8 @@ enum Option : int {
   kOptStageWaitNs = 1,      // bound of the device's staging wait in nanoseconds
   kOptDebugSkipStaging = 2, // debug: issue no staging copy, so that the bounded wait runs out
   kOptUseTuning = 3,        // 1: jobs take the measured launch choices of their bucket (tuning table)
+  kOptDefaultCandidates = 4,  // candidate capacity of a job that leaves max_results at 0
+  kOptRerunRecordBytes = 5,   // bytes of full records a re-run of an overflowed job may produce
   kOptCount
 };
 long long option(Option o);

@@ -141,3 +141,15 @@ def test_tuning_option_and_bucket():
     # another shape, another bucket
     c2, d2, (job2, bufs2) = _job(cases.quinary("double", cells=(3, 3, 3)))
     assert N.plan(job2)["bucket"] != p["bucket"]
+
+
+def test_candidate_budget_options():
+    assert N.get_option("default_candidates") == 1 << 20
+    assert N.get_option("rerun_record_bytes") == 4 << 30
+    with N.options(default_candidates=4096, rerun_record_bytes=1 << 24):
+        assert N.get_option("default_candidates") == 4096
+        assert N.get_option("rerun_record_bytes") == 1 << 24
+    assert N.get_option("default_candidates") == 1 << 20
+    for name in ("default_candidates", "rerun_record_bytes"):
+        with pytest.raises(N.NativeError):
+            N.set_option(name, 0)
