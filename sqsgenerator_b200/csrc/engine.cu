@@ -171,9 +171,8 @@ static int device_sm_count(int dev) {
 // The dynamic shared-memory attribute is per device: it is raised on the current device (every
 // caller has made the job's device current).
 static void configure_kernel(size_t smem) {
-  for (const void* k : {reinterpret_cast<const void*>(sqsg_engine_wide), reinterpret_cast<const void*>(sqsg_engine_mask),
-                        reinterpret_cast<const void*>(sqsg_engine_lat)}) {
-    const int err = raise_dynamic_smem(k, smem);
+  for (int kind = 0; kind < kKindCount; ++kind) {
+    const int err = raise_dynamic_smem(reinterpret_cast<const void*>(kernel_of(kind)), smem);
     if (err != 0)
       throw cuda_error(std::string("cudaFuncSetAttribute(MaxDynamicSharedMemorySize): ") +
                        cudaGetErrorString(static_cast<cudaError_t>(err)));
@@ -193,11 +192,13 @@ static uint32_t launch_grid(int dev, size_t smem, size_t n_tiles, EngineKernel k
 static size_t max_dynamic_smem(int dev) {
   int v = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes b{}, c{}, l{};
-  CUDA_CHECK(cudaFuncGetAttributes(&b, sqsg_engine_wide));
-  CUDA_CHECK(cudaFuncGetAttributes(&c, sqsg_engine_mask));
-  CUDA_CHECK(cudaFuncGetAttributes(&l, sqsg_engine_lat));
-  return static_cast<size_t>(v) - std::max({b.sharedSizeBytes, c.sharedSizeBytes, l.sharedSizeBytes});
+  size_t stat = 0;
+  for (int kind = 0; kind < kKindCount; ++kind) {
+    cudaFuncAttributes a{};
+    CUDA_CHECK(cudaFuncGetAttributes(&a, kernel_of(kind)));
+    stat = std::max<size_t>(stat, a.sharedSizeBytes);
+  }
+  return static_cast<size_t>(v) - stat;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -675,7 +676,12 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     for (size_t j = 1; j < nj; ++j) {
       const int kj = kind_of(pjs[j].desc);
       if (kj == kind) continue;
-      if (kj == kKindLat || kind == kKindLat) throw std::logic_error("lattice jobs mixed with others in one launch");
+      if (is_lattice_kind(kj) && is_lattice_kind(kind)) {  // the eight-species kernel holds every variant
+        kind = kKindLat;
+        continue;
+      }
+      if (is_lattice_kind(kj) || is_lattice_kind(kind))
+        throw std::logic_error("lattice jobs mixed with others in one launch");
       kind = kKindWide;
     }
     const EngineKernel kernel = kernel_of(kind);
@@ -902,15 +908,18 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
 // result does not depend on what else runs: its tiles and Philox counters depend only on the job.
 // One ring per (kernel, occupancy level): ring 0 runs sqsg_engine_mask at 5 CTAs per SM and takes
 // binary bit-mask jobs; rings 1-4 run sqsg_engine_wide at 4, 3, 2, 1 CTAs per SM; rings 5-6 run
-// sqsg_engine_lat at 2 and 1 CTAs per SM. A job goes to the ring of its kernel with the largest
-// shared-memory size it fits, i.e. the highest occupancy its data allow.
-constexpr int kBuckets = 7;
+// sqsg_engine_lat2 at 4 and 2, rings 7-8 sqsg_engine_lat5 at 3 and 1, rings 9-10 sqsg_engine_lat at 2
+// and 1 CTAs per SM. A job goes to the ring of its kernel with the largest shared-memory size it fits,
+// i.e. the highest occupancy its data allow; a bit-mask job that fits no mask ring may take a wide
+// ring, and a lattice job that fits no ring of its kernel a ring of sqsg_engine_lat.
+constexpr int kBuckets = 11;
 struct RingSpec {
   int kind;  // KernelKind
   int want;  // CTAs per SM
 };
 constexpr RingSpec kRingSpec[kBuckets] = {{kKindMask, 5}, {kKindWide, 4}, {kKindWide, 3}, {kKindWide, 2},
-                                          {kKindWide, 1}, {kKindLat, 2},  {kKindLat, 1}};
+                                          {kKindWide, 1}, {kKindLat2, 4}, {kKindLat2, 2}, {kKindLat5, 3},
+                                          {kKindLat5, 1}, {kKindLat, 2},  {kKindLat, 1}};
 constexpr int kMaxSm = 256;
 constexpr size_t kOnesBytes = 1u << 20;  // pinned 0xff source of distinct-configuration table resets
 constexpr uint64_t kRingCap = 1u << 20;
@@ -1940,9 +1949,11 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
         J->bucket = b;
         break;
       }
-    if (J->bucket < 0 && kind == kKindMask)  // a bit-mask job may run the general path as well
+    // a bit-mask job may run the general path as well, and every lattice job the eight-species kernel
+    const int other = kind == kKindMask ? kKindWide : (is_lattice_kind(kind) ? kKindLat : -1);
+    if (J->bucket < 0 && other >= 0)
       for (int b = 0; b < kBuckets; ++b)
-        if (kRingSpec[b].kind == kKindWide && need <= S.rings[b].smem) {
+        if (kRingSpec[b].kind == other && need <= S.rings[b].smem) {
           J->bucket = b;
           break;
         }

@@ -51,7 +51,9 @@ constexpr int kBlock = 128;       // threads per CTA (each owns one configuratio
 constexpr int kMinBlocks = 5;     // sqsg_engine_mask: CTAs per SM the register budget must allow (<= 102 registers)
 constexpr int kK2MaxShells = 4;   // shells of the binary bit-mask path (per-shell counters in registers)
 constexpr int kMinBlocksWide = 4; // sqsg_engine_wide (general path): 128 registers, no spills in the pair loop
-constexpr int kMinBlocksLat = 2;  // sqsg_engine_lat (lattice path): up to 255 registers, no spills
+constexpr int kMinBlocksLat = 2;   // sqsg_engine_lat (lattice path, up to 8 species): up to 255 registers
+constexpr int kMinBlocksLat2 = 4;  // sqsg_engine_lat2 (lattice path, binary parts): up to 128 registers
+constexpr int kMinBlocksLat5 = 3;  // sqsg_engine_lat5 (lattice path, up to 5 species): up to 168 registers
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
 constexpr int kMaxSpecies = 8;    // K per part handled by the packed-row counter
@@ -147,7 +149,7 @@ struct PartDesc {
   uint32_t k2_nbp_off;    // neighbour masks by bit position: u32 [S][32] (N <= 32) or uint2 [S][64]
   uint32_t k2_zeros;      // 1: count over the zeros (species 0 is the minority), else over the ones
   // lattice path (a supercell whose pairs form whole translation classes, see run_tile_lat)
-  uint32_t lat_km;        // 0: not on the lattice path; else 2, 4 or 8 >= K (unrolled species count)
+  uint32_t lat_km;        // 0: not on the lattice path; else the unrolled species count: K (K <= 5) or 8
   uint32_t lat_basis;     // unit-cell sites m
   uint32_t lat_cells;     // cells A*B*C (<= 64: one 64-bit plane per unit-cell site and species)
   uint32_t lat_chunks;    // ceil(cells / 4)
@@ -185,7 +187,7 @@ struct JobDesc {
   uint32_t big_off;       // keep >= 32: per-warp best lists of big_len doubles at this offset
   uint32_t big_len;       // entries per warp list in shared memory (0: the list is one register per lane)
   uint32_t lat;           // 1: every part takes the lattice path
-  uint32_t lat_pad;
+  uint32_t lat_kmax;      // lattice path: the largest unrolled species count (PartDesc.lat_km) of the parts
   uint32_t trace;         // 1: write every evaluated configuration to the trace buffers
   uint32_t trace_species_stride, trace_bonds_stride;
   uint64_t seed;

@@ -1142,25 +1142,43 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
   return obj;
 }
 
-template <class T>
+// One variant per unrolled species count up to the kernel's KMAX (a kernel holds only the variants
+// it may meet, so that its register budget is that of its largest variant).
+template <class T, int KMAX>
 __device__ __forceinline__ T lat_part(uint8_t* smem, const PartDesc& P, int t) {
-  switch (P.lat_km) {
-    case 2:
-      lat_planes<2>(smem, P, t);
-      return lat_objective<2, T>(smem, P, t);
-    case 4:
+  if (P.lat_km == 2) {
+    lat_planes<2>(smem, P, t);
+    return lat_objective<2, T>(smem, P, t);
+  }
+  if constexpr (KMAX >= 3) {
+    if (P.lat_km == 3) {
+      lat_planes<3>(smem, P, t);
+      return lat_objective<3, T>(smem, P, t);
+    }
+  }
+  if constexpr (KMAX >= 4) {
+    if (P.lat_km == 4) {
       lat_planes<4>(smem, P, t);
       return lat_objective<4, T>(smem, P, t);
-    default:
-      lat_planes<8>(smem, P, t);
-      return lat_objective<8, T>(smem, P, t);
+    }
   }
+  if constexpr (KMAX >= 5) {
+    if (P.lat_km == 5) {
+      lat_planes<5>(smem, P, t);
+      return lat_objective<5, T>(smem, P, t);
+    }
+  }
+  if constexpr (KMAX >= 8) {
+    lat_planes<8>(smem, P, t);
+    return lat_objective<8, T>(smem, P, t);
+  }
+  return T(0);  // not reached: the host launches a job only in a kernel with KMAX >= its lat_kmax
 }
 
 // The general tile loop with lattice counting. In trace mode the pair-stream count runs as well: its
 // ordered bonds go to the trace, and an objective that differs from the lattice path's is counted in
 // counters[kMismatch] (the host reports it as an error).
-template <class T, bool SYS>
+template <class T, bool SYS, int KMAX>
 __device__ __forceinline__ void run_tile_lat(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                              WarpState& ws) {
   using F = FP<T>;
@@ -1191,7 +1209,7 @@ __device__ __forceinline__ void run_tile_lat(const JobDesc& J, uint8_t* smem, Le
           if (it > 0) init_column(smem, P, t);
           shuffle_part(smem, P, t, 0u, tile.start + my_off + it, p, k0, k1);
         }
-        const T o = lat_part<T>(smem, P, t);
+        const T o = lat_part<T, KMAX>(smem, P, t);
         if (J.trace) {
           if (J.kw == 1)
             count_part<1>(smem, J.blob, P, t);
@@ -1273,13 +1291,13 @@ __device__ __forceinline__ void dispatch_mask(const JobDesc& sj, uint8_t* smem, 
   }
 }
 
-template <bool SYS>
+template <bool SYS, int KMAX>
 __device__ __forceinline__ void dispatch_lattice(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                                  WarpState& ws) {
   if (sj.prec == 1)
-    run_tile_lat<double, SYS>(sj, smem, ctab, tile, ws);
+    run_tile_lat<double, SYS, KMAX>(sj, smem, ctab, tile, ws);
   else
-    run_tile_lat<float, SYS>(sj, smem, ctab, tile, ws);
+    run_tile_lat<float, SYS, KMAX>(sj, smem, ctab, tile, ws);
 }
 
 template <bool SYS>
@@ -1300,7 +1318,8 @@ __device__ __forceinline__ void dispatch_general(const JobDesc& sj, uint8_t* sme
 
 // Each kernel holds some of the paths (see kernels.h); the host launches a job only in a kernel that
 // holds its path (a bit-mask job may also run the general path: its columns and stream exist too).
-template <bool SYS, bool GENERAL, bool MASK, bool LAT>
+// LAT: 0 = no lattice path; else the largest unrolled species count the kernel holds (4, 5 or 8).
+template <bool SYS, bool GENERAL, bool MASK, int LAT>
 __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                               WarpState& ws) {
   if constexpr (MASK) {
@@ -1309,9 +1328,9 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
       return;
     }
   }
-  if constexpr (LAT) {
-    if (sj.lat) {
-      dispatch_lattice<SYS>(sj, smem, ctab, tile, ws);
+  if constexpr (LAT > 0) {
+    if (sj.lat && sj.lat_kmax <= static_cast<uint32_t>(LAT)) {
+      dispatch_lattice<SYS, LAT>(sj, smem, ctab, tile, ws);
       return;
     }
   }
@@ -1330,7 +1349,7 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
 // whenever its next tile belongs to another job. In live mode every tile ends with a level flush and
 // a decrement of the job's tile count; the CTA that finishes a job's last tile publishes the job's
 // generation in done[slot] (host-mapped memory).
-template <bool GENERAL, bool MASK, bool LAT>
+template <bool GENERAL, bool MASK, int LAT>
 __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
                                             uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
                                             unsigned long long* status, volatile uint32_t* done) {

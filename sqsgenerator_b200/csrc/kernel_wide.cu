@@ -8,7 +8,7 @@ namespace sqsg {
 __global__ void __launch_bounds__(kBlock, kMinBlocksWide)
     sqsg_engine_wide(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                      const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done) {
-  engine_body<true, false, false>(jobs, tiles, n_tiles, q, cancel, status, done);
+  engine_body<true, false, 0>(jobs, tiles, n_tiles, q, cancel, status, done);
 }
 
 }  // namespace sqsg

@@ -23,10 +23,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksWide)
     sqsg_engine_wide(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                      const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
 
-// sqsg_engine_lat — the lattice path (supercells whose pairs are whole translation classes).
+// The lattice path (supercells whose pairs are whole translation classes), by the largest species
+// count of a job's parts: sqsg_engine_lat2 (binary, 4 CTAs per SM), sqsg_engine_lat5 (at most five,
+// 3 CTAs per SM) and sqsg_engine_lat (at most eight, 2 CTAs per SM).
 __global__ void __launch_bounds__(kBlock, kMinBlocksLat)
     sqsg_engine_lat(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
+__global__ void __launch_bounds__(kBlock, kMinBlocksLat2)
+    sqsg_engine_lat2(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
+__global__ void __launch_bounds__(kBlock, kMinBlocksLat5)
+    sqsg_engine_lat5(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
 
 // Rebuilds the full records (selection order) of n candidates of one job; counts objective mismatches.
 __global__ void __launch_bounds__(kBlock)
@@ -37,16 +45,34 @@ using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, 
                               unsigned long long*, volatile uint32_t*);
 
 // Kernel kinds: each job runs in the kernel that holds its path. A bit-mask job (k2) runs in
-// sqsg_engine_mask, a lattice job in sqsg_engine_lat, every other job in sqsg_engine_wide (which may
-// also take bit-mask jobs: their columns and pair stream exist too). A job given to a kernel without
-// its path is skipped on the device and flagged kErrBadJob in its counters.
-enum KernelKind : int { kKindMask = 0, kKindWide = 1, kKindLat = 2 };
-inline int kind_of(const JobDesc& d) { return d.k2 ? kKindMask : (d.lat ? kKindLat : kKindWide); }
+// sqsg_engine_mask, a lattice job in the lattice kernel of its largest species count (lat_kmax 2, at
+// most 5, at most 8), every other job in sqsg_engine_wide (which may also take bit-mask jobs: their
+// columns and pair stream exist too; sqsg_engine_lat likewise takes every lattice job). A job given to
+// a kernel without its path is skipped on the device and flagged kErrBadJob in its counters.
+enum KernelKind : int { kKindMask = 0, kKindWide = 1, kKindLat = 2, kKindLat2 = 3, kKindLat5 = 4, kKindCount = 5 };
+inline bool is_lattice_kind(int kind) { return kind == kKindLat || kind == kKindLat2 || kind == kKindLat5; }
+inline int kind_of(const JobDesc& d) {
+  if (d.k2) return kKindMask;
+  if (!d.lat) return kKindWide;
+  return d.lat_kmax <= 2 ? kKindLat2 : (d.lat_kmax <= 5 ? kKindLat5 : kKindLat);
+}
 inline EngineKernel kernel_of(int kind) {
-  return kind == kKindMask ? sqsg_engine_mask : (kind == kKindLat ? sqsg_engine_lat : sqsg_engine_wide);
+  switch (kind) {
+    case kKindMask: return sqsg_engine_mask;
+    case kKindLat: return sqsg_engine_lat;
+    case kKindLat2: return sqsg_engine_lat2;
+    case kKindLat5: return sqsg_engine_lat5;
+    default: return sqsg_engine_wide;
+  }
 }
 inline const char* kernel_name(int kind) {
-  return kind == kKindMask ? "sqsg_engine_mask" : (kind == kKindLat ? "sqsg_engine_lat" : "sqsg_engine_wide");
+  switch (kind) {
+    case kKindMask: return "sqsg_engine_mask";
+    case kKindLat: return "sqsg_engine_lat";
+    case kKindLat2: return "sqsg_engine_lat2";
+    case kKindLat5: return "sqsg_engine_lat5";
+    default: return "sqsg_engine_wide";
+  }
 }
 
 // Throws for the device-side errors a job's counters carry: a staging timeout, a job launched in a

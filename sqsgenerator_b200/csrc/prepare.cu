@@ -525,7 +525,8 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
     const LatticeTables& LT = lat[p];
     size_t planes = 0;  // lattice path: per-lane plane bytes
     if (job_lat) {
-      P.lat_km = sl.n_species <= 2 ? 2u : (sl.n_species <= 4 ? 4u : 8u);
+      P.lat_km = sl.n_species <= 5 ? sl.n_species : 8u;
+      d.lat_kmax = std::max(d.lat_kmax, P.lat_km);
       P.lat_basis = LT.m;
       P.lat_cells = LT.cells;
       P.lat_chunks = LT.chunks;

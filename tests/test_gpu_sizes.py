@@ -118,7 +118,20 @@ LATTICE_CASES = {
         lattice=(np.eye(3) * 2.87).tolist(), coords=[[0, 0, 0], [0.5, 0.5, 0.5]], species=[1] * 2,
         supercell=[4, 4, 2]), composition={"Ti": 16, "Al": 16, "Nb": 16, "V": 16},
         shell_weights={"1": 1.0, "2": 0.5, "3": 0.25}, iterations=200000, seed=21, thread_config=1, keep=9),
+    # six and eight species: the eight-species variant of the lattice path (sqsg_engine_lat)
+    "fcc_333_senary": lambda: fcc((3, 3, 3), {"Ti": 18, "Al": 18, "Nb": 18, "V": 18, "Zr": 18, "Hf": 18}, 2,
+                                  iterations=100000, seed=31, keep=5),
+    "bcc_444_octonary": lambda: dict(prec="double", structure=dict(
+        lattice=(np.eye(3) * 2.87).tolist(), coords=[[0, 0, 0], [0.5, 0.5, 0.5]], species=[1] * 2,
+        supercell=[4, 4, 4]), composition={e: 16 for e in ("Ti", "Al", "Nb", "V", "Zr", "Hf", "Ta", "Mo")},
+        shell_weights={"1": 1.0, "2": 0.5}, iterations=100000, seed=32, thread_config=1, keep=4),
 }
+
+# the lattice kernel of each case: binary parts, at most five species, at most eight
+LATTICE_KERNELS = {"config3": "sqsg_engine_lat5", "config4": "sqsg_engine_lat2", "fcc32_ternary": "sqsg_engine_lat5",
+                   "fcc32_systematic_ternary": "sqsg_engine_lat5", "perovskite_333": "sqsg_engine_lat5",
+                   "rocksalt_interact": "sqsg_engine_lat5", "bcc_4x4x2_quaternary": "sqsg_engine_lat5",
+                   "fcc_333_senary": "sqsg_engine_lat", "bcc_444_octonary": "sqsg_engine_lat"}
 
 
 @pytest.mark.parametrize("name", sorted(LATTICE_CASES))
@@ -128,6 +141,7 @@ def test_lattice_and_general_paths_agree(name):
     cfg = LATTICE_CASES[name]()
     plan = plan_of(cfg)
     assert [x["path"] for x in plan["parts"]] == ["lattice"] * len(plan["parts"])
+    assert plan["kernel"] == LATTICE_KERNELS[name]
     a = _full_records(cfg)
     with N.options(force_general=1):
         assert plan_of(cfg)["parts"][0]["path"] == "general"
@@ -135,7 +149,8 @@ def test_lattice_and_general_paths_agree(name):
     assert a[0] > 0 and a == b
 
 
-@pytest.mark.parametrize("name", ["fcc32_ternary", "perovskite_333", "bcc_4x4x2_quaternary", "rocksalt_interact"])
+@pytest.mark.parametrize("name", ["fcc32_ternary", "perovskite_333", "bcc_4x4x2_quaternary", "rocksalt_interact",
+                                  "fcc_333_senary", "bcc_444_octonary"])
 def test_lattice_trace_against_oracle(name):
     cfg = dict(LATTICE_CASES[name]())
     cfg["iterations"] = 4000
@@ -256,7 +271,7 @@ def test_staging_wait_runs_out_and_the_context_stays_usable():
 
 def test_plan_reports_occupancy_on_the_device():
     p = plan_of(config3())
-    assert p["kernel"] == "sqsg_engine_lat" and p["ctas_per_sm"] >= 1
+    assert p["kernel"] == "sqsg_engine_lat5" and p["ctas_per_sm"] >= 1
     with N.options(force_general=1):
         p = plan_of(config3())
     assert p["kernel"] == "sqsg_engine_wide" and p["ctas_per_sm"] >= 1

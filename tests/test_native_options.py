@@ -24,9 +24,9 @@ def test_plan_paths_without_a_device():
     p = plan_of(cases.fcc32("double"))
     assert p["kernel"] == "sqsg_engine_mask" and p["parts"][0]["path"] == "bitmask"
     p = plan_of(cases.quinary("double", cells=(4, 4, 4)))
-    assert p["kernel"] == "sqsg_engine_lat" and p["parts"][0]["path"] == "lattice"
+    assert p["kernel"] == "sqsg_engine_lat5" and p["parts"][0]["path"] == "lattice"
     p = plan_of(cases.rocksalt_split("double", cells=(3, 3, 3)))
-    assert p["kernel"] == "sqsg_engine_lat" and [x["path"] for x in p["parts"]] == ["lattice", "lattice"]
+    assert p["kernel"] == "sqsg_engine_lat2" and [x["path"] for x in p["parts"]] == ["lattice", "lattice"]
     with N.options(force_general=1):
         p = plan_of(cases.quinary("double", cells=(4, 4, 4)))
         assert p["kernel"] == "sqsg_engine_wide" and p["parts"][0]["path"] == "general"
