@@ -386,9 +386,14 @@ def measure(workload: str, steps: int, warmup: int, device: int, world: int, ran
                 finished=sum(o["finished"] for o in out))
 
 
-def roofline_of(res: dict, smem_bw: float, int_rate: float, world: int = 1) -> dict:
-    """Fixed algorithmic work per configuration: 2*P shared-memory species bytes (P pairs), 3*P integer
-    operations; divided by the kernel's CUDA-event time per launch and by the in-run peaks."""
+def roofline_of(res: dict, smem_bw: float, int_rate: float, world: int = 1, popc_rate: float | None = None) -> dict:
+    """Roofline of the dominant kernel, per launch (CUDA-event time) against the peaks measured in this run.
+
+    Pair-stream and bit-mask paths: fixed algorithmic work of 2*P shared-memory species bytes (P pairs)
+    and 3*P integer operations per configuration. Lattice path: it reads no species per pair; its work
+    is one 64-bit AND-popcount per (translation class, species pair a <= b < K-1), i.e. two 32-bit
+    population counts per unit (plan: lattice_units), against the measured popcount rate. The 2*P
+    figure is kept beside it (smem_equiv_frac) to compare the paths on one scale."""
     launch_s = res["loop"] / res["steps"]
     configs_per_launch = res["finished"] / res["steps"] / world
     P = res["P_total"]
@@ -398,16 +403,31 @@ def roofline_of(res: dict, smem_bw: float, int_rate: float, world: int = 1) -> d
     if os.path.exists(prof):
         pj = json.load(open(prof))
         traffic, traffic_case = pj.get("dram_bytes_per_launch"), pj.get("case")
-    return {"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
-            "frac": achieved / (smem_bw / 1e9), "traffic": traffic, "traffic_case": traffic_case,
-            "peak_source": "measured in this run: conflict-free LDS.32 microbenchmark (sqsg_microbench kind 0)",
-            "algorithmic": f"2*P = {2 * P} B of shared-memory species reads per configuration (P = {P} pairs)",
-            "int32_frac": (3 * P * configs_per_launch / launch_s) / int_rate, "int32_peak_ops": int_rate,
-            "kernel": res["plan"]["kernel"], "paths": [p["path"] for p in res["plan"]["parts"]],
-            "ctas_per_sm": res["plan"]["ctas_per_sm"]}
+    common = {"traffic": traffic, "traffic_case": traffic_case,
+              "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu), scaled to this "
+                              "launch's configurations where the capture ran a smaller case (traffic_case)",
+              "int32_frac": (3 * P * configs_per_launch / launch_s) / int_rate, "int32_peak_ops": int_rate,
+              "kernel": res["plan"]["kernel"], "paths": [p["path"] for p in res["plan"]["parts"]],
+              "ctas_per_sm": res["plan"]["ctas_per_sm"]}
+    parts = res["plan"]["parts"]
+    if popc_rate and parts and all(p["path"] == "lattice" for p in parts):
+        units = sum(p["lattice_units"] for p in parts)
+        rate = 2 * units * configs_per_launch / launch_s  # 32-bit popcounts per second
+        return dict({"bound": "popc", "achieved": rate / 1e9, "peak": popc_rate / 1e9, "unit": "Gpopc/s",
+                     "frac": rate / popc_rate,
+                     "peak_source": "measured in this run: independent AND-POPC-ADD chains (sqsg_microbench kind 2)",
+                     "algorithmic": f"2 x {units} 32-bit popcounts per configuration ({units} 64-bit AND-popcount "
+                                    "units: translation classes x species pairs)",
+                     "smem_equiv_frac": achieved / (smem_bw / 1e9)}, **common)
+    return dict({"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
+                 "frac": achieved / (smem_bw / 1e9),
+                 "peak_source": "measured in this run: conflict-free LDS.32 microbenchmark (sqsg_microbench kind 0)",
+                 "algorithmic": f"2*P = {2 * P} B of shared-memory species reads per configuration (P = {P} pairs)"},
+                **common)
 
 
-def extra_line(res: dict, smem_bw: float, int_rate: float, cpu: dict | None, parity: dict | None) -> dict:
+def extra_line(res: dict, smem_bw: float, int_rate: float, cpu: dict | None, parity: dict | None,
+               popc_rate: float | None = None) -> dict:
     last = res["out"][-1]
     return {"workload": res["desc"], "value": res["finished"] / res["loop"], "unit": "configs/s",
             "steps": res["steps"], "ms_per_step": res["loop"] / res["steps"] * 1e3,
@@ -415,7 +435,7 @@ def extra_line(res: dict, smem_bw: float, int_rate: float, cpu: dict | None, par
             "e2e": {"value": res["finished"] / res["wall"], "unit": "configs/s", "h2d_bytes_per_step": last["h2d"],
                     "d2h_bytes_per_step": last["d2h"], "ms_per_step": res["wall"] / res["steps"] * 1e3,
                     "host_stages_s": last["stages"]},
-            "roofline": roofline_of(res, smem_bw, int_rate), "clocks": res["clocks"], "cpu_baseline": cpu,
+            "roofline": roofline_of(res, smem_bw, int_rate, 1, popc_rate), "clocks": res["clocks"], "cpu_baseline": cpu,
             "parity": parity, "results": {"records_per_step": last["results"], "truncated": last["truncated"],
                                           "best_levels": last["levels"][:3]}}
 
@@ -466,8 +486,9 @@ def run_b200(args):
                   "source": "tests/golden/fcc32_systematic_levels.json (the oracle's exhaustive enumeration)"}
     smem_bw, _ = N.microbench(0, device)
     int_rate, _ = N.microbench(1, device)
+    popc_rate, _ = N.microbench(2, device)
     res_w = dict(res, loop=loop, wall=wall, finished=finished)
-    roofline = roofline_of(res_w, smem_bw, int_rate, world)
+    roofline = roofline_of(res_w, smem_bw, int_rate, world, popc_rate)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         n, dt, threads, sample = cpu_sample(args.cpu_seconds, c.keep, args.workload)
@@ -499,7 +520,7 @@ def run_b200(args):
                 cpu_x = {"value": n / dt, "unit": "configs/s", "cores": threads, "kind": "port", "sample": sample}
                 prec = "double" if int(r["config"].prec) == 1 else "single"
                 par = check_records(r["data"], prec, r["out"][-1]["sample"])
-            extras[name] = extra_line(r, smem_bw, int_rate, cpu_x, par)
+            extras[name] = extra_line(r, smem_bw, int_rate, cpu_x, par, popc_rate)
             line["gpu_launches"] += r["steps"] * (1 + 1)  # engine + rebuilt records per step
         import copy
 

@@ -256,7 +256,8 @@ typedef struct {
   int32_t path;           /* SQSG_PATH_* */
   int32_t stream_narrow;  /* general path: 16-bit neighbour offsets (sites <= 512) */
   int32_t stream_staged;  /* general path: pair stream staged in shared memory (0: read through L1) */
-  int32_t reserved;
+  uint32_t lattice_units; /* lattice path: 64-bit AND-popcount units per configuration (translation
+                             classes x species pairs a <= b < K-1); 0 on the other paths */
 } sqsg_part_plan;
 
 typedef struct {
@@ -296,7 +297,9 @@ sqsg_status sqsg_autotune(const sqsg_job* job, double seconds, sqsg_tuning* best
                           uint32_t* n_tried);
 
 /* Peak-rate microbenchmarks used as roofline denominators (no reference counterpart).
- * kind 0: shared-memory load bandwidth (bytes/s); kind 1: 32-bit integer lane operations per second. */
+ * kind 0: shared-memory load bandwidth (bytes/s); kind 1: 32-bit integer lane operations per second;
+ * kind 2: 32-bit population counts per second, each with the logic op and the add that the lattice
+ * path pairs with it. */
 sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds);
 
 /* Allocation-free variant of sqsg_optimize, for callers that cannot allocate device memory (a host

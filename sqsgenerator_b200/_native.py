@@ -109,7 +109,7 @@ class SqsgJob(C.Structure):
 
 class SqsgPartPlan(C.Structure):
     _fields_ = [("path", C.c_int32), ("stream_narrow", C.c_int32), ("stream_staged", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("lattice_units", C.c_uint32)]
 
 
 class SqsgPlan(C.Structure):
@@ -255,7 +255,8 @@ def plan(job) -> dict:
     p = SqsgPlan()
     check(lib().sqsg_plan_job(C.byref(job), C.byref(p)))
     parts = [dict(path=PATH_NAMES.get(p.parts[k].path, str(p.parts[k].path)),
-                  stream_narrow=bool(p.parts[k].stream_narrow), stream_staged=bool(p.parts[k].stream_staged))
+                  stream_narrow=bool(p.parts[k].stream_narrow), stream_staged=bool(p.parts[k].stream_staged),
+                  lattice_units=int(p.parts[k].lattice_units))
              for k in range(p.n_parts)]
     return dict(kernel=p.kernel.decode(), smem_bytes=int(p.smem_bytes), ctas_per_sm=int(p.ctas_per_sm),
                 record_bytes=int(p.record_bytes), parts=parts, bucket=int(p.bucket), tuned=bool(p.tuned))
@@ -399,7 +400,8 @@ def unrank_permutation(conf, rank):
 
 
 def microbench(kind: int, device: int = 0):
-    """(rate, seconds) of the shared-memory (kind 0, bytes/s) or INT32 (kind 1, ops/s) microbenchmark."""
+    """(rate, seconds) of the shared-memory (kind 0, bytes/s), INT32 (kind 1, lane ops/s) or popcount
+    (kind 2, 32-bit popcounts/s) microbenchmark."""
     r = C.c_double()
     t = C.c_double()
     check(lib().sqsg_microbench(kind, device, C.byref(r), C.byref(t)))

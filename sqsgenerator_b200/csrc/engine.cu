@@ -1616,6 +1616,16 @@ sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
       plan->parts[p].path = bitmask ? SQSG_PATH_BITMASK : (d.lat ? SQSG_PATH_LATTICE : SQSG_PATH_GENERAL);
       plan->parts[p].stream_narrow = static_cast<int32_t>(P.stream_narrow);
       plan->parts[p].stream_staged = P.stream_global ? 0 : 1;
+      if (d.lat) {  // classes per shell from the part's shell table (first class, ..., end, pairs)
+        const uint32_t na = P.n_species - 1;
+        uint64_t classes = 0;
+        for (uint32_t sh = 0; sh < P.n_shells; ++sh) {
+          uint32_t e[4];
+          std::memcpy(e, pj.blob.data() + P.blob_off + P.lat_shell_off + 16 * sh, 16);
+          classes += e[2] - e[0];
+        }
+        plan->parts[p].lattice_units = static_cast<uint32_t>(classes * na * (na + 1) / 2);
+      }
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) == cudaSuccess && job->device >= 0 && job->device < ndev) {

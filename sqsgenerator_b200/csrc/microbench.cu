@@ -53,17 +53,36 @@ __global__ void __launch_bounds__(kMbBlock) mb_int_kernel(unsigned* out, unsigne
   if (r == 0x9e3779b9u) out[0] = r;
 }
 
+// Independent population-count chains, eight per thread: per step one logic op, one POPC and one add
+// (the lattice path's AND-popcount-accumulate).
+__global__ void __launch_bounds__(kMbBlock) mb_popc_kernel(unsigned* out, unsigned seed) {
+  unsigned a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed + threadIdx.x * 7u + k;
+  const unsigned m = seed * 0x9e3779b9u;
+  for (int it = 0; it < kMbIters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] += static_cast<unsigned>(__popc(a[k] ^ m));
+  }
+  unsigned r = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r ^= a[k];
+  if (r == 0x9e3779b9u) out[0] = r;
+}
+
 }  // namespace sqsg
 
 using namespace sqsg;
 
 extern "C" {
 
-// kind 0: shared-memory load bandwidth in bytes/s; kind 1: 32-bit integer ops/s (lane operations).
+// kind 0: shared-memory load bandwidth in bytes/s; kind 1: 32-bit integer ops/s (lane operations);
+// kind 2: 32-bit population counts per second (with a logic op and an add each).
 // Also returns the kernel time in seconds.
 sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds) {
   return guarded([&] {
     if (!rate) throw std::invalid_argument("null pointer");
+    if (kind < 0 || kind > 2) throw std::invalid_argument("microbenchmark kind must be 0, 1 or 2");
     if (cudaSetDevice(device) != cudaSuccess) throw cuda_error("cudaSetDevice failed");
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -78,14 +97,17 @@ sqsg_status sqsg_microbench(int kind, int device, double* rate, double* seconds)
       cudaEventRecord(a);
       if (kind == 0)
         mb_smem_kernel<<<grid, kMbBlock>>>(out, 1u + rep);
-      else
+      else if (kind == 1)
         mb_int_kernel<<<grid, kMbBlock>>>(out, 1u + rep);
+      else
+        mb_popc_kernel<<<grid, kMbBlock>>>(out, 1u + rep);
       cudaEventRecord(b);
       cudaEventSynchronize(b);
       float ms = 0;
       cudaEventElapsedTime(&ms, a, b);
       const double threads = static_cast<double>(grid) * kMbBlock;
-      const double work = kind == 0 ? threads * kMbIters * 8 * 4.0 : threads * kMbIters * 8 * 4.0;
+      // bytes (kind 0: 8 loads of 4 bytes), lane ops (kind 1: 4 per chain step), popcounts (kind 2)
+      const double work = threads * kMbIters * 8 * (kind == 2 ? 1.0 : 4.0);
       const double r = work / (ms * 1e-3);
       if (rep > 0 && r > best) {
         best = r;
