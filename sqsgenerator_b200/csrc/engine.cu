@@ -364,6 +364,41 @@ static uint64_t rerun_limit(const PreparedJob& pj) {
   return static_cast<uint64_t>(option(kOptRerunRecordBytes)) / pj.record_bytes;
 }
 
+// Lattice path: 64-bit AND-popcount units per configuration of part p (translation classes from the
+// part's shell table {first class, first self-reverse class, end, pairs} x species pairs a <= b < K-1).
+static uint64_t lattice_units(const PreparedJob& pj, uint32_t p) {
+  const PartDesc& P = pj.desc.parts[p];
+  const uint64_t na = P.n_species - 1;
+  uint64_t classes = 0;
+  for (uint32_t sh = 0; sh < P.n_shells; ++sh) {
+    uint32_t e[4];
+    std::memcpy(e, pj.blob.data() + P.blob_off + P.lat_shell_off + 16 * sh, 16);
+    classes += e[2] - e[0];
+  }
+  return classes * na * (na + 1) / 2;
+}
+
+// Estimated cost of one configuration in pair evaluations of the pair-stream path (its unit of
+// work), from B200 measurements: the pair stream costs one per pair, the lattice path about one per
+// AND-popcount unit, the bit-mask path about an eighth per pair; shuffling and setting up a
+// configuration cost about two per site on every path. The served form sizes tiles and divides the
+// SMs between its rings by it.
+static double config_cost(const PreparedJob& pj) {
+  double cost = 0.0;
+  for (uint32_t p = 0; p < pj.desc.n_parts; ++p) {
+    const PartDesc& P = pj.desc.parts[p];
+    const double sites = static_cast<double>(P.n_sites);
+    const double pairs = static_cast<double>(pj.parts[p].P);
+    if (pj.desc.k2)
+      cost += pairs / 8.0 + sites;
+    else if (pj.desc.lat)
+      cost += static_cast<double>(lattice_units(pj, p)) + 2.0 * sites;
+    else
+      cost += pairs + 2.0 * sites;
+  }
+  return std::max(1.0, cost);
+}
+
 static RecordLayout record_layout(const PreparedJob& pj) {
   RecordLayout L;
   L.record_bytes = static_cast<uint32_t>(pj.record_bytes);
@@ -920,6 +955,13 @@ struct RingSpec {
 constexpr RingSpec kRingSpec[kBuckets] = {{kKindMask, 5}, {kKindWide, 4}, {kKindWide, 3}, {kKindWide, 2},
                                           {kKindWide, 1}, {kKindLat2, 4}, {kKindLat2, 2}, {kKindLat5, 3},
                                           {kKindLat5, 1}, {kKindLat, 2},  {kKindLat, 1}};
+// CTAs per SM of the most occupied ring of a kernel kind.
+static int ring_top_occupancy(int kind) {
+  int top = 1;
+  for (const RingSpec& r : kRingSpec)
+    if (r.kind == kind) top = std::max(top, r.want);
+  return top;
+}
 constexpr int kMaxSm = 256;
 constexpr size_t kOnesBytes = 1u << 20;  // pinned 0xff source of distinct-configuration table resets
 constexpr uint64_t kRingCap = 1u << 20;
@@ -929,7 +971,7 @@ constexpr uint64_t kRepartitionNs = 2000000;  // at most one SM repartition per 
 constexpr uint64_t kRelaunchNs = 1000000;     // at most one top-up launch per ring per ms
 constexpr uint8_t kNoOwner = 0xff;
 constexpr int kReservedSm = 2;                // SMs left to no ring: result selection runs there
-constexpr uint64_t kTilePairs = 1u << 19;     // pair evaluations per thread and tile, at most
+constexpr double kTilePairs = 1u << 19;       // estimated pair evaluations per thread and tile, at most
 
 struct ServerJob {
   uint64_t ticket = 0;
@@ -938,7 +980,7 @@ struct ServerJob {
   PreparedJob pj;
   std::vector<Tile> tiles;
   std::vector<uint64_t> cum;  // cum[k] = configurations in tiles[0, k)
-  uint64_t pairs = 0;         // pair evaluations per configuration
+  double cost = 1.0;          // estimated cost of a configuration in pair evaluations (config_cost)
   size_t arena_off = 0, arena_bytes = 0, blob_bytes = 0;
   uint64_t capacity = 0;
   uint64_t slots = 0;         // > 0: deduplicating re-run (distinct-configuration table after the records)
@@ -1293,7 +1335,9 @@ static void schedule(ServerState& S) {
     if (head >= x->ring_end) continue;
     const uint64_t k0 = head > x->ring_begin ? head - x->ring_begin : 0;
     const double configs = static_cast<double>(x->cum.back() - x->cum[k0]);
-    work[x->bucket] += configs * static_cast<double>(x->pairs) / S.rings[x->bucket].per_sm;
+    // SM-time: the cost is measured at the kernel's highest occupancy; a ring of fewer CTAs per SM
+    // takes proportionally longer per configuration
+    work[x->bucket] += configs * x->cost * ring_top_occupancy(kRingSpec[x->bucket].kind) / S.rings[x->bucket].per_sm;
   }
   for (int b = 0; b < kBuckets; ++b) {
     total += work[b];
@@ -1616,16 +1660,7 @@ sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
       plan->parts[p].path = bitmask ? SQSG_PATH_BITMASK : (d.lat ? SQSG_PATH_LATTICE : SQSG_PATH_GENERAL);
       plan->parts[p].stream_narrow = static_cast<int32_t>(P.stream_narrow);
       plan->parts[p].stream_staged = P.stream_global ? 0 : 1;
-      if (d.lat) {  // classes per shell from the part's shell table (first class, ..., end, pairs)
-        const uint32_t na = P.n_species - 1;
-        uint64_t classes = 0;
-        for (uint32_t sh = 0; sh < P.n_shells; ++sh) {
-          uint32_t e[4];
-          std::memcpy(e, pj.blob.data() + P.blob_off + P.lat_shell_off + 16 * sh, 16);
-          classes += e[2] - e[0];
-        }
-        plan->parts[p].lattice_units = static_cast<uint32_t>(classes * na * (na + 1) / 2);
-      }
+      if (d.lat) plan->parts[p].lattice_units = static_cast<uint32_t>(lattice_units(pj, p));
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) == cudaSuccess && job->device >= 0 && job->device < ndev) {
@@ -1970,8 +2005,8 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
     if (J->bucket < 0) throw unsupported_error("the job needs more shared memory per CTA than this device offers");
     J->user_capacity = job->max_results != 0;
     J->capacity = job->max_results ? job->max_results : S.opt.default_max_results;
-    for (uint32_t p = 0; p < job->n_sublattices; ++p) J->pairs += job->sublattices[p].n_pairs;
-    make_tiles(J->pj, 0, J->tiles, std::max<uint64_t>(1, kTilePairs / std::max<uint64_t>(1, J->pairs)));
+    J->cost = config_cost(J->pj);
+    make_tiles(J->pj, 0, J->tiles, std::max<uint64_t>(1, static_cast<uint64_t>(kTilePairs / J->cost)));
     if (J->tiles.size() > kRingCap) throw unsupported_error("the job has more tiles than the ring holds");
     J->cum.assign(J->tiles.size() + 1, 0);
     for (size_t k = 0; k < J->tiles.size(); ++k) J->cum[k + 1] = J->cum[k] + J->tiles[k].count;

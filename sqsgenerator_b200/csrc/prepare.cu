@@ -581,7 +581,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
     tsp += sl.n_sites;
     P.trace_bonds_off = static_cast<uint32_t>(tbd);
     tbd += skk;
-    pj.parts.push_back(PartMeta{sl.n_sites, sl.n_species, sl.n_shells});
+    pj.parts.push_back(PartMeta{sl.n_sites, sl.n_species, sl.n_shells, sl.n_pairs});
     if (pj.systematic) pj.total = window_permutations(sl, P);
     if (k2 && (!pj.systematic || (P.unrank_k == 2 && P.unrank_rev[0] == 0 && P.unrank_rev[1] == 1)))
       d.k2 = sl.n_sites <= 32 ? 1 : 2;

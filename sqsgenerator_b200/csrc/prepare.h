@@ -34,6 +34,7 @@ void tuning_store(uint64_t key, const Tuning& t);
 
 struct PartMeta {
   uint32_t N, K, S;
+  uint32_t P;  // pairs
 };
 
 struct PreparedJob {

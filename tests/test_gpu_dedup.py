@@ -39,12 +39,16 @@ CASES = {
                     pair_weights=None), 300000, 4, {"force_general": 1}, _multinomial([3, 29])),
     "lattice_fcc32_ternary": lambda: (
         cases.fcc32("double", composition={"Ti": 1, "Al": 30, "Nb": 1}, iterations=150000, seed=23, keep=3),
-        150000, 3, {}, _multinomial([1, 30, 1])),
+        150000, 3, {"use_tuning": 0}, _multinomial([1, 30, 1])),  # the rules' path: lattice
     "split_rocksalt": lambda: (
         cases.rocksalt_split("double", iterations=200000, seed=24, keep=3,
                              composition=[{"sites": "Na", "Ti": 1, "Al": 31}, {"sites": "Cl", "N": 31, "B": 1}]),
-        200000, 3, {}, _multinomial([1, 31]) * _multinomial([31, 1])),
+        200000, 3, {"use_tuning": 0}, _multinomial([1, 31]) * _multinomial([31, 1])),
 }
+
+
+PATH = {"bitmask_fcc32_a3b29": "bitmask", "general_fcc32_a3b29_single": "general", "lattice_fcc32_ternary": "lattice",
+        "split_rocksalt": "lattice"}
 
 
 def _expected(cfg, n, keep):
@@ -100,7 +104,9 @@ def test_dedup_rerun_equals_full_trace(name, form):
     _records.double = int(c.prec) == 1
     with N.options(**opts):
         job, bufs = build_job(c, d)
-        record_bytes = N.plan(job)["record_bytes"]
+        plan = N.plan(job)
+        assert plan["parts"][0]["path"] == PATH[name]
+        record_bytes = plan["record_bytes"]
         with N.options(default_candidates=max(need // 4, 64), rerun_record_bytes=need * record_bytes):
             if form == "plain":
                 run = C.c_void_p()

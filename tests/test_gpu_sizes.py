@@ -65,7 +65,7 @@ def config4(prec="double", iterations=3000):
                                 composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}])
 
 
-PATHS = {"lattice": {}, "general": {"force_general": 1}}
+PATHS = {"lattice": {"use_tuning": 0}, "general": {"force_general": 1}}  # the rules' path, not the table's
 
 
 @pytest.mark.parametrize("path", sorted(PATHS))
@@ -139,10 +139,11 @@ def test_lattice_and_general_paths_agree(name):
     """The same job on the lattice path and on the pair-stream path: the same result set (objectives,
     ids, species, SRO) and the same exact objective levels."""
     cfg = LATTICE_CASES[name]()
-    plan = plan_of(cfg)
-    assert [x["path"] for x in plan["parts"]] == ["lattice"] * len(plan["parts"])
-    assert plan["kernel"] == LATTICE_KERNELS[name]
-    a = _full_records(cfg)
+    with N.options(use_tuning=0):  # the rules' path (the tuning table may prefer the pair stream)
+        plan = plan_of(cfg)
+        assert [x["path"] for x in plan["parts"]] == ["lattice"] * len(plan["parts"])
+        assert plan["kernel"] == LATTICE_KERNELS[name]
+        a = _full_records(cfg)
     with N.options(force_general=1):
         assert plan_of(cfg)["parts"][0]["path"] == "general"
         b = _full_records(cfg)
@@ -154,8 +155,9 @@ def test_lattice_and_general_paths_agree(name):
 def test_lattice_trace_against_oracle(name):
     cfg = dict(LATTICE_CASES[name]())
     cfg["iterations"] = 4000
-    assert plan_of(cfg)["parts"][0]["path"] == "lattice"
-    traced(cfg, 4000, cfg["prec"])
+    with N.options(use_tuning=0):
+        assert plan_of(cfg)["parts"][0]["path"] == "lattice"
+        traced(cfg, 4000, cfg["prec"])
 
 
 def test_narrow_stream_read_through_l1_fcc500():
