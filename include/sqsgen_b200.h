@@ -157,10 +157,11 @@ typedef struct {
   uint32_t n_sublattices;     /* interact: 1 (windows carry the sublattices); split: one per sublattice */
   const sqsg_sublattice* sublattices;
   uint64_t iterations;        /* random: configurations to evaluate; systematic: 0 = all permutations */
-  uint64_t chunk_size;        /* progress-callback granularity in configurations (0: default) */
-  uint64_t keep;              /* the reference's `keep` (1..31 in this build) */
+  uint64_t chunk_size;        /* progress-callback granularity in configurations (0: default); the
+                                 reference's block size in the "rapidrand" debug mode */
+  uint64_t keep;              /* the reference's `keep` (1..1023 in this build) */
   int64_t max_results_per_objective; /* < 0: unset */
-  uint64_t seed;              /* random mode: Philox key */
+  uint64_t seed;              /* random mode: Philox key (rapidrand seed in the "rapidrand" debug mode) */
   int32_t has_seed;           /* 0: a random seed is drawn */
   int32_t device;             /* CUDA device ordinal */
   const volatile int32_t* cancel; /* optional: set non-zero from any thread to stop early */
@@ -246,6 +247,13 @@ sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t ca
  *                              species multisets number at most 2^40) stores each distinct
  *                              configuration once, with its smallest id. Otherwise the result set is
  *                              truncated (sqsg_run_info) and the objective levels stay exact.
+ *   "rapidrand"          0/1   debug (default 0): random jobs follow the reference's seeded
+ *                              single-thread run (core/shuffle.h:23-50 with rapidhash's rapidrand,
+ *                              blocks of chunk_size, sqs.h:348-466) instead of the Philox stream; each
+ *                              block runs as one chain on one GPU thread, so a job has only
+ *                              iterations / chunk_size-way parallelism. Configuration ids are the
+ *                              reference's iteration indices. Pair-stream path only; sqsg_optimize,
+ *                              sqsg_optimize_batch and traces only (not the server, not ranges).
  * Unknown names give SQSG_ERR_INVALID_ARGUMENT. */
 sqsg_status sqsg_set_option(const char* name, int64_t value);
 sqsg_status sqsg_get_option(const char* name, int64_t* value);

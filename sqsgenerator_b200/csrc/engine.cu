@@ -40,9 +40,10 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 // ------------------------------------------------------------------------------------------------
 // Process-wide options
 static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}, {1},
-                                                      {1ll << 20}, {4ll << 30}};
+                                                      {1ll << 20}, {4ll << 30}, {0}};
 static const char* const kOptionNames[kOptCount] = {"force_general", "stage_wait_ns", "debug_skip_staging",
-                                                    "use_tuning", "default_candidates", "rerun_record_bytes"};
+                                                    "use_tuning", "default_candidates", "rerun_record_bytes",
+                                                    "rapidrand"};
 
 long long option(Option o) { return g_options[o].load(std::memory_order_relaxed); }
 
@@ -1985,6 +1986,7 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
     if (job->callback || job->cancel) throw std::invalid_argument("served jobs take no callback or cancel flag");
     auto J = std::make_unique<ServerJob>();
     J->pj = prepare(*job, 0);
+    if (J->pj.chain) throw unsupported_error("the rapidrand debug mode runs through sqsg_optimize, not the server");
     J->t_submit = now_ns();
     const size_t need = J->pj.desc.smem_bytes;
     const int kind = kind_of(J->pj.desc);

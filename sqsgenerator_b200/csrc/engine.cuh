@@ -165,6 +165,9 @@ struct PartDesc {
   uint32_t dd_counts[kMaxSpecies];
   unsigned long long dd_space;
   unsigned long long dd_stride;
+  // reference-stream debug mode: random words one shuffle of the part draws (sum over windows of n_w - 1)
+  uint32_t chain_draws;
+  uint32_t chain_pad;
 };
 
 // A translation of the cell grid (bit c = x + A*(y + B*z)) by (dx, dy, dz), as rotations inside rows
@@ -208,6 +211,11 @@ struct JobDesc {
   uint32_t reserved_dbg;
   DedupSlot* dedup;       // random-mode re-run: distinct-configuration table (null: candidates are appended)
   uint64_t dedup_mask;    // table slots - 1 (a power of two)
+  // Reference-stream debug mode (random mode): configurations follow the reference's seeded
+  // single-thread run, chained within the thread-pool blocks of [0, total) (see run_tile_chain).
+  uint32_t chain;         // 1: this mode
+  uint32_t chain_split;   // 1: split mode (shuffle, then evaluate); 0: interact (evaluate, then shuffle)
+  uint64_t chain_blocks, chain_block, chain_rem;  // blocks, their base length, blocks one longer
   PartDesc parts[kMaxParts];
 };
 
@@ -215,8 +223,8 @@ struct Tile {
   uint32_t job;         // index into the job table (a slot in live mode)
   uint32_t gen;         // live mode: generation of the job occupying the slot
   uint64_t start;       // random: index of the tile's first configuration; systematic: its 1-based rank
-  uint64_t count;       // configurations in the tile
-  uint64_t reserved2;
+  uint64_t count;       // configurations in the tile (reference-stream mode: blocks, one per thread)
+  uint64_t chain_configs;  // reference-stream mode: configurations of the tile's blocks (else unused)
 };
 
 // Queue control block of the persistent kernel, in device memory.

@@ -266,6 +266,49 @@ __device__ __forceinline__ void shuffle_part(uint8_t* smem, const PartDesc& P, i
   }
 }
 
+// ------------------------------------------------------------------------------ reference random stream
+// Debug mode that reproduces the reference's seeded single-thread trajectories. Its random words are
+// rapidrand's (core/shuffle.h:23-26): the state advances by rapidhash's secret 0 per draw and the
+// word is rapidhash's mix of (state, state ^ secret 1), the 64x64->128-bit product folded by xor
+// (core/helpers/rapidhash.h:129-131,149-213); the shuffle uses its low 32 bits (core/shuffle.h:28-32).
+constexpr unsigned long long kRapidSecret0 = 0x2d358dccaa6c78a5ull;
+constexpr unsigned long long kRapidSecret1 = 0x8bb84b93962eacc9ull;
+
+__device__ __forceinline__ uint32_t rapid_next(unsigned long long& s) {
+  s += kRapidSecret0;
+  const unsigned long long b = s ^ kRapidSecret1;
+  return static_cast<uint32_t>((s * b) ^ __umul64hi(s, b));
+}
+
+// core/shuffle.h:39-50 on the reference's stream: Fisher-Yates per window, one word per step.
+__device__ __forceinline__ void shuffle_part_rapid(uint8_t* smem, const PartDesc& P, int t, unsigned long long& s) {
+  uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
+  const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
+  for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
+    const uint32_t lo = win[2 * wi];
+    for (uint32_t i = win[2 * wi + 1] - lo; i > 1; --i) swap_draw(col, lo, i, rapid_next(s));
+  }
+}
+
+// The reference's thread-pool blocks over [0, total) (sqs.h:461-466): chain_rem blocks of
+// chain_block + 1 configurations, then blocks of chain_block; the last block ends at total.
+__device__ __forceinline__ uint64_t chain_block_start(const JobDesc& J, uint64_t b) {
+  return b * J.chain_block + (b < J.chain_rem ? b : J.chain_rem);
+}
+__device__ __forceinline__ uint64_t chain_block_end(const JobDesc& J, uint64_t b) {
+  return b + 1 == J.chain_blocks ? J.total : chain_block_start(J, b + 1);
+}
+__device__ __forceinline__ uint64_t chain_block_of(const JobDesc& J, uint64_t id) {
+  const uint64_t edge = J.chain_rem * (J.chain_block + 1);
+  const uint64_t b = id < edge ? id / (J.chain_block + 1) : J.chain_rem + (id - edge) / J.chain_block;
+  return b < J.chain_blocks ? b : J.chain_blocks - 1;
+}
+// Stream state of a part at the start of the block that begins with configuration `first`: a single
+// thread runs the blocks in order, each configuration shuffles once, each shuffle draws chain_draws.
+__device__ __forceinline__ unsigned long long chain_state(const JobDesc& J, const PartDesc& P, uint64_t first) {
+  return J.seed + first * static_cast<unsigned long long>(P.chain_draws) * kRapidSecret0;
+}
+
 // core/permutation.h:80-102 on the lane's window bytes.
 __device__ __forceinline__ void next_permutation(uint8_t* col, uint32_t lo, uint32_t n) {
   if (n < 2) return;
@@ -1291,6 +1334,49 @@ __device__ __forceinline__ void dispatch_mask(const JobDesc& sj, uint8_t* smem, 
   }
 }
 
+// Reference-stream debug mode (random jobs, general path): each thread runs one of the reference's
+// thread-pool blocks as a chain, like its single worker thread does (sqs.h:348-455 with one thread):
+// the block starts from the packed arrangement (sqs.h:374) and the part's stream at the block's state;
+// interact mode evaluates, then shuffles (sqs.h:397-403,439-440); split mode shuffles every part,
+// then evaluates it (sqs.h:404-413). A tile is up to 128 consecutive blocks; configuration ids are
+// the reference's iteration indices.
+template <class T, int KW>
+__device__ __forceinline__ void run_tile_chain(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
+                                               WarpState& ws) {
+  using F = FP<T>;
+  const int t = threadIdx.x;
+  const bool mine = static_cast<uint64_t>(t) < tile.count;
+  const uint64_t b = tile.start + static_cast<uint64_t>(t);
+  const uint64_t first = mine ? chain_block_start(J, b) : 0, last = mine ? chain_block_end(J, b) : 0;
+  unsigned long long st[kMaxParts];
+  for (uint32_t p = 0; p < J.n_parts; ++p) {
+    init_column(smem, J.parts[p], t);
+    st[p] = chain_state(J, J.parts[p], first);
+  }
+  T thr_g = load_threshold<T>(J);
+  // every lane steps through the longest block (chain_block + 1): the candidate steps are warp-wide
+  for (uint64_t j = 0; j <= J.chain_block; ++j) {
+    const uint64_t id = first + j;
+    const bool active = mine && id < last;
+    T total = T(0);
+    if (active) {
+      for (uint32_t p = 0; p < J.n_parts; ++p) {
+        const PartDesc& P = J.parts[p];
+        if (J.chain_split) shuffle_part_rapid(smem, P, t, st[p]);
+        count_part<KW>(smem, J.blob, P, t);
+        const T o = objective_part<T>(smem, P, t);
+        total = p == 0 ? o : F::add(total, o);
+      }
+    }
+    if ((j & 15) == 0) thr_g = load_threshold<T>(J);
+    const double bound = fmin(ws.list_thr, static_cast<double>(thr_g));
+    const bool pass = active && static_cast<double>(total) <= bound;
+    handle_candidates<T>(J, ctab, ws, pass, total, thr_g, id, t, [&] { return column_key(smem, J, t); });
+    if (J.trace && active) write_trace<T>(J, smem, id - J.trace_base, total, id, t);
+    if (active && !J.chain_split) shuffle_part_rapid(smem, J.parts[0], t, st[0]);
+  }
+}
+
 template <bool SYS, int KMAX>
 __device__ __forceinline__ void dispatch_lattice(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                                  WarpState& ws) {
@@ -1303,6 +1389,20 @@ __device__ __forceinline__ void dispatch_lattice(const JobDesc& sj, uint8_t* sme
 template <bool SYS>
 __device__ __forceinline__ void dispatch_general(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                                  WarpState& ws) {
+  if (!SYS && sj.chain) {
+    if (sj.prec == 1) {
+      if (sj.kw == 1)
+        run_tile_chain<double, 1>(sj, smem, ctab, tile, ws);
+      else
+        run_tile_chain<double, 2>(sj, smem, ctab, tile, ws);
+    } else {
+      if (sj.kw == 1)
+        run_tile_chain<float, 1>(sj, smem, ctab, tile, ws);
+      else
+        run_tile_chain<float, 2>(sj, smem, ctab, tile, ws);
+    }
+    return;
+  }
   if (sj.prec == 1) {
     if (sj.kw == 1)
       run_tile<double, 1, SYS>(sj, smem, ctab, tile, ws);
@@ -1449,7 +1549,7 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
       __syncthreads();
     }
     if (threadIdx.x == 0) {
-      atomicAdd(&sj.counters[kFinished], static_cast<unsigned long long>(tile.count));
+      atomicAdd(&sj.counters[kFinished], static_cast<unsigned long long>(sj.chain ? tile.chain_configs : tile.count));
       atomicAdd(&sj.counters[kTilesDone], 1ull);
       if (live) {
         __threadfence();  // this tile's counts land before the job's tile count drops

@@ -5,7 +5,8 @@
 // arrangement; systematic mode: the multiset permutation of rank id (core/permutation.h:52-78) — so
 // the full record of a selected candidate (species, per-part objective and SRO cube) is rebuilt here,
 // once, through the general pair-stream path: ordered bonds (core/optimization.h:74-77), objective and
-// SRO (optimization.h:79-103), parts summed left to right (sqs.h:417-418). The rebuilt objective must
+// SRO (optimization.h:79-103), parts summed left to right (sqs.h:417-418). In the reference-stream
+// debug mode a configuration is rebuilt by replaying its block's chain up to its id. The rebuilt objective must
 // equal the candidate's bit for bit; every mismatch is counted in *bad (the host raises an error).
 #include "engine_device.cuh"
 #include "kernels.h"
@@ -22,6 +23,14 @@ __device__ __forceinline__ void materialize_one(const JobDesc& J, uint8_t* smem,
     const PartDesc& P = J.parts[0];
     const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
     unrank_window(part_base(smem, P) + P.col_off + 4 * t, P, win[0], win[1] - win[0], id, J.total);
+  } else if (J.chain) {
+    // reference-stream mode: replay the configuration's block from its start (run_tile_chain)
+    const uint64_t first = chain_block_start(J, chain_block_of(J, id));
+    for (uint32_t p = 0; p < J.n_parts; ++p) {
+      unsigned long long st = chain_state(J, J.parts[p], first);
+      const uint64_t shuffles = id - first + (J.chain_split ? 1 : 0);
+      for (uint64_t k = 0; k < shuffles; ++k) shuffle_part_rapid(smem, J.parts[p], t, st);
+    }
   } else {
     const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
     for (uint32_t p = 0; p < J.n_parts; ++p) shuffle_part(smem, J.parts[p], t, 0u, id, p, k0, k1);

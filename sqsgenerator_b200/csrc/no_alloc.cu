@@ -129,6 +129,7 @@ static Err run(const sqsg_job& job, void* stream, uint32_t* n_levels, double* va
     sqsg_last_error(msg, sizeof(msg));
     NA_FAIL(ps, msg);
   }
+  if (pj.chain) NA_FAIL(SQSG_ERR_UNSUPPORTED, "the rapidrand debug mode runs through sqsg_optimize");
   if (pj.blob.size() > kBlobBytes) NA_FAIL(SQSG_ERR_CAPACITY, "job data exceeds the 3 MiB static staging area");
   if (too_many) NA_FAIL(SQSG_ERR_CAPACITY, "the job needs more tiles than the static tile list holds");
   JobDesc d = pj.desc;

@@ -379,7 +379,9 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
   std::vector<std::vector<uint32_t>> k2_nbp_data;
   // validation, pair streams and lattice tables of every part first: the path is chosen per job
   std::vector<LatticeTables> lat(job.n_sublattices);
-  bool job_lat = option(kOptForceGeneral) == 0;
+  // reference-stream debug mode: random jobs only, on the pair-stream path
+  pj.chain = !pj.systematic && option(kOptRapidrand) != 0;
+  bool job_lat = option(kOptForceGeneral) == 0 && !pj.chain;
   bool will_k2 = false;
   for (uint32_t p = 0; p < job.n_sublattices; ++p) {
     const sqsg_sublattice& sl = job.sublattices[p];
@@ -404,7 +406,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
     streams[p] = build_stream(sl);  // validates the pair list
     job_lat = job_lat && lattice_tables(sl, lat[p]) && sl.n_species >= 2;
     if (job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64 && sl.n_shells <= kK2MaxShells &&
-        job.keep < 32 && option(kOptForceGeneral) == 0) {
+        job.keep < 32 && option(kOptForceGeneral) == 0 && !pj.chain) {
       bool has0 = false, has1 = false;  // systematic: the window must hold both species
       for (uint32_t x = sl.windows[0]; x < sl.windows[1]; ++x) (sl.species[x] ? has1 : has0) = true;
       will_k2 = !pj.systematic || (has0 && has1);
@@ -587,6 +589,27 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       d.k2 = sl.n_sites <= 32 ? 1 : 2;
   }
   if (!pj.systematic) pj.total = job.iterations;
+  if (pj.chain) {
+    // The reference's thread-pool blocks over [0, iterations) (BS_thread_pool v5 blocks, sqs.h:461-466):
+    // iterations / chunk_size blocks (at least one), the remainder spread one by one over the first.
+    if (job.range_first != 0 || (job.range_count != 0 && job.range_count != job.iterations))
+      throw unsupported_error("the rapidrand debug mode runs whole jobs (no range_first/range_count)");
+    const uint64_t total = job.iterations;
+    uint64_t nb = job.chunk_size ? total / job.chunk_size : 0;
+    if (nb == 0) nb = 1;
+    nb = std::max<uint64_t>(1, std::min<uint64_t>(nb, std::max<uint64_t>(total, 1)));
+    d.chain = 1;
+    d.chain_split = job.sublattice_mode == 1 ? 1u : 0u;
+    d.chain_blocks = nb;
+    d.chain_block = total / nb;
+    d.chain_rem = total % nb;
+    for (uint32_t p = 0; p < job.n_sublattices; ++p) {
+      const sqsg_sublattice& sl = job.sublattices[p];
+      uint32_t draws = 0;
+      for (uint32_t w = 0; w < sl.n_windows; ++w) draws += sl.windows[2 * w + 1] - sl.windows[2 * w] - 1;
+      d.parts[p].chain_draws = draws;
+    }
+  }
   // Random mode: exact configuration keys for a deduplicating re-run (see column_key), when the
   // product of the parts' arrangement counts stays within kDedupMaxSpace.
   if (!pj.systematic && trace_capacity == 0) {
@@ -689,6 +712,21 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
 
 
 void make_tiles(PreparedJob& pj, uint32_t job_index, std::vector<Tile>& tiles, uint64_t max_per_thread) {
+  if (pj.chain) {  // reference-stream mode: up to kBlock consecutive blocks per tile, one per thread
+    const JobDesc& d = pj.desc;
+    if (pj.total == 0) return;
+    for (uint64_t b = 0; b < d.chain_blocks; b += kBlock) {
+      Tile t{};
+      t.job = job_index;
+      t.start = b;
+      t.count = std::min<uint64_t>(kBlock, d.chain_blocks - b);
+      const uint64_t e = b + t.count;
+      const auto start = [&](uint64_t x) { return x * d.chain_block + std::min(x, d.chain_rem); };
+      t.chain_configs = (e == d.chain_blocks ? pj.total : start(e)) - start(b);
+      tiles.push_back(t);
+    }
+    return;
+  }
   size_t added = 0;
   for_each_tile(
       pj.range_first, pj.range_count, pj.systematic,

@@ -62,6 +62,9 @@ struct PreparedJob {
   // kDedupMaxSpace = dedup_space), so a re-run may deduplicate on the device
   bool dedup_ok = false;
   uint64_t dedup_space = 0;
+  // reference-stream debug mode (option "rapidrand", random jobs): the reference's thread-pool blocks
+  // run as chains, one per thread (JobDesc.chain)
+  bool chain = false;
 };
 
 // A job may have at most this many tiles (about 1.4e14 configurations at full-size tiles).

@@ -21,6 +21,7 @@ enum Option : int {
   kOptUseTuning = 3,        // 1: jobs take the measured launch choices of their bucket (tuning table)
   kOptDefaultCandidates = 4,  // candidate capacity of a job that leaves max_results at 0
   kOptRerunRecordBytes = 5,   // bytes of full records a re-run of an overflowed job may produce
+  kOptRapidrand = 6,          // debug: random jobs follow the reference's seeded single-thread trajectory
   kOptCount
 };
 long long option(Option o);

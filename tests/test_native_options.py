@@ -153,3 +153,14 @@ def test_candidate_budget_options():
     for name in ("default_candidates", "rerun_record_bytes"):
         with pytest.raises(N.NativeError):
             N.set_option(name, 0)
+
+
+def test_rapidrand_debug_option_takes_the_pair_stream():
+    """The reference-stream debug mode runs on the pair-stream path (its chains need the species
+    columns); without it the same job takes the bit-mask path."""
+    assert N.get_option("rapidrand") == 0
+    cfg = cases.fcc32("double", iterations=5000, chunk_size=1000)
+    assert plan_of(cfg)["parts"][0]["path"] == "bitmask"
+    with N.options(rapidrand=1):
+        assert plan_of(cfg)["parts"][0]["path"] == "general"
+    assert N.get_option("rapidrand") == 0
