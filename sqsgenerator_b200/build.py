@@ -21,7 +21,7 @@ OBJDIR = os.path.join(LIBDIR, "obj")
 LIB = os.path.join(LIBDIR, "libsqsg_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["engine.cu", "kernel_mask.cu", "kernel_wide.cu", "kernel_lat.cu", "kernel_lat2.cu", "kernel_lat5.cu", "kernel_materialize.cu", "geometry.cpp", "microbench.cu", "no_alloc.cu",
+SOURCES = ["engine.cu", "kernel_mask.cu", "kernel_wide.cu", "kernel_lat.cu", "kernel_lat2.cu", "kernel_lat5.cu", "kernel_latw.cu", "kernel_materialize.cu", "geometry.cpp", "microbench.cu", "no_alloc.cu",
            "prepare.cu", "select.cu"]
 HEADERS = ["attr_tracker.h", "engine.cuh", "engine_device.cuh", "kernels.h", "permutation.h", "philox.cuh",
            "prepare.h", "select.h", "sqsg_internal.h", "tiles.h", "tuning_table.inc"]

@@ -366,7 +366,8 @@ static uint64_t rerun_limit(const PreparedJob& pj) {
 }
 
 // Lattice path: 64-bit AND-popcount units per configuration of part p (translation classes from the
-// part's shell table {first class, first self-reverse class, end, pairs} x species pairs a <= b < K-1).
+// part's shell table {first class, first self-reverse class, end, pairs} x species pairs a <= b < K-1
+// x words per cell set).
 static uint64_t lattice_units(const PreparedJob& pj, uint32_t p) {
   const PartDesc& P = pj.desc.parts[p];
   const uint64_t na = P.n_species - 1;
@@ -376,7 +377,7 @@ static uint64_t lattice_units(const PreparedJob& pj, uint32_t p) {
     std::memcpy(e, pj.blob.data() + P.blob_off + P.lat_shell_off + 16 * sh, 16);
     classes += e[2] - e[0];
   }
-  return classes * na * (na + 1) / 2;
+  return classes * na * (na + 1) / 2 * pj.desc.lat_words;  // one unit per 64-bit word of a cell set
 }
 
 // Estimated cost of one configuration in pair evaluations of the pair-stream path (its unit of
@@ -712,8 +713,8 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     for (size_t j = 1; j < nj; ++j) {
       const int kj = kind_of(pjs[j].desc);
       if (kj == kind) continue;
-      if (is_lattice_kind(kj) && is_lattice_kind(kind)) {  // the eight-species kernel holds every variant
-        kind = kKindLat;
+      if (is_lattice_kind(kj) && is_lattice_kind(kind) && kj != kKindLatW && kind != kKindLatW) {
+        kind = kKindLat;  // the eight-species kernel holds every one-word variant
         continue;
       }
       if (is_lattice_kind(kj) || is_lattice_kind(kind))
@@ -945,17 +946,19 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
 // One ring per (kernel, occupancy level): ring 0 runs sqsg_engine_mask at 5 CTAs per SM and takes
 // binary bit-mask jobs; rings 1-4 run sqsg_engine_wide at 4, 3, 2, 1 CTAs per SM; rings 5-6 run
 // sqsg_engine_lat2 at 4 and 2, rings 7-8 sqsg_engine_lat5 at 3 and 1, rings 9-10 sqsg_engine_lat at 2
-// and 1 CTAs per SM. A job goes to the ring of its kernel with the largest shared-memory size it fits,
-// i.e. the highest occupancy its data allow; a bit-mask job that fits no mask ring may take a wide
-// ring, and a lattice job that fits no ring of its kernel a ring of sqsg_engine_lat.
-constexpr int kBuckets = 11;
+// and 1, rings 11-12 sqsg_engine_latw at 2 and 1 CTAs per SM. A job goes to the ring of its kernel
+// with the largest shared-memory size it fits, i.e. the highest occupancy its data allow; a bit-mask
+// job that fits no mask ring may take a wide ring, and a lattice job of up to 64 cells that fits no
+// ring of its kernel a ring of sqsg_engine_lat.
+constexpr int kBuckets = 13;
 struct RingSpec {
   int kind;  // KernelKind
   int want;  // CTAs per SM
 };
 constexpr RingSpec kRingSpec[kBuckets] = {{kKindMask, 5}, {kKindWide, 4}, {kKindWide, 3}, {kKindWide, 2},
                                           {kKindWide, 1}, {kKindLat2, 4}, {kKindLat2, 2}, {kKindLat5, 3},
-                                          {kKindLat5, 1}, {kKindLat, 2},  {kKindLat, 1}};
+                                          {kKindLat5, 1}, {kKindLat, 2},  {kKindLat, 1},  {kKindLatW, 2},
+                                          {kKindLatW, 1}};
 // CTAs per SM of the most occupied ring of a kernel kind.
 static int ring_top_occupancy(int kind) {
   int top = 1;
@@ -1997,7 +2000,7 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
         break;
       }
     // a bit-mask job may run the general path as well, and every lattice job the eight-species kernel
-    const int other = kind == kKindMask ? kKindWide : (is_lattice_kind(kind) ? kKindLat : -1);
+    const int other = kind == kKindMask ? kKindWide : (is_lattice_kind(kind) && kind != kKindLatW ? kKindLat : -1);
     if (J->bucket < 0 && other >= 0)
       for (int b = 0; b < kBuckets; ++b)
         if (kRingSpec[b].kind == other && need <= S.rings[b].smem) {

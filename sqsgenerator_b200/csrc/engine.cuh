@@ -54,6 +54,7 @@ constexpr int kMinBlocksWide = 4; // sqsg_engine_wide (general path): 128 regist
 constexpr int kMinBlocksLat = 2;   // sqsg_engine_lat (lattice path, up to 8 species): up to 255 registers
 constexpr int kMinBlocksLat2 = 4;  // sqsg_engine_lat2 (lattice path, binary parts): up to 128 registers
 constexpr int kMinBlocksLat5 = 3;  // sqsg_engine_lat5 (lattice path, up to 5 species): up to 168 registers
+constexpr int kMinBlocksLatW = 2;  // sqsg_engine_latw (lattice path, 65-128 cells, up to 5 species)
 constexpr int kMaxParts = 8;      // sublattices of a split-mode job
 constexpr int kMaxWindows = 16;   // shuffle windows of an interact-mode job
 constexpr int kMaxSpecies = 8;    // K per part handled by the packed-row counter
@@ -151,15 +152,16 @@ struct PartDesc {
   // lattice path (a supercell whose pairs form whole translation classes, see run_tile_lat)
   uint32_t lat_km;        // 0: not on the lattice path; else the unrolled species count: K (K <= 5) or 8
   uint32_t lat_basis;     // unit-cell sites m
-  uint32_t lat_cells;     // cells A*B*C (<= 64: one 64-bit plane per unit-cell site and species)
+  uint32_t lat_cells;     // cells A*B*C (<= 128: one plane of lat_words words per unit-cell site and species)
   uint32_t lat_chunks;    // ceil(cells / 4)
   uint32_t lat_site_off;  // staged: u32 column offsets by (unit-cell site, cell), m x 4*chunks
   uint32_t lat_ent_off;   // staged: u32 classes  beta | beta2 << 4 | translation << 8, by shell
   uint32_t lat_shell_off; // staged: uint4 per shell (first class, first self-reverse class, end, pairs)
   uint32_t lat_tr_off;    // staged: LatTr per translation
   uint32_t lat_deg_off;   // staged: u32 shell-s neighbours of each unit-cell site, S x m
-  uint32_t lat_planes_off;// shared-memory-only: per lane m x (K-1) one-hot planes (u64, interleaved by lane)
-  unsigned long long lat_full;  // the cells' bits
+  uint32_t lat_planes_off;// shared-memory-only: per lane m x (K-1) one-hot planes of lat_words u64 (interleaved by lane)
+  unsigned long long lat_full;     // the cells' bits (first word)
+  unsigned long long lat_full_hi;  // cells 64..127 (two-word cell sets)
   // configuration keys of a deduplicating re-run: species counts of the part (all its sites), the
   // number of their distinct arrangements, and the product of the earlier parts' numbers
   uint32_t dd_counts[kMaxSpecies];
@@ -171,10 +173,11 @@ struct PartDesc {
 };
 
 // A translation of the cell grid (bit c = x + A*(y + B*z)) by (dx, dy, dz), as rotations inside rows
-// of A bits, blocks of A*B bits and the whole grid; a zero shift skips its stage.
+// of A bits, blocks of A*B bits and the whole grid; a zero shift skips its stage. Masks have two words
+// (cell sets of up to 128 cells); sets of up to 64 cells use the first.
 struct LatTr {
   uint32_t sx, sxr, sy, syr, sz, szr, pad0, pad1;
-  unsigned long long mxh, mxl, myh, myl;
+  unsigned long long mxh[2], mxl[2], myh[2], myl[2];
 };
 
 struct JobDesc {
@@ -191,6 +194,8 @@ struct JobDesc {
   uint32_t big_len;       // entries per warp list in shared memory (0: the list is one register per lane)
   uint32_t lat;           // 1: every part takes the lattice path
   uint32_t lat_kmax;      // lattice path: the largest unrolled species count (PartDesc.lat_km) of the parts
+  uint32_t lat_words;     // lattice path: 64-bit words per cell set (1: up to 64 cells, 2: up to 128)
+  uint32_t lat_pad2;
   uint32_t trace;         // 1: write every evaluated configuration to the trace buffers
   uint32_t trace_species_stride, trace_bonds_stride;
   uint64_t seed;

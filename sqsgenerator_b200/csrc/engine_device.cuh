@@ -1009,66 +1009,152 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
 // A supercell of A x B x C copies of a unit cell with m sites: site (beta, c) is unit-cell site beta
 // in cell c = x + A*(y + B*z). Translating every site by one cell vector maps the pair list onto
 // itself (distances and shells depend only on the difference vector), so the pairs of one shell fall
-// into classes {(beta, c), (beta2, c + d)} over all cells c. With X[beta][a] the 64-bit set of cells
-// whose site beta holds species a, the pairs of one class with species {a, b} number
+// into classes {(beta, c), (beta2, c + d)} over all cells c. With X[beta][a] the set of cells whose
+// site beta holds species a (W 64-bit words: up to 64 or 128 cells), the pairs of one class with
+// species {a, b} number
 //   popc(X[beta][a] & Y[b]) + popc(X[beta][b] & Y[a]),  Y[b] = X[beta2][b] translated by -d,
 // (one popcount of the OR: the two sets are disjoint), and a class that is its own reverse
 // (beta == beta2, 2d = 0) counts each pair twice. Counting only the species a, b < K-1 and closing with
 // the degree identity sum_b (1 + [a == b]) U(a, b) = sum_{sites i of species a} deg_s(i) gives the
 // unordered counts U(a, b) = bonds(s,a,b) + bonds(s,b,a) (a != b) and U(a, a) = bonds(s,a,a) that
 // core/optimization.h:79-103 reads, exactly. A class costs one AND (+ OR) and one popcount per
-// species pair instead of one gather per pair of sites.
+// species pair and word instead of one gather per pair of sites.
 
-__device__ __forceinline__ unsigned long long lat_translate(unsigned long long v, const LatTr* t,
-                                                            unsigned long long full) {
-  const uint32_t sx = t->sx, sy = t->sy, sz = t->sz;
-  if (sx) v = ((v << sx) & t->mxh) | ((v >> t->sxr) & t->mxl);
-  if (sy) v = ((v << sy) & t->myh) | ((v >> t->syr) & t->myl);
-  if (sz) v = ((v << sz) | (v >> t->szr)) & full;
+// W-word cell sets; shifts by 0 < k < 64 W (a warp-uniform amount: one translation for all lanes).
+template <int W> struct LatBits {
+  unsigned long long w[W];
+};
+
+template <int W> __device__ __forceinline__ LatBits<W> lat_shl(const LatBits<W>& v, uint32_t k) {
+  LatBits<W> r;
+  if constexpr (W == 1) {
+    r.w[0] = v.w[0] << k;
+  } else {
+    if (k >= 64) {
+      r.w[1] = v.w[0] << (k - 64);
+      r.w[0] = 0ull;
+    } else {
+      r.w[1] = (v.w[1] << k) | (v.w[0] >> (64 - k));
+      r.w[0] = v.w[0] << k;
+    }
+  }
+  return r;
+}
+
+template <int W> __device__ __forceinline__ LatBits<W> lat_shr(const LatBits<W>& v, uint32_t k) {
+  LatBits<W> r;
+  if constexpr (W == 1) {
+    r.w[0] = v.w[0] >> k;
+  } else {
+    if (k >= 64) {
+      r.w[0] = v.w[1] >> (k - 64);
+      r.w[1] = 0ull;
+    } else {
+      r.w[0] = (v.w[0] >> k) | (v.w[1] << (64 - k));
+      r.w[1] = v.w[1] >> k;
+    }
+  }
+  return r;
+}
+
+// Translation of a cell set by (tx, ty, tz): rotations inside rows of A bits, blocks of A*B bits and
+// the whole grid of A*B*C bits (masks select the cells that wrap); a zero shift skips its stage.
+template <int W>
+__device__ __forceinline__ LatBits<W> lat_translate(LatBits<W> v, const LatTr* t, const LatBits<W>& full) {
+  if (t->sx) {
+    const LatBits<W> h = lat_shl<W>(v, t->sx), l = lat_shr<W>(v, t->sxr);
+#pragma unroll
+    for (int k = 0; k < W; ++k) v.w[k] = (h.w[k] & t->mxh[k]) | (l.w[k] & t->mxl[k]);
+  }
+  if (t->sy) {
+    const LatBits<W> h = lat_shl<W>(v, t->sy), l = lat_shr<W>(v, t->syr);
+#pragma unroll
+    for (int k = 0; k < W; ++k) v.w[k] = (h.w[k] & t->myh[k]) | (l.w[k] & t->myl[k]);
+  }
+  if (t->sz) {
+    const LatBits<W> h = lat_shl<W>(v, t->sz), l = lat_shr<W>(v, t->szr);
+#pragma unroll
+    for (int k = 0; k < W; ++k) v.w[k] = (h.w[k] | l.w[k]) & full.w[k];
+  }
+  return v;
+}
+
+template <int W> __device__ __forceinline__ LatBits<W> lat_full(const PartDesc& P) {
+  LatBits<W> f;
+  f.w[0] = P.lat_full;
+  if constexpr (W == 2) f.w[1] = P.lat_full_hi;
+  return f;
+}
+
+// Plane (beta, a) of lane t: W words at [(beta * (K-1) + a) * W + k] * kBlock + t.
+template <int W>
+__device__ __forceinline__ LatBits<W> lat_load(const unsigned long long* X, uint32_t plane) {
+  LatBits<W> v;
+#pragma unroll
+  for (int k = 0; k < W; ++k) v.w[k] = X[(plane * W + k) * kBlock];
   return v;
 }
 
 // The lane's one-hot planes X[beta][a] (a < K-1) from its species column: four sites per step, bit k
 // of each site's species gathered into a nibble (binary planes), then one-hot by AND/NOT.
-template <int KM>
+template <int KM, int W>
 __device__ __forceinline__ void lat_planes(uint8_t* smem, const PartDesc& P, int t) {
   uint8_t* part = part_base(smem, P);
   const uint8_t* col = part + P.col_off + 4 * t;
   const uint4* so4 = reinterpret_cast<const uint4*>(part + P.lat_site_off);
   unsigned long long* X = reinterpret_cast<unsigned long long*>(part + P.lat_planes_off) + t;
   const uint32_t km1 = P.n_species - 1, chunks = P.lat_chunks;
-  const unsigned long long full = P.lat_full;
+  const LatBits<W> full = lat_full<W>(P);
   constexpr int NB = KM <= 2 ? 1 : (KM <= 4 ? 2 : 3);
   for (uint32_t beta = 0; beta < P.lat_basis; ++beta) {
-    unsigned long long B[NB];
+    unsigned long long B[NB][W];
 #pragma unroll
-    for (int k = 0; k < NB; ++k) B[k] = 0ull;
+    for (int k = 0; k < NB; ++k)
+#pragma unroll
+      for (int w = 0; w < W; ++w) B[k][w] = 0ull;
     for (uint32_t q = 0; q < chunks; ++q) {
       const uint4 o = so4[beta * chunks + q];
-      const uint32_t w = static_cast<uint32_t>(col[o.x]) | (static_cast<uint32_t>(col[o.y]) << 8) |
-                         (static_cast<uint32_t>(col[o.z]) << 16) | (static_cast<uint32_t>(col[o.w]) << 24);
+      const uint32_t w4 = static_cast<uint32_t>(col[o.x]) | (static_cast<uint32_t>(col[o.y]) << 8) |
+                          (static_cast<uint32_t>(col[o.z]) << 16) | (static_cast<uint32_t>(col[o.w]) << 24);
 #pragma unroll
       for (int k = 0; k < NB; ++k) {  // species codes are 8 * species: bit k of the species is bit 3 + k
-        const uint32_t nib = ((((w >> (3 + k)) & 0x01010101u) * 0x00204081u) >> 21) & 0xfu;
-        B[k] |= static_cast<unsigned long long>(nib) << (4 * q);
+        const unsigned long long nib = ((((w4 >> (3 + k)) & 0x01010101u) * 0x00204081u) >> 21) & 0xfu;
+        if constexpr (W == 1) {
+          B[k][0] |= nib << (4 * q);
+        } else {
+          if (q < 16)
+            B[k][0] |= nib << (4 * q);
+          else
+            B[k][1] |= nib << (4 * (q - 16));
+        }
       }
     }
 #pragma unroll
     for (int a = 0; a < KM - 1; ++a) {
       if (a >= static_cast<int>(km1)) break;
-      unsigned long long x = full;
 #pragma unroll
-      for (int k = 0; k < NB; ++k) x &= ((a >> k) & 1) ? B[k] : ~B[k];
-      X[(beta * km1 + a) * kBlock] = x;
+      for (int w = 0; w < W; ++w) {
+        unsigned long long x = full.w[w];
+#pragma unroll
+        for (int k = 0; k < NB; ++k) x &= ((a >> k) & 1) ? B[k][w] : ~B[k][w];
+        X[((beta * km1 + a) * W + w) * kBlock] = x;
+      }
     }
   }
 }
 
 template <int NA> __host__ __device__ constexpr int lat_idx(int a, int b) { return a * NA - a * (a - 1) / 2 + (b - a); }
 
+template <int W> __device__ __forceinline__ uint32_t lat_popc(const LatBits<W>& v) {
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 0; k < W; ++k) c += __popcll(v.w[k]);
+  return c;
+}
+
 // Objective of one part (core/optimization.h:79-103, terms in the reference's order) from the lane's
 // planes.
-template <int KM, class T>
+template <int KM, class T, int W>
 __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int t) {
   using F = FP<T>;
   constexpr int NA = KM - 1;  // species with planes, at most
@@ -1080,7 +1166,7 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
   const LatTr* trs = reinterpret_cast<const LatTr*>(part + P.lat_tr_off);
   const uint32_t* deg = reinterpret_cast<const uint32_t*>(part + P.lat_deg_off);
   const uint32_t K = P.n_species, km1 = K - 1, S = P.n_shells, m = P.lat_basis;
-  const unsigned long long full = P.lat_full;
+  const LatBits<W> full = lat_full<W>(P);
   const uint32_t skk = S * K * K;
   const T* f = reinterpret_cast<const T*>(part + P.cube_off);
   const T* w = f + skk;
@@ -1092,9 +1178,11 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
     for (int k = 0; k < NT; ++k) acc[k] = 0u;
     const uint4 sh = shl[s];
     uint32_t key = ~0u, cur = ~0u;
-    unsigned long long Y[NA], Xa[NA];
+    LatBits<W> Y[NA], Xa[NA];
 #pragma unroll
-    for (int a = 0; a < NA; ++a) Y[a] = Xa[a] = 0ull;
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int k = 0; k < W; ++k) Y[a].w[k] = Xa[a].w[k] = 0ull;
     for (uint32_t e = sh.x; e < sh.z; ++e) {
       if (e == sh.y) {  // self-reverse classes count every pair twice: double what came before
 #pragma unroll
@@ -1108,7 +1196,7 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
           if (a >= static_cast<int>(km1)) break;
-          Y[a] = lat_translate(X[(b2 * km1 + a) * kBlock], tr, full);
+          Y[a] = lat_translate<W>(lat_load<W>(X, b2 * km1 + a), tr, full);
         }
       }
       if ((en & 0xfu) != cur) {
@@ -1116,7 +1204,7 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
           if (a >= static_cast<int>(km1)) break;
-          Xa[a] = X[(cur * km1 + a) * kBlock];
+          Xa[a] = lat_load<W>(X, cur * km1 + a);
         }
       }
 #pragma unroll
@@ -1124,8 +1212,12 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
 #pragma unroll
         for (int b = a; b < NA; ++b) {
           if (b >= static_cast<int>(km1)) break;
-          acc[lat_idx<NA>(a, b)] +=
-              a == b ? __popcll(Xa[a] & Y[a]) : __popcll((Xa[a] & Y[b]) | (Xa[b] & Y[a]));
+          uint32_t c = 0;
+#pragma unroll
+          for (int k = 0; k < W; ++k)
+            c += a == b ? __popcll(Xa[a].w[k] & Y[a].w[k])
+                        : __popcll((Xa[a].w[k] & Y[b].w[k]) | (Xa[b].w[k] & Y[a].w[k]));
+          acc[lat_idx<NA>(a, b)] += c;
         }
       }
     }
@@ -1142,7 +1234,7 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
       ue[a] = 0u;
       if (a >= static_cast<int>(km1)) break;
       uint32_t h = 0u;
-      for (uint32_t beta = 0; beta < m; ++beta) h += deg[s * m + beta] * __popcll(X[(beta * km1 + a) * kBlock]);
+      for (uint32_t beta = 0; beta < m; ++beta) h += deg[s * m + beta] * lat_popc<W>(lat_load<W>(X, beta * km1 + a));
       uint32_t u = h - 2u * acc[lat_idx<NA>(a, a)];
 #pragma unroll
       for (int b = 0; b < NA; ++b) {
@@ -1187,33 +1279,33 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
 
 // One variant per unrolled species count up to the kernel's KMAX (a kernel holds only the variants
 // it may meet, so that its register budget is that of its largest variant).
-template <class T, int KMAX>
+template <class T, int KMAX, int W>
 __device__ __forceinline__ T lat_part(uint8_t* smem, const PartDesc& P, int t) {
   if (P.lat_km == 2) {
-    lat_planes<2>(smem, P, t);
-    return lat_objective<2, T>(smem, P, t);
+    lat_planes<2, W>(smem, P, t);
+    return lat_objective<2, T, W>(smem, P, t);
   }
   if constexpr (KMAX >= 3) {
     if (P.lat_km == 3) {
-      lat_planes<3>(smem, P, t);
-      return lat_objective<3, T>(smem, P, t);
+      lat_planes<3, W>(smem, P, t);
+      return lat_objective<3, T, W>(smem, P, t);
     }
   }
   if constexpr (KMAX >= 4) {
     if (P.lat_km == 4) {
-      lat_planes<4>(smem, P, t);
-      return lat_objective<4, T>(smem, P, t);
+      lat_planes<4, W>(smem, P, t);
+      return lat_objective<4, T, W>(smem, P, t);
     }
   }
   if constexpr (KMAX >= 5) {
     if (P.lat_km == 5) {
-      lat_planes<5>(smem, P, t);
-      return lat_objective<5, T>(smem, P, t);
+      lat_planes<5, W>(smem, P, t);
+      return lat_objective<5, T, W>(smem, P, t);
     }
   }
   if constexpr (KMAX >= 8) {
-    lat_planes<8>(smem, P, t);
-    return lat_objective<8, T>(smem, P, t);
+    lat_planes<8, W>(smem, P, t);
+    return lat_objective<8, T, W>(smem, P, t);
   }
   return T(0);  // not reached: the host launches a job only in a kernel with KMAX >= its lat_kmax
 }
@@ -1221,7 +1313,7 @@ __device__ __forceinline__ T lat_part(uint8_t* smem, const PartDesc& P, int t) {
 // The general tile loop with lattice counting. In trace mode the pair-stream count runs as well: its
 // ordered bonds go to the trace, and an objective that differs from the lattice path's is counted in
 // counters[kMismatch] (the host reports it as an error).
-template <class T, bool SYS, int KMAX>
+template <class T, bool SYS, int KMAX, int W>
 __device__ __forceinline__ void run_tile_lat(const JobDesc& J, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                              WarpState& ws) {
   using F = FP<T>;
@@ -1252,7 +1344,7 @@ __device__ __forceinline__ void run_tile_lat(const JobDesc& J, uint8_t* smem, Le
           if (it > 0) init_column(smem, P, t);
           shuffle_part(smem, P, t, 0u, tile.start + my_off + it, p, k0, k1);
         }
-        const T o = lat_part<T, KMAX>(smem, P, t);
+        const T o = lat_part<T, KMAX, W>(smem, P, t);
         if (J.trace) {
           if (J.kw == 1)
             count_part<1>(smem, J.blob, P, t);
@@ -1377,13 +1469,13 @@ __device__ __forceinline__ void run_tile_chain(const JobDesc& J, uint8_t* smem, 
   }
 }
 
-template <bool SYS, int KMAX>
+template <bool SYS, int KMAX, int W>
 __device__ __forceinline__ void dispatch_lattice(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                                  WarpState& ws) {
   if (sj.prec == 1)
-    run_tile_lat<double, SYS, KMAX>(sj, smem, ctab, tile, ws);
+    run_tile_lat<double, SYS, KMAX, W>(sj, smem, ctab, tile, ws);
   else
-    run_tile_lat<float, SYS, KMAX>(sj, smem, ctab, tile, ws);
+    run_tile_lat<float, SYS, KMAX, W>(sj, smem, ctab, tile, ws);
 }
 
 template <bool SYS>
@@ -1418,8 +1510,9 @@ __device__ __forceinline__ void dispatch_general(const JobDesc& sj, uint8_t* sme
 
 // Each kernel holds some of the paths (see kernels.h); the host launches a job only in a kernel that
 // holds its path (a bit-mask job may also run the general path: its columns and stream exist too).
-// LAT: 0 = no lattice path; else the largest unrolled species count the kernel holds (4, 5 or 8).
-template <bool SYS, bool GENERAL, bool MASK, int LAT>
+// LAT: 0 = no lattice path; else the largest unrolled species count the kernel holds (2, 5 or 8);
+// LATW: the words per cell set of its lattice jobs (1: up to 64 cells, 2: up to 128).
+template <bool SYS, bool GENERAL, bool MASK, int LAT, int LATW>
 __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, LevelSlot* ctab, const Tile& tile,
                                               WarpState& ws) {
   if constexpr (MASK) {
@@ -1429,8 +1522,8 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
     }
   }
   if constexpr (LAT > 0) {
-    if (sj.lat && sj.lat_kmax <= static_cast<uint32_t>(LAT)) {
-      dispatch_lattice<SYS, LAT>(sj, smem, ctab, tile, ws);
+    if (sj.lat && sj.lat_kmax <= static_cast<uint32_t>(LAT) && sj.lat_words == static_cast<uint32_t>(LATW)) {
+      dispatch_lattice<SYS, LAT, LATW>(sj, smem, ctab, tile, ws);
       return;
     }
   }
@@ -1449,7 +1542,7 @@ __device__ __forceinline__ void dispatch_tile(const JobDesc& sj, uint8_t* smem, 
 // whenever its next tile belongs to another job. In live mode every tile ends with a level flush and
 // a decrement of the job's tile count; the CTA that finishes a job's last tile publishes the job's
 // generation in done[slot] (host-mapped memory).
-template <bool GENERAL, bool MASK, int LAT>
+template <bool GENERAL, bool MASK, int LAT, int LATW = 1>
 __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles,
                                             uint32_t n_tiles, QueueCtl* q, const volatile int32_t* cancel,
                                             unsigned long long* status, volatile uint32_t* done) {
@@ -1539,9 +1632,9 @@ __device__ __forceinline__ void engine_body(const JobDesc* __restrict__ jobs, co
       ws.reset(sj, smem);
     }
     if (sj.mode == 1)
-      dispatch_tile<true, GENERAL, MASK, LAT>(sj, smem, ctab, tile, ws);
+      dispatch_tile<true, GENERAL, MASK, LAT, LATW>(sj, smem, ctab, tile, ws);
     else
-      dispatch_tile<false, GENERAL, MASK, LAT>(sj, smem, ctab, tile, ws);
+      dispatch_tile<false, GENERAL, MASK, LAT, LATW>(sj, smem, ctab, tile, ws);
     __syncthreads();  // every thread is done with this tile before s_tile changes
     if (live) {
       flush_levels(ctab, sj);

@@ -35,6 +35,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksLat2)
 __global__ void __launch_bounds__(kBlock, kMinBlocksLat5)
     sqsg_engine_lat5(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
                      const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
+// sqsg_engine_latw: lattice jobs of 65 to 128 unit cells (two-word cell sets), at most five species.
+__global__ void __launch_bounds__(kBlock, kMinBlocksLatW)
+    sqsg_engine_latw(const JobDesc* __restrict__ jobs, const Tile* __restrict__ tiles, uint32_t n_tiles, QueueCtl* q,
+                     const volatile int32_t* cancel, unsigned long long* status, volatile uint32_t* done);
 
 // Rebuilds the full records (selection order) of n candidates of one job; counts objective mismatches.
 __global__ void __launch_bounds__(kBlock)
@@ -45,15 +49,19 @@ using EngineKernel = void (*)(const JobDesc*, const Tile*, uint32_t, QueueCtl*, 
                               unsigned long long*, volatile uint32_t*);
 
 // Kernel kinds: each job runs in the kernel that holds its path. A bit-mask job (k2) runs in
-// sqsg_engine_mask, a lattice job in the lattice kernel of its largest species count (lat_kmax 2, at
-// most 5, at most 8), every other job in sqsg_engine_wide (which may also take bit-mask jobs: their
-// columns and pair stream exist too; sqsg_engine_lat likewise takes every lattice job). A job given to
-// a kernel without its path is skipped on the device and flagged kErrBadJob in its counters.
-enum KernelKind : int { kKindMask = 0, kKindWide = 1, kKindLat = 2, kKindLat2 = 3, kKindLat5 = 4, kKindCount = 5 };
-inline bool is_lattice_kind(int kind) { return kind == kKindLat || kind == kKindLat2 || kind == kKindLat5; }
+// sqsg_engine_mask; a lattice job of up to 64 cells in the lattice kernel of its largest species count
+// (lat_kmax 2, at most 5, at most 8), one of 65-128 cells in sqsg_engine_latw; every other job in
+// sqsg_engine_wide (which may also take bit-mask jobs: their columns and pair stream exist too;
+// sqsg_engine_lat likewise takes every lattice job of up to 64 cells). A job given to a kernel without
+// its path is skipped on the device and flagged kErrBadJob in its counters.
+enum KernelKind : int {
+  kKindMask = 0, kKindWide = 1, kKindLat = 2, kKindLat2 = 3, kKindLat5 = 4, kKindLatW = 5, kKindCount = 6
+};
+inline bool is_lattice_kind(int kind) { return kind >= kKindLat && kind <= kKindLatW; }
 inline int kind_of(const JobDesc& d) {
   if (d.k2) return kKindMask;
   if (!d.lat) return kKindWide;
+  if (d.lat_words == 2) return kKindLatW;
   return d.lat_kmax <= 2 ? kKindLat2 : (d.lat_kmax <= 5 ? kKindLat5 : kKindLat);
 }
 inline EngineKernel kernel_of(int kind) {
@@ -62,6 +70,7 @@ inline EngineKernel kernel_of(int kind) {
     case kKindLat: return sqsg_engine_lat;
     case kKindLat2: return sqsg_engine_lat2;
     case kKindLat5: return sqsg_engine_lat5;
+    case kKindLatW: return sqsg_engine_latw;
     default: return sqsg_engine_wide;
   }
 }
@@ -71,6 +80,7 @@ inline const char* kernel_name(int kind) {
     case kKindLat: return "sqsg_engine_lat";
     case kKindLat2: return "sqsg_engine_lat2";
     case kKindLat5: return "sqsg_engine_lat5";
+    case kKindLatW: return "sqsg_engine_latw";
     default: return "sqsg_engine_wide";
   }
 }

@@ -133,8 +133,8 @@ static uint64_t window_permutations(const sqsg_sublattice& sl, PartDesc& pd) {
 // class {(beta, c), (beta2, c + d)} that the pair list holds completely — once per cell, or once per
 // pair of cells for a class that is its own reverse (beta == beta2, 2d = 0).
 struct LatticeTables {
-  uint32_t m = 0, A = 0, B = 0, C = 0, cells = 0, chunks = 0;
-  unsigned long long full = 0;
+  uint32_t m = 0, A = 0, B = 0, C = 0, cells = 0, chunks = 0, words = 1;
+  unsigned long long full[2] = {0, 0};
   std::vector<uint32_t> site_off;  // m x 4*chunks column offsets (cells past the grid repeat cell 0)
   std::vector<uint32_t> ent;       // beta | beta2 << 4 | translation << 8
   std::vector<uint32_t> shell;     // per shell: first class, first self-reverse class, end, pairs
@@ -148,7 +148,7 @@ static bool lattice_tables(const sqsg_sublattice& sl, LatticeTables& L) {
   const uint32_t A = sl.cells[0], B = sl.cells[1], C = sl.cells[2], m = sl.n_basis;
   if (A == 0 || B == 0 || C == 0 || m == 0 || m > 15) return false;
   const uint64_t cells = static_cast<uint64_t>(A) * B * C;
-  if (cells > 64 || cells * m != N) return false;
+  if (cells > 128 || cells * m != N) return false;
   std::vector<uint32_t> beta(N), cx(N), cy(N), cz(N), site_at(N, ~0u);
   for (uint32_t x = 0; x < N; ++x) {
     const uint32_t* h = sl.lattice + 4 * static_cast<size_t>(x);
@@ -204,7 +204,8 @@ static bool lattice_tables(const sqsg_sublattice& sl, LatticeTables& L) {
   L.C = C;
   L.cells = static_cast<uint32_t>(cells);
   L.chunks = (L.cells + 3) / 4;
-  L.full = cells == 64 ? ~0ull : ((1ull << cells) - 1ull);
+  L.words = cells > 64 ? 2 : 1;
+  for (uint32_t c = 0; c < L.cells; ++c) L.full[c / 64] |= 1ull << (c % 64);
   L.site_off.assign(static_cast<size_t>(m) * 4 * L.chunks, 0);
   for (uint32_t b = 0; b < m; ++b)
     for (uint32_t c = 0; c < 4 * L.chunks; ++c)
@@ -226,14 +227,9 @@ static bool lattice_tables(const sqsg_sublattice& sl, LatticeTables& L) {
     t.szr = L.cells - A * B * tz;
     for (uint32_t c = 0; c < L.cells; ++c) {
       const uint32_t x = c % A, y = (c / A) % B;
-      if (x >= tx)
-        t.mxh |= 1ull << c;
-      else
-        t.mxl |= 1ull << c;
-      if (y >= ty)
-        t.myh |= 1ull << c;
-      else
-        t.myl |= 1ull << c;
+      const unsigned long long bit = 1ull << (c % 64);
+      (x >= tx ? t.mxh : t.mxl)[c / 64] |= bit;
+      (y >= ty ? t.myh : t.myl)[c / 64] |= bit;
     }
     const uint32_t idx = static_cast<uint32_t>(L.tr.size());
     L.tr.push_back(t);
@@ -405,6 +401,9 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       throw std::invalid_argument("In \"systematic\" iteration mode only one sublattice is allowed");
     streams[p] = build_stream(sl);  // validates the pair list
     job_lat = job_lat && lattice_tables(sl, lat[p]) && sl.n_species >= 2;
+    // two-word cell sets (65..128 cells) run in sqsg_engine_latw, which holds up to five species;
+    // every part of a job uses the same width
+    job_lat = job_lat && (lat[p].words == 1 || sl.n_species <= 5) && lat[p].words == lat[0].words;
     if (job.n_sublattices == 1 && sl.n_species == 2 && sl.n_sites <= 64 && sl.n_shells <= kK2MaxShells &&
         job.keep < 32 && option(kOptForceGeneral) == 0 && !pj.chain) {
       bool has0 = false, has1 = false;  // systematic: the window must hold both species
@@ -532,7 +531,9 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       P.lat_basis = LT.m;
       P.lat_cells = LT.cells;
       P.lat_chunks = LT.chunks;
-      P.lat_full = LT.full;
+      P.lat_full = LT.full[0];
+      P.lat_full_hi = LT.full[1];
+      d.lat_words = LT.words;
       P.lat_site_off = static_cast<uint32_t>(off);
       off = align_up(off + 4 * LT.site_off.size(), 16);
       P.lat_ent_off = static_cast<uint32_t>(off);
@@ -543,7 +544,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       off = align_up(off + sizeof(LatTr) * LT.tr.size(), 16);
       P.lat_deg_off = static_cast<uint32_t>(off);
       off = align_up(off + 4 * LT.deg.size(), 16);
-      planes = static_cast<size_t>(LT.m) * (sl.n_species - 1) * 8 * kBlock;
+      planes = static_cast<size_t>(LT.m) * (sl.n_species - 1) * 8 * LT.words * kBlock;
     }
     P.stream_off = static_cast<uint32_t>(off);
     const size_t with_stream = align_up(off + 4ull * streams[p].size(), 16);

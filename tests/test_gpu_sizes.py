@@ -118,6 +118,16 @@ LATTICE_CASES = {
         lattice=(np.eye(3) * 2.87).tolist(), coords=[[0, 0, 0], [0.5, 0.5, 0.5]], species=[1] * 2,
         supercell=[4, 4, 2]), composition={"Ti": 16, "Al": 16, "Nb": 16, "V": 16},
         shell_weights={"1": 1.0, "2": 0.5, "3": 0.25}, iterations=200000, seed=21, thread_config=1, keep=9),
+    # 65-128 cells: two-word cell sets (sqsg_engine_latw)
+    "fcc500_ternary_4shells": lambda: fcc((5, 5, 5), {"Ti": 167, "Al": 167, "Nb": 166}, 4, iterations=60000, seed=41,
+                                          keep=6),
+    "bcc250_quinary": lambda: dict(prec="double", structure=dict(
+        lattice=(np.eye(3) * 2.87).tolist(), coords=[[0, 0, 0], [0.5, 0.5, 0.5]], species=[1] * 2,
+        supercell=[5, 5, 5]), composition={"Ti": 50, "Al": 50, "Nb": 50, "V": 50, "Zr": 50},
+        shell_weights={"1": 1.0, "2": 0.5, "3": 0.25}, iterations=60000, seed=42, thread_config=1, keep=5),
+    "fcc_445_quaternary_single": lambda: fcc((4, 4, 5), {"Ti": 80, "Al": 80, "Nb": 80, "V": 80}, 3, prec="single",
+                                             iterations=60000, seed=43, keep=4),
+    "fcc500_binary": lambda: fcc((5, 5, 5), {"Ti": 250, "Al": 250}, 2, iterations=60000, seed=44, keep=5),
     # six and eight species: the eight-species variant of the lattice path (sqsg_engine_lat)
     "fcc_333_senary": lambda: fcc((3, 3, 3), {"Ti": 18, "Al": 18, "Nb": 18, "V": 18, "Zr": 18, "Hf": 18}, 2,
                                   iterations=100000, seed=31, keep=5),
@@ -131,7 +141,9 @@ LATTICE_CASES = {
 LATTICE_KERNELS = {"config3": "sqsg_engine_lat5", "config4": "sqsg_engine_lat2", "fcc32_ternary": "sqsg_engine_lat5",
                    "fcc32_systematic_ternary": "sqsg_engine_lat5", "perovskite_333": "sqsg_engine_lat5",
                    "rocksalt_interact": "sqsg_engine_lat5", "bcc_4x4x2_quaternary": "sqsg_engine_lat5",
-                   "fcc_333_senary": "sqsg_engine_lat", "bcc_444_octonary": "sqsg_engine_lat"}
+                   "fcc_333_senary": "sqsg_engine_lat", "bcc_444_octonary": "sqsg_engine_lat",
+                   "fcc500_ternary_4shells": "sqsg_engine_latw", "bcc250_quinary": "sqsg_engine_latw",
+                   "fcc_445_quaternary_single": "sqsg_engine_latw", "fcc500_binary": "sqsg_engine_latw"}
 
 
 @pytest.mark.parametrize("name", sorted(LATTICE_CASES))
@@ -151,7 +163,8 @@ def test_lattice_and_general_paths_agree(name):
 
 
 @pytest.mark.parametrize("name", ["fcc32_ternary", "perovskite_333", "bcc_4x4x2_quaternary", "rocksalt_interact",
-                                  "fcc_333_senary", "bcc_444_octonary"])
+                                  "fcc_333_senary", "bcc_444_octonary", "fcc500_ternary_4shells", "bcc250_quinary",
+                                  "fcc_445_quaternary_single"])
 def test_lattice_trace_against_oracle(name):
     cfg = dict(LATTICE_CASES[name]())
     cfg["iterations"] = 4000
@@ -164,10 +177,11 @@ def test_narrow_stream_read_through_l1_fcc500():
     """fcc 5x5x5 (500 sites), three species, four shells (12/6/24/12 neighbours): staging the stream
     would cost a CTA per SM, so it is read from the job blob through L1."""
     cfg = fcc((5, 5, 5), {"Ti": 167, "Al": 167, "Nb": 166}, 4, iterations=1500)
-    p = plan_of(cfg)  # 125 cells: more than the lattice path's 64
-    assert p["parts"][0]["path"] == "general"
-    assert p["parts"][0]["stream_narrow"] and not p["parts"][0]["stream_staged"]
-    c, d, sp, ob, ids = traced(cfg, 1500, "double")
+    with N.options(force_general=1):  # the cell would take the two-word lattice path
+        p = plan_of(cfg)
+        assert p["parts"][0]["path"] == "general"
+        assert p["parts"][0]["stream_narrow"] and not p["parts"][0]["stream_staged"]
+        c, d, sp, ob, ids = traced(cfg, 1500, "double")
     assert len(d[0].species_packed) == 500
 
 

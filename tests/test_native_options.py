@@ -61,10 +61,24 @@ def test_lattice_hint_is_checked():
     assert N.plan(job)["parts"][0]["path"] == "general"
 
 
-def test_lattice_hint_of_more_than_64_cells_is_not_used():
+def test_lattice_hint_up_to_128_cells():
+    """Cell sets of two words: 125 cells take sqsg_engine_latw up to five species; six species or more
+    than 128 cells take the pair stream."""
     cfg = cases.fcc32("double", composition={"Ti": 250, "Al": 250}, iterations=1000)
     cfg["structure"]["supercell"] = [5, 5, 5]
     c, d, (job, bufs) = _job(cfg)
+    with N.options(use_tuning=0):  # the rules' path (a tuning table may prefer the pair stream)
+        p = N.plan(job)
+    assert p["parts"][0]["path"] == "lattice" and p["kernel"] == "sqsg_engine_latw"
+    cfg6 = cases.fcc32("double", composition={e: 500 // 6 + (1 if k < 500 % 6 else 0)
+                                              for k, e in enumerate(("Ti", "Al", "Nb", "V", "Zr", "Hf"))},
+                       iterations=1000)
+    cfg6["structure"]["supercell"] = [5, 5, 5]
+    c, d, (job, bufs) = _job(cfg6)
+    assert N.plan(job)["parts"][0]["path"] == "general"
+    cfg216 = cases.fcc32("double", composition={"Ti": 432, "Al": 432}, iterations=1000)
+    cfg216["structure"]["supercell"] = [6, 6, 6]
+    c, d, (job, bufs) = _job(cfg216)
     assert N.plan(job)["parts"][0]["path"] == "general"
 
 
