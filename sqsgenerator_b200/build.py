@@ -23,7 +23,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["engine.cu", "kernel_mask.cu", "kernel_wide.cu", "kernel_lat.cu", "kernel_lat2.cu", "kernel_lat5.cu", "kernel_latw.cu", "kernel_materialize.cu", "geometry.cpp", "microbench.cu", "no_alloc.cu",
            "prepare.cu", "select.cu"]
-HEADERS = ["attr_tracker.h", "engine.cuh", "engine_device.cuh", "kernels.h", "permutation.h", "philox.cuh",
+HEADERS = ["attr_tracker.h", "engine.cuh", "engine_device.cuh", "host_copy.h", "kernels.h", "permutation.h", "philox.cuh",
            "prepare.h", "select.h", "sqsg_internal.h", "tiles.h", "tuning_table.inc"]
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "--fmad=false",
          "-Xcompiler", "-fPIC,-ffp-contract=off,-O2"]

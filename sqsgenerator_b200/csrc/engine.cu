@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "attr_tracker.h"
+#include "host_copy.h"
 #include "kernels.h"
 #include "permutation.h"
 #include "prepare.h"
@@ -1816,12 +1817,12 @@ sqsg_status sqsg_run_copy(const sqsg_run* run, uint64_t first, uint64_t n, void*
       sp += p.N;
       skk += static_cast<size_t>(p.S) * p.K * p.K;
     }
-    if (objective) std::memcpy(objective, r.objective.data() + first * r.tsz, n * r.tsz);
+    if (objective) parallel_copy(objective, r.objective.data() + first * r.tsz, n * r.tsz);
     if (sub_objectives)
-      std::memcpy(sub_objectives, r.sub_objective.data() + first * r.n_parts * r.tsz, n * r.n_parts * r.tsz);
-    if (species) std::memcpy(species, r.species.data() + first * sp, n * sp);
-    if (sro) std::memcpy(sro, r.sro.data() + first * skk * r.tsz, n * skk * r.tsz);
-    if (id) std::memcpy(id, r.id.data() + first, n * 8);
+      parallel_copy(sub_objectives, r.sub_objective.data() + first * r.n_parts * r.tsz, n * r.n_parts * r.tsz);
+    if (species) parallel_copy(species, r.species.data() + first * sp, n * sp);
+    if (sro) parallel_copy(sro, r.sro.data() + first * skk * r.tsz, n * skk * r.tsz);
+    if (id) parallel_copy(id, r.id.data() + first, n * 8);
   });
 }
 

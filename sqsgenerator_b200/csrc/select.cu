@@ -19,6 +19,7 @@
 #include <cstring>
 #include <string>
 
+#include "host_copy.h"
 #include "kernels.h"
 #include "select.h"
 #include "sqsg_internal.h"
@@ -70,7 +71,7 @@ void copy_out(SelectScratch& S, cudaStream_t st, void* dst, const void* src, siz
   int b = 0;
   auto drain = [&](int k) {
     SEL_CHECK(cudaEventSynchronize(S.bounce_done[k]));
-    std::memcpy(static_cast<uint8_t*>(dst) + pend_off[k], S.bounce[k], pend_len[k]);
+    parallel_copy(static_cast<uint8_t*>(dst) + pend_off[k], S.bounce[k], pend_len[k]);
     pend[k] = false;
   };
   for (size_t off = 0; off < bytes; off += kBounceBytes, b ^= 1) {
