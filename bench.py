@@ -62,6 +62,12 @@ def workload_config(name: str):
                                     composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}]), (
             "rocksalt 3x3x3 (216 sites) split: Ti54Al54 cations and N96B12 anions optimised together, 2 shells per "
             "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations, float32")
+    if name == "fcc500":
+        cfg = cases.fcc32("double", composition={"Ti": 167, "Al": 167, "Nb": 166}, iterations=20_000_000, seed=5,
+                          shell_weights={"1": 1.0, "2": 0.5, "3": 1.0 / 3, "4": 0.25}, keep=10)
+        cfg["structure"]["supercell"] = [5, 5, 5]
+        return cfg, ("fcc 5x5x5 (500 sites) A167B167C166 random, 4 shells (12/6/24/12, P=13500), weights 1/k, "
+                     "2e7 configurations, float64 (the largest cell of the served mixed stream)")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -512,7 +518,7 @@ def run_b200(args):
             "parity": parity}
     if world == 1 and args.extras:
         extras = {}
-        for name, steps in (("random", 20), ("quinary", 2), ("split", 2), ("split_single", 2)):
+        for name, steps in (("random", 20), ("quinary", 2), ("split", 2), ("split_single", 2), ("fcc500", 2)):
             r = measure(name, steps, 1, device, 1, 0, 0)
             cpu_x, par = None, None
             if not args.no_cpu_baseline:
@@ -761,7 +767,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="systematic",
-                    choices=["systematic", "random", "quinary", "split", "split_single", "served"])
+                    choices=["systematic", "random", "quinary", "split", "split_single", "fcc500", "served"])
     ap.add_argument("--jobs", type=int, default=200, help="served: jobs in the stream")
     ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate, jobs/s")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

@@ -254,6 +254,7 @@ sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t ca
  *                              iterations / chunk_size-way parallelism. Configuration ids are the
  *                              reference's iteration indices. Pair-stream path only; sqsg_optimize,
  *                              sqsg_optimize_batch and traces only (not the server, not ranges).
+ *   "server_finalizers"  > 0   result-selection threads of servers created afterwards (default 4).
  * Unknown names give SQSG_ERR_INVALID_ARGUMENT. */
 sqsg_status sqsg_set_option(const char* name, int64_t value);
 sqsg_status sqsg_get_option(const char* name, int64_t* value);

@@ -41,10 +41,10 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 // ------------------------------------------------------------------------------------------------
 // Process-wide options
 static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}, {1},
-                                                      {1ll << 20}, {4ll << 30}, {0}};
+                                                      {1ll << 20}, {4ll << 30}, {0}, {4}};
 static const char* const kOptionNames[kOptCount] = {"force_general", "stage_wait_ns", "debug_skip_staging",
                                                     "use_tuning", "default_candidates", "rerun_record_bytes",
-                                                    "rapidrand"};
+                                                    "rapidrand", "server_finalizers"};
 
 long long option(Option o) { return g_options[o].load(std::memory_order_relaxed); }
 
@@ -1630,7 +1630,8 @@ sqsg_status sqsg_set_option(const char* name, int64_t value) {
   return guarded([&] {
     const int k = option_index(name);
     if (k < 0) throw std::invalid_argument(std::string("unknown option: ") + (name ? name : "(null)"));
-    if ((k == kOptStageWaitNs || k == kOptDefaultCandidates || k == kOptRerunRecordBytes) && value <= 0)
+    if ((k == kOptStageWaitNs || k == kOptDefaultCandidates || k == kOptRerunRecordBytes ||
+         k == kOptServerFinalizers) && value <= 0)
       throw std::out_of_range(std::string(kOptionNames[k]) + " must be positive");
     g_options[k].store(value);
   });
@@ -1977,7 +1978,8 @@ sqsg_status sqsg_server_create(const sqsg_server_options* options, sqsg_server**
     S.slots.resize(nslot);
     S.slot_gen.assign(nslot, 0);
     S.worker = std::thread(server_loop, &S);
-    for (int k = 0; k < 4; ++k) S.finalizers.emplace_back(finalizer_loop, &S);
+    const int finalizers = static_cast<int>(std::min<long long>(32, std::max<long long>(1, option(kOptServerFinalizers))));
+    for (int k = 0; k < finalizers; ++k) S.finalizers.emplace_back(finalizer_loop, &S);
     *out = srv.release();
   });
 }

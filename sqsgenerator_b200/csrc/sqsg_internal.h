@@ -22,6 +22,7 @@ enum Option : int {
   kOptDefaultCandidates = 4,  // candidate capacity of a job that leaves max_results at 0
   kOptRerunRecordBytes = 5,   // bytes of full records a re-run of an overflowed job may produce
   kOptRapidrand = 6,          // debug: random jobs follow the reference's seeded single-thread trajectory
+  kOptServerFinalizers = 7,   // result-selection threads of a server created afterwards
   kOptCount
 };
 long long option(Option o);
