@@ -131,7 +131,8 @@ typedef struct {
    * unit-cell site among this structure's unit-cell sites (0..n_basis-1) and its cell indices along
    * the three lattice vectors. The library checks the hint against the pair list: when every shell's
    * pairs are whole translation classes it counts bonds with translated bit planes (SQSG_PATH_LATTICE,
-   * up to 64 cells); otherwise the hint is ignored. Results do not depend on it. */
+   * up to 64 cells, or up to 128 cells with at most five species); otherwise the hint is ignored.
+   * Results do not depend on it. */
   const uint32_t* lattice;
   uint32_t cells[3];
   uint32_t n_basis;
