@@ -61,13 +61,55 @@ def representative_jobs() -> dict:
     return jobs
 
 
+def summarize(report: dict) -> str:
+    """Markdown table of a tuning report: per representative job the chosen launch choices, their rate, the
+    rate of the fixed rules' choice (the path and stream staging `sqsg_plan_job` gives without the table, all
+    CTAs that fit, tile cap 65536) and the spread of every measured choice. Needs no GPU."""
+    rows = ["| representative job | bucket | chosen: path, staged, CTAs/SM, tile cap | configs/s | rules' choice configs/s "
+            "| chosen / rules | choices | best / worst |", "|---|---:|---|---:|---:|---:|---:|---:|"]
+    jobs = representative_jobs()
+    prev = _native.get_option("use_tuning")
+    _native.set_option("use_tuning", 0)
+    try:
+        for name, r in report.items():
+            b, tried = r["best"], r["tried"]
+            rules = None
+            if name in jobs:
+                c = parse_config(jobs[name])
+                job, keep = build_job(c, prepare(c))
+                part = _native.plan(job)["parts"][0]
+                staged = int(part["stream_staged"]) if part["path"] == "general" else -1
+                for t in tried:
+                    if (t["path"] == part["path"] and t["ctas_per_sm"] == 0 and t["tile_cap"] == 65536
+                            and (part["path"] != "general" or t["stream_staged"] == staged)):
+                        rules = t["configs_per_s"]
+                        break
+            worst = min(t["configs_per_s"] for t in tried)
+            rules_s = f"{rules / 1e6:.1f}e6" if rules else "—"
+            ratio = f"{b['configs_per_s'] / rules:.2f}" if rules else "—"
+            rows.append(f"| {name} | {r['bucket']} | {b['path']}, {b['stream_staged']}, {b['ctas_per_sm'] or 'all'}, "
+                        f"{b['tile_cap']} | {b['configs_per_s'] / 1e6:.1f}e6 | {rules_s} | {ratio} | {len(tried)} | "
+                        f"{b['configs_per_s'] / worst:.2f} |")
+    finally:
+        _native.set_option("use_tuning", prev)
+    return "\n".join(rows) + "\n"
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--seconds", type=float, default=1.5, help="measuring budget per job")
-    ap.add_argument("--out", required=True, help="path of the tuning_table.inc to write")
+    ap.add_argument("--out", default=None, help="path of the tuning_table.inc to write")
+    ap.add_argument("--summarize", default=None, metavar="REPORT",
+                    help="print the markdown summary of a report written by --report (no GPU needed) and exit")
     ap.add_argument("--report", default=None, help="JSON report of every measured choice")
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args()
+    if args.summarize:
+        with open(args.summarize) as f:
+            print(summarize(json.load(f)), end="")
+        return
+    if not args.out:
+        ap.error("--out is required when measuring")
     _native.set_option("use_tuning", 0)
     entries, report = {}, {}
     for name, cfg in representative_jobs().items():
