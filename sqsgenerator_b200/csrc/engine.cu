@@ -461,7 +461,7 @@ static void levels_from_records(const PreparedJob& pj, const std::vector<Cand>& 
   }
 }
 
-static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, const std::vector<LevelSlot>& lv,
+static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, const LevelSlot* lv,
                       const std::vector<Cand>& recs, uint64_t stored, uint64_t capacity, bool may_rerun,
                       uint64_t max_capacity) {
   Outcome o;
@@ -469,8 +469,8 @@ static Outcome assess(const PreparedJob& pj, const unsigned long long* cnt, cons
   const bool overflow = cnt[kLevelOverflow] != 0;
   if (!overflow) {
     std::vector<LevelSlot> used;
-    for (auto& x : lv)
-      if (x.key) used.push_back(x);
+    for (int k = 0; k < kLevelSlots; ++k)
+      if (lv[k].key) used.push_back(lv[k]);
     std::sort(used.begin(), used.end(), [](const LevelSlot& a, const LevelSlot& b) { return a.key < b.key; });
     uint64_t need = 0;
     for (size_t k = 0; k < used.size() && k <= pj.keep; ++k) {
@@ -809,12 +809,12 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
     std::vector<std::vector<Cand>> recs(nj);
     std::vector<Outcome> outc(nj);
     uint64_t d2h_bytes = cnt.size() * sizeof(unsigned long long) + 8;
+    std::vector<LevelSlot> lv_all(nj * kLevelSlots);  // every job's level table in one copy
+    CUDA_CHECK(cudaMemcpy(lv_all.data(), ws->levels.p, lv_all.size() * sizeof(LevelSlot), cudaMemcpyDeviceToHost));
+    d2h_bytes += lv_all.size() * sizeof(LevelSlot);
     for (size_t j = 0; j < nj; ++j) {
       const unsigned long long* cj = &cnt[j * kNumCounters];
-      std::vector<LevelSlot> lv(kLevelSlots);
-      CUDA_CHECK(cudaMemcpy(lv.data(), static_cast<LevelSlot*>(ws->levels.p) + j * kLevelSlots,
-                            kLevelSlots * sizeof(LevelSlot), cudaMemcpyDeviceToHost));
-      d2h_bytes += kLevelSlots * sizeof(LevelSlot);
+      const LevelSlot* lv = lv_all.data() + j * kLevelSlots;
       const uint64_t n = std::min<uint64_t>(cj[kCandidates], capacity[j]);
       if (cj[kLevelOverflow]) {
         recs[j].resize(n);
@@ -1261,7 +1261,8 @@ static void finalizer_loop(ServerState* Sp) {
     try {
       if (!error.empty()) throw cuda_error(error);
       check_job_counters(cnt);
-      o = assess(J.pj, cnt, c.levels, c.records, n, J.capacity, !J.user_capacity && J.attempt < 2, arena_records);
+      o = assess(J.pj, cnt, c.levels.data(), c.records, n, J.capacity, !J.user_capacity && J.attempt < 2,
+                 arena_records);
       if (!o.rerun) {
         r.prec = J.pj.prec;
         r.n_parts = J.pj.desc.n_parts;
