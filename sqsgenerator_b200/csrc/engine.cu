@@ -20,6 +20,7 @@
 #include <mutex>
 #include <random>
 #include <string>
+#include <exception>
 #include <thread>
 #include <unordered_set>
 #include <vector>
@@ -1612,7 +1613,7 @@ static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, co
       classes[{kind, -per_sm}].push_back(j);
     }
     std::vector<std::unique_ptr<sqsg_run>> done(n);
-    for (auto& [key, idx] : classes) {
+    auto run_class = [&](const std::vector<uint32_t>& idx) {
       std::vector<PreparedJob> g;
       std::vector<const sqsg_job*> gs;
       for (uint32_t j : idx) {
@@ -1622,6 +1623,34 @@ static sqsg_status run_jobs(const sqsg_job* jobs, uint32_t n, sqsg_run** out, co
       std::vector<Run> runs;
       execute(g, gs, device, runs, nullptr);
       for (size_t k = 0; k < idx.size(); ++k) done[idx[k]].reset(new sqsg_run{std::move(runs[k])});
+    };
+    // Classes run from one host thread each, on their own workspaces and streams: a class's persistent
+    // kernel takes the SMs as the previous one's CTAs run out of tiles, and each class's result
+    // selection overlaps the others' kernels. Progress callbacks are promised on the calling thread,
+    // so a batch with any callback runs its classes one after another here.
+    bool callbacks = false;
+    for (uint32_t j = 0; j < n; ++j) callbacks |= jobs[j].callback != nullptr;
+    if (callbacks || classes.size() == 1) {
+      for (auto& [key, idx] : classes) run_class(idx);
+    } else {
+      std::vector<std::thread> threads;
+      std::vector<std::exception_ptr> errors(classes.size());
+      size_t k = 0;
+      for (auto& [key, idx] : classes) {
+        const std::vector<uint32_t>* ids = &idx;
+        std::exception_ptr* err = &errors[k++];
+        threads.emplace_back([&, ids, err] {
+          try {
+            CUDA_CHECK(cudaSetDevice(device));
+            run_class(*ids);
+          } catch (...) {
+            *err = std::current_exception();
+          }
+        });
+      }
+      for (auto& t : threads) t.join();
+      for (auto& e : errors)
+        if (e) std::rethrow_exception(e);
     }
     for (uint32_t j = 0; j < n; ++j) out[j] = done[j].release();
   });
