@@ -445,20 +445,34 @@ struct Outcome {
 };
 
 static void levels_from_records(const PreparedJob& pj, const std::vector<Cand>& recs, uint64_t n, Outcome& o) {
-  std::vector<std::pair<unsigned long long, uint64_t>> e(n);
-  for (uint64_t i = 0; i < n; ++i) e[i] = {ord_bits(recs[i].objective), mix64(recs[i].id)};
-  std::sort(e.begin(), e.end());
-  for (size_t i = 0; i < e.size() && o.value.size() <= pj.keep;) {
-    size_t k = i;
-    uint32_t sa = 0, sb = 0;
-    for (; k < e.size() && e[k].first == e[i].first; ++k) {
-      sa += static_cast<uint32_t>(e[k].second);
-      sb += static_cast<uint32_t>(e[k].second >> 32);
-    }
-    o.value.push_back(from_ord(e[i].first));
-    o.count.push_back(k - i);
-    o.checksum.push_back(static_cast<uint64_t>(sa) | (static_cast<uint64_t>(sb) << 32));
-    i = k;
+  // the keep+1 smallest distinct keys, ascending: one pass that inserts only keys below the current
+  // largest (rare once the array is full), then one pass that counts the records at those keys
+  const size_t m = static_cast<size_t>(pj.keep) + 1;
+  std::vector<unsigned long long> best;
+  best.reserve(m + 1);
+  for (uint64_t i = 0; i < n; ++i) {
+    const unsigned long long key = ord_bits(recs[i].objective);
+    if (best.size() == m && key >= best.back()) continue;
+    const auto it = std::lower_bound(best.begin(), best.end(), key);
+    if (it != best.end() && *it == key) continue;
+    best.insert(it, key);
+    if (best.size() > m) best.pop_back();
+  }
+  std::vector<uint64_t> count(best.size(), 0);
+  std::vector<uint32_t> sa(best.size(), 0), sb(best.size(), 0);
+  for (uint64_t i = 0; i < n && !best.empty(); ++i) {
+    const unsigned long long key = ord_bits(recs[i].objective);
+    if (key > best.back()) continue;
+    const size_t k = static_cast<size_t>(std::lower_bound(best.begin(), best.end(), key) - best.begin());
+    const unsigned long long h = mix64(recs[i].id);
+    count[k]++;
+    sa[k] += static_cast<uint32_t>(h);
+    sb[k] += static_cast<uint32_t>(h >> 32);
+  }
+  for (size_t k = 0; k < best.size(); ++k) {
+    o.value.push_back(from_ord(best[k]));
+    o.count.push_back(count[k]);
+    o.checksum.push_back(static_cast<uint64_t>(sa[k]) | (static_cast<uint64_t>(sb[k]) << 32));
   }
 }
 
