@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -241,18 +242,62 @@ static bool lattice_tables(const sqsg_sublattice& sl, LatticeTables& L) {
   for (uint32_t s = 0; s < S; ++s) {
     std::vector<std::pair<uint64_t, uint32_t>> normal, self;  // (sort key, entry)
     uint32_t pairs = 0;
+    // A class {(beta, c), (beta2, c + d)} counts the same pairs when read from either end: as beta's
+    // planes against beta2's translated by -d, or beta2's against beta's translated by +d. Each
+    // distinct (translated site, translation) costs one translation of its planes per configuration,
+    // so the ends are chosen greedily to share as few of them as possible.
+    struct Option {
+      uint32_t beta, beta2, dpack;
+      uint64_t key;  // translated site and translation
+    };
+    auto option_of = [&](uint32_t b1, uint32_t b2, uint32_t dpack) {
+      const uint32_t dx = dpack % 64, dy = (dpack / 64) % 64, dz = dpack / 4096;
+      const uint64_t tkey = (A - dx) % A + 64ull * ((B - dy) % B + 64ull * ((C - dz) % C));
+      return Option{b1, b2, dpack, b2 | (tkey << 4)};
+    };
+    auto negate = [&](uint32_t dpack) {
+      const uint32_t dx = dpack % 64, dy = (dpack / 64) % 64, dz = dpack / 4096;
+      return (A - dx) % A + 64u * ((B - dy) % B + 64u * ((C - dz) % C));
+    };
+    std::vector<std::array<Option, 2>> opts;
     for (auto& c : classes) {
       const uint32_t cs = static_cast<uint32_t>(c.key >> 26);
       if (cs != s) continue;
       const uint32_t b1 = static_cast<uint32_t>(c.key >> 22) & 0xfu, b2 = static_cast<uint32_t>(c.key >> 18) & 0xfu;
-      const uint32_t t = translation(static_cast<uint32_t>(c.key & 0x3ffffull));
-      const uint32_t en = b1 | (b2 << 4) | (t << 8);
-      // classes sharing (beta2, translation) are adjacent: their translated planes are computed once
-      const uint64_t sk = (static_cast<uint64_t>(en >> 4) << 4) | b1;
-      (c.self ? self : normal).emplace_back(sk, en);
+      const uint32_t dpack = static_cast<uint32_t>(c.key & 0x3ffffull);
       pairs += c.count;
       L.deg[s * m + b1] += 1;
       if (!c.self) L.deg[s * m + b2] += 1;
+      if (c.self) {  // its own reverse: either end gives the same entry
+        const uint32_t en = b1 | (b2 << 4) | (translation(dpack) << 8);
+        self.emplace_back((static_cast<uint64_t>(en >> 4) << 4) | b1, en);
+      } else {
+        opts.push_back({option_of(b1, b2, dpack), option_of(b2, b1, negate(dpack))});
+      }
+    }
+    std::vector<int> pick(opts.size(), -1);
+    for (size_t left = opts.size(); left > 0;) {
+      std::map<uint64_t, uint32_t> freq;
+      for (size_t k = 0; k < opts.size(); ++k)
+        if (pick[k] < 0) {
+          freq[opts[k][0].key]++;
+          if (opts[k][1].key != opts[k][0].key) freq[opts[k][1].key]++;
+        }
+      uint64_t best = 0;
+      uint32_t best_n = 0;
+      for (auto& [key, cnt] : freq)  // most shared first; ties: the smaller key (deterministic)
+        if (cnt > best_n) best = key, best_n = cnt;
+      for (size_t k = 0; k < opts.size(); ++k)
+        if (pick[k] < 0 && (opts[k][0].key == best || opts[k][1].key == best)) {
+          pick[k] = opts[k][0].key == best ? 0 : 1;
+          --left;
+        }
+    }
+    for (size_t k = 0; k < opts.size(); ++k) {
+      const Option& o = opts[k][pick[k]];
+      const uint32_t en = o.beta | (o.beta2 << 4) | (translation(o.dpack) << 8);
+      // classes sharing (beta2, translation) are adjacent: their translated planes are computed once
+      normal.emplace_back((static_cast<uint64_t>(en >> 4) << 4) | o.beta, en);
     }
     std::sort(normal.begin(), normal.end());
     std::sort(self.begin(), self.end());
