@@ -233,76 +233,36 @@ __device__ __forceinline__ T objective_part(uint8_t* smem, const PartDesc& P, in
   return obj;
 }
 
-
-// Fisher-Yates over the window [lo, lo + n) of a lane's column (core/shuffle.h:39-50): for i = n..2,
-// swap positions i-1 and p = (x * i) >> 32 (core/shuffle.h:28-32) for the next word x of `words`.
-// The steps form a chain through shared memory (a step's stores may feed the next step's loads), so
-// the loads of step i-1 are issued before the stores of step i and the two ways they can alias are
-// forwarded in registers: the next top (position i-2) or the next random position equals this step's
-// p. (Neither can be position i-1, which the next step never touches.) The result is the plain
-// sequential swap order's; only the shared-memory latency of each step overlaps the previous one.
-template <class Words>
-__device__ __forceinline__ void fisher_yates(uint8_t* col, uint32_t lo, uint32_t n, Words& words) {
-  if (n < 2) return;
-  uint32_t i = n;
-  uint32_t a = site_off(lo + i - 1), b = site_off(lo + __umulhi(words(), i));
-  uint8_t top = col[a], vb = col[b];
-  for (;;) {
-    const uint8_t va = top;
-    if (i == 2) {
-      col[a] = vb;
-      col[b] = va;
-      return;
-    }
-    const uint32_t an = site_off(lo + i - 2), bn = site_off(lo + __umulhi(words(), i - 1));
-    uint8_t topn = col[an], vbn = col[bn];  // loaded before this step's stores
-    col[a] = vb;
-    col[b] = va;
-    topn = an == b ? va : topn;
-    vbn = bn == b ? va : vbn;
-    --i;
-    a = an;
-    b = bn;
-    top = topn;
-    vb = vbn;
-  }
+__device__ __forceinline__ void swap_draw(uint8_t* col, uint32_t lo, uint32_t i, uint32_t x) {
+  const uint32_t p = __umulhi(x, i);  // (x * i) >> 32, core/shuffle.h:28-32 on a Philox word
+  const uint32_t a = site_off(lo + i - 1), b = site_off(lo + p);
+  const uint8_t va = col[a], vb = col[b];
+  col[a] = vb;
+  col[b] = va;
 }
 
-// Philox4x32-10 words, four per call: counter (block, iteration, chain, part), key = seed. The words
-// of a call are handed out in order by shifting (no indexed array: it would live in local memory).
-struct PhiloxWords {
-  uint32_t blk, it, c_lo, c_hi, k0, k1, left;
-  uint32_t w0, w1, w2, w3;
-  __device__ __forceinline__ uint32_t operator()() {
-    if (left == 0) {
-      const philox_ctr r = philox4x32_10(philox_ctr{blk++, it, c_lo, c_hi}, k0, k1);
-      w0 = r.x;
-      w1 = r.y;
-      w2 = r.z;
-      w3 = r.w;
-      left = 4;
-    }
-    const uint32_t x = w0;
-    w0 = w1;
-    w1 = w2;
-    w2 = w3;
-    --left;
-    return x;
-  }
-};
-
 // core/shuffle.h:39-50 with Philox4x32-10 words: counter (block, iteration, chain, part), key = seed.
-// Every window draws from a fresh block of four words (the stream the bit-mask path uses as well).
 __device__ __forceinline__ void shuffle_part(uint8_t* smem, const PartDesc& P, int t, uint32_t it,
                                              unsigned long long chain, uint32_t part, uint32_t k0, uint32_t k1) {
   uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
   const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
-  PhiloxWords words{0u, it, static_cast<uint32_t>(chain), (static_cast<uint32_t>(chain >> 32) << 8) | part,
-                    k0, k1, 0u, 0u, 0u, 0u, 0u};
+  const uint32_t c_lo = static_cast<uint32_t>(chain);
+  const uint32_t c_hi = (static_cast<uint32_t>(chain >> 32) << 8) | part;
+  uint32_t blk = 0;
   for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
     const uint32_t lo = win[2 * wi];
-    words.left = 0;  // a window starts on a fresh block (blk continues)
-    fisher_yates(col, lo, win[2 * wi + 1] - lo, words);
+    uint32_t i = win[2 * wi + 1] - lo;
+    while (i > 1) {
+      const philox_ctr r = philox4x32_10(philox_ctr{blk++, it, c_lo, c_hi}, k0, k1);
+      swap_draw(col, lo, i, r.x);
+      if (--i <= 1) break;
+      swap_draw(col, lo, i, r.y);
+      if (--i <= 1) break;
+      swap_draw(col, lo, i, r.z);
+      if (--i <= 1) break;
+      swap_draw(col, lo, i, r.w);
+      --i;
+    }
   }
 }
 
@@ -320,19 +280,13 @@ __device__ __forceinline__ uint32_t rapid_next(unsigned long long& s) {
   return static_cast<uint32_t>((s * b) ^ __umul64hi(s, b));
 }
 
-struct RapidWords {
-  unsigned long long& s;
-  __device__ __forceinline__ uint32_t operator()() { return rapid_next(s); }
-};
-
 // core/shuffle.h:39-50 on the reference's stream: Fisher-Yates per window, one word per step.
 __device__ __forceinline__ void shuffle_part_rapid(uint8_t* smem, const PartDesc& P, int t, unsigned long long& s) {
   uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
   const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
-  RapidWords words{s};
   for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
     const uint32_t lo = win[2 * wi];
-    fisher_yates(col, lo, win[2 * wi + 1] - lo, words);
+    for (uint32_t i = win[2 * wi + 1] - lo; i > 1; --i) swap_draw(col, lo, i, rapid_next(s));
   }
 }
 
