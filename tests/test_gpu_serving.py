@@ -15,9 +15,23 @@ from sqsgenerator_b200.optimize import build_job
 pytestmark = pytest.mark.gpu
 
 
+def _fcc555(**kw):
+    """fcc 5x5x5 (500 sites, 125 cells: the two-word lattice path), three species."""
+    cfg = cases.fcc32("double", composition={"Ti": 167, "Al": 167, "Nb": 166}, **kw)
+    cfg["structure"]["supercell"] = [5, 5, 5]
+    return cfg
+
+
+def _senary(**kw):
+    """fcc 3x3x3 (108 sites) with six species: the eight-species lattice kernel."""
+    return cases.quinary("double", composition={e: 18 for e in ("Ti", "Al", "Nb", "V", "Zr", "Hf")}, **kw)
+
+
 def mix():
-    """Uneven jobs: sizes, species, shells, modes and precisions differ."""
+    """Uneven jobs: sizes, species, shells, modes, precisions and kernels differ."""
     return [
+        _fcc555(iterations=30000, seed=8, keep=3),
+        _senary(iterations=30000, seed=9, keep=4),
         cases.fcc32("double", iterations=300000, seed=1, pair_weights=None),
         cases.quinary("double", iterations=40000, seed=2),
         cases.settings_16("single"),

@@ -128,6 +128,9 @@ LATTICE_CASES = {
     "fcc_445_quaternary_single": lambda: fcc((4, 4, 5), {"Ti": 80, "Al": 80, "Nb": 80, "V": 80}, 3, prec="single",
                                              iterations=60000, seed=43, keep=4),
     "fcc500_binary": lambda: fcc((5, 5, 5), {"Ti": 250, "Al": 250}, 2, iterations=60000, seed=44, keep=5),
+    "rocksalt_445_split": lambda: cases.rocksalt_split("double", cells=(4, 4, 5), iterations=40000, seed=45, keep=4,
+                                                      composition=[{"sites": "Na", "Ti": 160, "Al": 160},
+                                                                   {"sites": "Cl", "N": 280, "B": 40}]),
     # six and eight species: the eight-species variant of the lattice path (sqsg_engine_lat)
     "fcc_333_senary": lambda: fcc((3, 3, 3), {"Ti": 18, "Al": 18, "Nb": 18, "V": 18, "Zr": 18, "Hf": 18}, 2,
                                   iterations=100000, seed=31, keep=5),
@@ -143,7 +146,8 @@ LATTICE_KERNELS = {"config3": "sqsg_engine_lat5", "config4": "sqsg_engine_lat2",
                    "rocksalt_interact": "sqsg_engine_lat5", "bcc_4x4x2_quaternary": "sqsg_engine_lat5",
                    "fcc_333_senary": "sqsg_engine_lat", "bcc_444_octonary": "sqsg_engine_lat",
                    "fcc500_ternary_4shells": "sqsg_engine_latw", "bcc250_quinary": "sqsg_engine_latw",
-                   "fcc_445_quaternary_single": "sqsg_engine_latw", "fcc500_binary": "sqsg_engine_latw"}
+                   "fcc_445_quaternary_single": "sqsg_engine_latw", "fcc500_binary": "sqsg_engine_latw",
+                   "rocksalt_445_split": "sqsg_engine_latw"}
 
 
 @pytest.mark.parametrize("name", sorted(LATTICE_CASES))
