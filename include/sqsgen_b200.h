@@ -372,7 +372,7 @@ sqsg_status sqsg_server_submit(sqsg_server* server, const sqsg_job* job, uint64_
 sqsg_status sqsg_server_wait(sqsg_server* server, uint64_t ticket, int64_t timeout_us, sqsg_run** run);
 sqsg_status sqsg_server_stats(sqsg_server* server, sqsg_server_counters* stats);
 /* Persistent-kernel launches still running. CTAs leave after a bounded number of empty polls of
- * their ring (about 0.5 ms), so this drops to 0 soon after the server runs out of work. */
+ * their ring (about 5 ms), so this drops to 0 soon after the server runs out of work. */
 sqsg_status sqsg_server_running(sqsg_server* server, uint32_t* launches);
 sqsg_status sqsg_server_destroy(sqsg_server* server);
 

@@ -985,9 +985,9 @@ static int ring_top_occupancy(int kind) {
 constexpr int kMaxSm = 256;
 constexpr size_t kOnesBytes = 1u << 20;  // pinned 0xff source of distinct-configuration table resets
 constexpr uint64_t kRingCap = 1u << 20;
-constexpr uint32_t kIdlePolls = 250;          // ~0.5 ms of empty polls before a CTA leaves its ring
+constexpr uint32_t kIdlePolls = 2500;         // ~5 ms of empty polls before a CTA leaves its ring
 constexpr int kLaunchSlots = 32;              // concurrent launches per ring
-constexpr uint64_t kRepartitionNs = 2000000;  // at most one SM repartition per 2 ms
+constexpr uint64_t kRepartitionNs = 5000000;  // at most one SM repartition per 5 ms
 constexpr uint64_t kRelaunchNs = 1000000;     // at most one top-up launch per ring per ms
 constexpr uint8_t kNoOwner = 0xff;
 constexpr int kReservedSm = 2;                // SMs left to no ring: result selection runs there
