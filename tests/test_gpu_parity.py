@@ -262,7 +262,7 @@ def test_random_records_bit_exact_and_deduplicated():
 @pytest.mark.parametrize("cell,prec,keep,cap", [("fcc32", "double", 3, None), ("fcc32", "double", 10, 7),
                                                 ("fcc32", "single", 5, 2), ("fcc32", "double", 64, None),
                                                 ("fcc32", "single", 100, 3), ("quinary", "double", 100, None),
-                                                ("quinary", "single", 64, 1)])
+                                                ("quinary", "single", 64, 1), ("quinary", "double", 1023, None)])
 def test_random_result_set_from_full_trace(cell, prec, keep, cap):
     """Every evaluation of a random run is traced; the result set must equal the rule restated here on
     the trace: the keep+1 smallest distinct objectives, one record per distinct configuration (the
