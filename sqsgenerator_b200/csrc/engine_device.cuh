@@ -241,28 +241,17 @@ __device__ __forceinline__ void swap_draw(uint8_t* col, uint32_t lo, uint32_t i,
   col[b] = va;
 }
 
-// core/shuffle.h:39-50 with Philox4x32-10 words: counter (block, iteration, chain, part), key = seed.
+// core/shuffle.h:39-50 with the words of shuffle_words (philox.cuh): a xoshiro128** generator seeded
+// by the Philox4x32-10 block of (seed; iteration, chain, part); the windows draw one after another.
 __device__ __forceinline__ void shuffle_part(uint8_t* smem, const PartDesc& P, int t, uint32_t it,
                                              unsigned long long chain, uint32_t part, uint32_t k0, uint32_t k1) {
   uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
   const uint32_t* win = reinterpret_cast<const uint32_t*>(part_base(smem, P) + P.win_off);
-  const uint32_t c_lo = static_cast<uint32_t>(chain);
-  const uint32_t c_hi = (static_cast<uint32_t>(chain >> 32) << 8) | part;
-  uint32_t blk = 0;
+  xoshiro128ss words =
+      shuffle_words(it, static_cast<uint32_t>(chain), (static_cast<uint32_t>(chain >> 32) << 8) | part, k0, k1);
   for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
     const uint32_t lo = win[2 * wi];
-    uint32_t i = win[2 * wi + 1] - lo;
-    while (i > 1) {
-      const philox_ctr r = philox4x32_10(philox_ctr{blk++, it, c_lo, c_hi}, k0, k1);
-      swap_draw(col, lo, i, r.x);
-      if (--i <= 1) break;
-      swap_draw(col, lo, i, r.y);
-      if (--i <= 1) break;
-      swap_draw(col, lo, i, r.z);
-      if (--i <= 1) break;
-      swap_draw(col, lo, i, r.w);
-      --i;
-    }
+    for (uint32_t i = win[2 * wi + 1] - lo; i > 1; --i) swap_draw(col, lo, i, words.next());
   }
 }
 
@@ -925,27 +914,19 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
     const bool active = it < my_count;
     T total = T(0);
     if (active) {
-      if (!systematic) {  // core/shuffle.h:39-50 on bits, same Philox words as the general path
+      if (!systematic) {  // core/shuffle.h:39-50 on bits, the same words as the general path
         const uint64_t cid = tile.start + my_off + it;
-        const uint32_t c_lo = static_cast<uint32_t>(cid), c_hi = static_cast<uint32_t>(cid >> 32) << 8;
-        uint32_t blk = 0;
+        xoshiro128ss words =
+            shuffle_words(0u, static_cast<uint32_t>(cid), static_cast<uint32_t>(cid >> 32) << 8, k0, k1);
         v = v0;
         for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
           const uint32_t lo = win[2 * wi];
-          uint32_t i = win[2 * wi + 1] - lo;
           const uint32_t top = N - 1 - lo;  // bit of the window's first site
-          while (i > 1) {
-            const philox_ctr r = philox4x32_10(philox_ctr{blk++, 0u, c_lo, c_hi}, k0, k1);
-            const uint32_t xs[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              if (i <= 1) break;
-              const uint32_t pp = __umulhi(xs[q], i);
-              const uint32_t ba = top - (i - 1), bb = top - pp;
-              const V dlt = ((v >> ba) ^ (v >> bb)) & V(1);
-              v ^= (dlt << ba) | (dlt << bb);
-              --i;
-            }
+          for (uint32_t i = win[2 * wi + 1] - lo; i > 1; --i) {
+            const uint32_t pp = __umulhi(words.next(), i);
+            const uint32_t ba = top - (i - 1), bb = top - pp;
+            const V dlt = ((v >> ba) ^ (v >> bb)) & V(1);
+            v ^= (dlt << ba) | (dlt << bb);
           }
         }
       }

@@ -1,8 +1,8 @@
-"""Test-side Philox4x32-10 (Salmon et al., SC'11) and the Fisher-Yates chain the device runs.
+"""Test-side Philox4x32-10 (Salmon et al., SC'11), xoshiro128** and the Fisher-Yates shuffle the device runs.
 
-Used to predict, configuration by configuration, what the random mode evaluates: configuration g of
-a job is the (g - c)-th shuffle of the chain that starts at index c, each shuffle drawing Philox words
-with counter (block, iteration, chain_lo, chain_hi << 8 | part) and key (seed_lo, seed_hi), bounded
+Used to predict, configuration by configuration, what the random mode evaluates: configuration g of a job
+is the Fisher-Yates shuffle of the packed arrangement whose words come from a xoshiro128** generator seeded
+with the Philox block of counter (0, iteration, g_lo, g_hi << 8 | part) and key (seed_lo, seed_hi), bounded
 like core/shuffle.h:28-32 of the reference: p = (x * i) >> 32.
 """
 M0, M1 = 0xD2511F53, 0xCD9E8D57
@@ -30,22 +30,43 @@ def philox4x32_10(ctr, key):
     return c0, c1, c2, c3
 
 
+def rotl32(x, k):
+    return ((x << k) | (x >> (32 - k))) & MASK
+
+
+class Xoshiro128ss:
+    """xoshiro128** (Blackman and Vigna, ACM TOMS 2021): 128-bit state, 32-bit outputs."""
+
+    def __init__(self, s):
+        self.s = list(s)
+        if not any(self.s):
+            self.s[0] = 1
+
+    def next(self):
+        s0, s1, s2, s3 = self.s
+        r = (rotl32((s1 * 5) & MASK, 7) * 9) & MASK
+        t = (s1 << 9) & MASK
+        s2 ^= s0
+        s3 ^= s1
+        s1 ^= s2
+        s0 ^= s3
+        s2 ^= t
+        s3 = rotl32(s3, 11)
+        self.s = [s0, s1, s2, s3]
+        return r
+
+
 def shuffle(species, windows, seed, chain, iteration, part=0):
-    """One Fisher-Yates pass over every window, in place on a list."""
+    """One Fisher-Yates pass over every window, in place on a list: the words come from a xoshiro128**
+    generator whose state is the Philox4x32-10 block of counter (0, iteration, chain_lo,
+    chain_hi << 8 | part) and key (seed_lo, seed_hi)."""
     k = (seed & MASK, (seed >> 32) & MASK)
     c_lo = chain & MASK
     c_hi = (((chain >> 32) << 8) | part) & MASK
-    blk = 0
+    gen = Xoshiro128ss(philox4x32_10((0, iteration & MASK, c_lo, c_hi), k))
     for lo, hi in windows:
-        i = hi - lo
-        while i > 1:
-            words = philox4x32_10((blk, iteration & MASK, c_lo, c_hi), k)
-            blk += 1
-            for x in words:
-                if i <= 1:
-                    break
-                p = (x * i) >> 32
-                a, b = lo + i - 1, lo + p
-                species[a], species[b] = species[b], species[a]
-                i -= 1
+        for i in range(hi - lo, 1, -1):
+            p = (gen.next() * i) >> 32
+            a, b = lo + i - 1, lo + p
+            species[a], species[b] = species[b], species[a]
     return species
