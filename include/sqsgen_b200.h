@@ -162,7 +162,8 @@ typedef struct {
                                  reference's block size in the "rapidrand" debug mode */
   uint64_t keep;              /* the reference's `keep` (1..1023 in this build) */
   int64_t max_results_per_objective; /* < 0: unset */
-  uint64_t seed;              /* random mode: Philox key (rapidrand seed in the "rapidrand" debug mode) */
+  uint64_t seed;              /* random mode: key of the Philox4x32-10 blocks that seed each configuration's
+                                 shuffle words (rapidrand seed in the "rapidrand" debug mode) */
   int32_t has_seed;           /* 0: a random seed is drawn */
   int32_t device;             /* CUDA device ordinal */
   const volatile int32_t* cancel; /* optional: set non-zero from any thread to stop early */
@@ -250,7 +251,7 @@ sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t ca
  *                              truncated (sqsg_run_info) and the objective levels stay exact.
  *   "rapidrand"          0/1   debug (default 0): random jobs follow the reference's seeded
  *                              single-thread run (core/shuffle.h:23-50 with rapidhash's rapidrand,
- *                              blocks of chunk_size, sqs.h:348-466) instead of the Philox stream; each
+ *                              blocks of chunk_size, sqs.h:348-466) instead of this library's stream; each
  *                              block runs as one chain on one GPU thread, so a job has only
  *                              iterations / chunk_size-way parallelism. Configuration ids are the
  *                              reference's iteration indices. Pair-stream path only; sqsg_optimize,

@@ -426,7 +426,7 @@ static RecordLayout record_layout(const PreparedJob& pj) {
 //    the threshold was still high). Then, if the record buffer held every candidate, the levels are
 //    rebuilt from the records: every evaluation at or below the threshold of its time — so every
 //    evaluation at or below T* — is a record.
-//  - A record buffer that overflowed asks for a re-run (same tiles, same Philox counters, same
+//  - A record buffer that overflowed asks for a re-run (same tiles, same seeds and ids, same
 //    evaluations) whose threshold starts at T* (exact levels: the buffer is sized from their counts)
 //    or at the (keep+1)-th distinct objective of the stored records, an upper bound of T*.
 //  - When the evaluations at or below T* are too many for any buffer but the random job's
@@ -958,7 +958,7 @@ static void execute(std::vector<PreparedJob>& pjs, const std::vector<const sqsg_
 // tail; the bucket's persistent kernel, already running other jobs' tiles, picks them up. The CTA
 // that finishes a job's last tile marks the job's slot done in host-mapped memory; the worker then
 // downloads its records and levels, selects the result set and wakes the waiting caller. A job's
-// result does not depend on what else runs: its tiles and Philox counters depend only on the job.
+// result does not depend on what else runs: its tiles and random words depend only on the job.
 // One ring per (kernel, occupancy level): ring 0 runs sqsg_engine_mask at 5 CTAs per SM and takes
 // binary bit-mask jobs; rings 1-4 run sqsg_engine_wide at 4, 3, 2, 1 CTAs per SM; rings 5-6 run
 // sqsg_engine_lat2 at 4 and 2, rings 7-8 sqsg_engine_lat5 at 3 and 1, rings 9-10 sqsg_engine_lat at 2

@@ -1,7 +1,7 @@
 // Device engine of the SQS optimisation: job/tile descriptors and the persistent tile kernel.
 //
 // One CTA of kBlock threads works on one tile at a time. A tile is a slice of one job's
-// configuration space: in random mode kBlock independent Philox chains, in systematic mode a
+// configuration space: in random mode kBlock independent shuffles per step, in systematic mode a
 // contiguous interval of 1-based permutation ranks. Every thread owns one configuration at a time,
 // stored as one byte per site in its own column of shared memory. Bond counting walks a per-shell,
 // per-site grouped pair stream that every lane reads at the same address (a shared-memory

@@ -2,8 +2,9 @@
 //
 // Per configuration a thread
 //   1. (random mode) Fisher-Yates-shuffles every window of every part of the packed initial
-//      arrangement with Philox4x32-10 draws (key = seed, counter = (draw block, 0, configuration id,
-//      part)) and the reference's bounded draw p = (x * i) >> 32 (include/sqsgen/core/shuffle.h:28-50);
+//      arrangement with the words of a xoshiro128** generator seeded by one Philox4x32-10 block
+//      (key = seed, counter = (0, 0, configuration id, part); philox.cuh) and the reference's bounded
+//      draw p = (x * i) >> 32 (include/sqsgen/core/shuffle.h:28-50);
 //   2. counts ordered bonds (s, species[i], species[j]) over the part's pairs (optimization.h:74-77);
 //   3. evaluates the objective in T with the reference's loop order and no FMA contraction
 //      (optimization.h:79-103), summing parts left to right from T(0) (sqs.h:417-418, fold.h:51-53);
@@ -234,7 +235,7 @@ __device__ __forceinline__ T objective_part(uint8_t* smem, const PartDesc& P, in
 }
 
 __device__ __forceinline__ void swap_draw(uint8_t* col, uint32_t lo, uint32_t i, uint32_t x) {
-  const uint32_t p = __umulhi(x, i);  // (x * i) >> 32, core/shuffle.h:28-32 on a Philox word
+  const uint32_t p = __umulhi(x, i);  // (x * i) >> 32, core/shuffle.h:28-32 on a 32-bit word
   const uint32_t a = site_off(lo + i - 1), b = site_off(lo + p);
   const uint8_t va = col[a], vb = col[b];
   col[a] = vb;
@@ -701,9 +702,9 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
   const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
   const uint64_t max_count = base + (rem ? 1 : 0);
   constexpr bool systematic = SYS;  // J.mode == 1
-  // random mode: configuration id is the Philox Fisher-Yates shuffle, with counter id, of the
-  // packed initial arrangement; it depends on nothing but (seed, id), so any split of the job into
-  // tiles, launches or devices evaluates the same configurations
+  // random mode: configuration id is the Fisher-Yates shuffle of the packed initial arrangement with
+  // the words seeded by (seed, id) (shuffle_words); it depends on nothing but (seed, id), so any split
+  // of the job into tiles, launches or devices evaluates the same configurations
   const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
 
   for (uint32_t p = 0; p < J.n_parts; ++p) init_column(smem, J.parts[p], t);

@@ -372,8 +372,9 @@ def test_fcc32_systematic_full_space_levels(prec):
 @pytest.mark.parametrize("composition", [{"Ti": 16, "Al": 16}, {"Ti": 11, "Al": 11, "Nb": 10}],
                          ids=["binary_fast_path", "ternary_general_path"])
 def test_random_stream_is_philox_fisher_yates(composition):
-    """Configuration g is the Philox Fisher-Yates shuffle, with counter g, of the packed initial
-    arrangement: it depends on (seed, g) alone, not on tiles, launches or devices."""
+    """Configuration g is the Fisher-Yates shuffle of the packed initial arrangement with xoshiro128** words
+    seeded by the Philox block of counter g (tests/philox_ref.py): it depends on (seed, g) alone, not on
+    tiles, launches or devices."""
     import philox_ref
 
     total = 2_097_153

@@ -1,5 +1,5 @@
 """Reference-stream debug mode (option "rapidrand"): random jobs follow the reference's seeded
-single-thread run instead of the Philox stream. Its words come from rapidrand (core/shuffle.h:23-32);
+single-thread run instead of this library's stream. Its words come from rapidrand (core/shuffle.h:23-32);
 the work is split into thread-pool blocks of chunk_size configurations (sqs.h:461-466) that restart
 from the packed arrangement (sqs.h:374) while the stream continues; interact mode evaluates and then
 shuffles (sqs.h:397-403,439-440), split mode shuffles every sublattice and then evaluates
