@@ -5,6 +5,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cstddef>
 #include <cstring>
 #include <system_error>
@@ -13,10 +14,31 @@
 
 namespace sqsg {
 
+// Helper threads of all copies in flight share one budget (half the host's hardware threads, at most
+// 8), so that concurrent callers (a server's finalizers) do not oversubscribe the host and starve the
+// threads that feed the GPU.
+inline std::atomic<int>& copy_threads_in_use() {
+  static std::atomic<int> n{0};
+  return n;
+}
+
 inline void parallel_copy(void* dst, const void* src, size_t bytes) {
   constexpr size_t kMinPerThread = 4u << 20;
-  const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency() / 2);
-  const size_t n = std::min<size_t>({8, hw, bytes / kMinPerThread});
+  const int budget = static_cast<int>(std::min<size_t>(8, std::max<size_t>(1, std::thread::hardware_concurrency() / 2)));
+  size_t want = std::min<size_t>(static_cast<size_t>(budget), bytes / kMinPerThread);
+  int helpers = 0;  // helper threads reserved from the budget (the caller copies one share itself)
+  if (want > 1) {
+    int used = copy_threads_in_use().load();
+    for (;;) {
+      helpers = std::min<int>(static_cast<int>(want) - 1, budget - used);
+      if (helpers <= 0) {
+        helpers = 0;
+        break;
+      }
+      if (copy_threads_in_use().compare_exchange_weak(used, used + helpers)) break;
+    }
+  }
+  const size_t n = static_cast<size_t>(helpers) + 1;
   if (n <= 1) {
     std::memcpy(dst, src, bytes);
     return;
@@ -36,6 +58,7 @@ inline void parallel_copy(void* dst, const void* src, size_t bytes) {
   std::memcpy(dst, src, std::min(per, bytes));
   if (done < bytes) std::memcpy(static_cast<char*>(dst) + done, static_cast<const char*>(src) + done, bytes - done);
   for (auto& t : th) t.join();
+  copy_threads_in_use().fetch_sub(helpers);
 }
 
 }  // namespace sqsg
