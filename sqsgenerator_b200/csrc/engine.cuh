@@ -173,12 +173,13 @@ struct PartDesc {
 };
 
 // A translation of the cell grid (bit c = x + A*(y + B*z)) by (dx, dy, dz), as rotations inside rows
-// of A bits, blocks of A*B bits and the whole grid; a zero shift skips its stage. Masks have two words
-// (cell sets of up to 128 cells); sets of up to 64 cells use the first.
-struct LatTr {
+// of A bits, blocks of A*B bits and the whole grid; a zero shift skips its stage. The masks have one
+// 64-bit word per word of the job's cell sets (W = lat_words): the staged table holds LatTrW<W>.
+template <int W> struct LatTrW {
   uint32_t sx, sxr, sy, syr, sz, szr, pad0, pad1;
-  unsigned long long mxh[2], mxl[2], myh[2], myl[2];
+  unsigned long long mxh[W], mxl[W], myh[W], myl[W];
 };
+using LatTr = LatTrW<2>;  // the host's working form (written out at the job's width)
 
 struct JobDesc {
   uint32_t prec;          // 0 float, 1 double

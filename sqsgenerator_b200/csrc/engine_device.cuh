@@ -1042,7 +1042,7 @@ template <int W> __device__ __forceinline__ LatBits<W> lat_shr(const LatBits<W>&
 // Translation of a cell set by (tx, ty, tz): rotations inside rows of A bits, blocks of A*B bits and
 // the whole grid of A*B*C bits (masks select the cells that wrap); a zero shift skips its stage.
 template <int W>
-__device__ __forceinline__ LatBits<W> lat_translate(LatBits<W> v, const LatTr* t, const LatBits<W>& full) {
+__device__ __forceinline__ LatBits<W> lat_translate(LatBits<W> v, const LatTrW<W>* t, const LatBits<W>& full) {
   if (t->sx) {
     const LatBits<W> h = lat_shl<W>(v, t->sx), l = lat_shr<W>(v, t->sxr);
 #pragma unroll
@@ -1145,7 +1145,7 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
   const unsigned long long* X = reinterpret_cast<const unsigned long long*>(part + P.lat_planes_off) + t;
   const uint32_t* ent = reinterpret_cast<const uint32_t*>(part + P.lat_ent_off);
   const uint4* shl = reinterpret_cast<const uint4*>(part + P.lat_shell_off);
-  const LatTr* trs = reinterpret_cast<const LatTr*>(part + P.lat_tr_off);
+  const LatTrW<W>* trs = reinterpret_cast<const LatTrW<W>*>(part + P.lat_tr_off);
   const uint32_t* deg = reinterpret_cast<const uint32_t*>(part + P.lat_deg_off);
   const uint32_t K = P.n_species, km1 = K - 1, S = P.n_shells, m = P.lat_basis;
   const LatBits<W> full = lat_full<W>(P);
@@ -1174,7 +1174,7 @@ __device__ __forceinline__ T lat_objective(uint8_t* smem, const PartDesc& P, int
       if ((en >> 4) != key) {  // (beta2, translation) changed: translate beta2's planes
         key = en >> 4;
         const uint32_t b2 = key & 0xfu;
-        const LatTr* tr = trs + (key >> 4);
+        const LatTrW<W>* tr = trs + (key >> 4);
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
           if (a >= static_cast<int>(km1)) break;

@@ -586,7 +586,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       P.lat_shell_off = static_cast<uint32_t>(off);
       off = align_up(off + 4 * LT.shell.size(), 16);
       P.lat_tr_off = static_cast<uint32_t>(off);
-      off = align_up(off + sizeof(LatTr) * LT.tr.size(), 16);
+      off = align_up(off + (LT.words == 1 ? sizeof(LatTrW<1>) : sizeof(LatTrW<2>)) * LT.tr.size(), 16);
       P.lat_deg_off = static_cast<uint32_t>(off);
       off = align_up(off + 4 * LT.deg.size(), 16);
       planes = static_cast<size_t>(LT.m) * (sl.n_species - 1) * 8 * LT.words * kBlock;
@@ -735,7 +735,15 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       std::memcpy(base + P.lat_site_off, LT.site_off.data(), 4 * LT.site_off.size());
       std::memcpy(base + P.lat_ent_off, LT.ent.data(), 4 * LT.ent.size());
       std::memcpy(base + P.lat_shell_off, LT.shell.data(), 4 * LT.shell.size());
-      std::memcpy(base + P.lat_tr_off, LT.tr.data(), sizeof(LatTr) * LT.tr.size());
+      if (LT.words == 2) {
+        std::memcpy(base + P.lat_tr_off, LT.tr.data(), sizeof(LatTrW<2>) * LT.tr.size());
+      } else {  // one-word cell sets: the masks' first words only
+        for (size_t k = 0; k < LT.tr.size(); ++k) {
+          const LatTr& t = LT.tr[k];
+          const LatTrW<1> o{t.sx, t.sxr, t.sy, t.syr, t.sz, t.szr, 0u, 0u, {t.mxh[0]}, {t.mxl[0]}, {t.myh[0]}, {t.myl[0]}};
+          std::memcpy(base + P.lat_tr_off + k * sizeof(LatTrW<1>), &o, sizeof(o));
+        }
+      }
       std::memcpy(base + P.lat_deg_off, LT.deg.data(), 4 * LT.deg.size());
     }
   }
