@@ -990,7 +990,7 @@ constexpr int kLaunchSlots = 32;              // concurrent launches per ring
 constexpr uint64_t kRepartitionNs = 5000000;  // at most one SM repartition per 5 ms
 constexpr uint64_t kRelaunchNs = 1000000;     // at most one top-up launch per ring per ms
 constexpr uint8_t kNoOwner = 0xff;
-constexpr int kReservedSm = 2;                // SMs left to no ring: result selection runs there
+constexpr int kReservedSm = 16;               // SMs left to no ring: result selection runs there
 constexpr double kTilePairs = 1u << 19;       // estimated pair evaluations per thread and tile, at most
 
 struct ServerJob {
