@@ -257,6 +257,12 @@ sqsg_status sqsg_optimize_trace(const sqsg_job* job, sqsg_run** run, uint64_t ca
  *                              reference's iteration indices. Pair-stream path only; sqsg_optimize,
  *                              sqsg_optimize_batch and traces only (not the server, not ranges).
  *   "server_finalizers"  > 0   result-selection threads of servers created afterwards (default 4).
+ *   "binary_floyd"       0/1   1 (default): in random mode a shuffle window that holds exactly two
+ *                              species draws the sites of its rarer species (Floyd's sampling: m
+ *                              draws for m such sites) instead of n - 1 Fisher-Yates swaps; both give
+ *                              every arrangement of the window the same probability. 0: Fisher-Yates
+ *                              on every window. Read when a job is prepared; it selects the stream,
+ *                              so results of one seed differ between the two settings.
  * Unknown names give SQSG_ERR_INVALID_ARGUMENT. */
 sqsg_status sqsg_set_option(const char* name, int64_t value);
 sqsg_status sqsg_get_option(const char* name, int64_t* value);

@@ -42,10 +42,10 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 // ------------------------------------------------------------------------------------------------
 // Process-wide options
 static std::atomic<long long> g_options[kOptCount] = {{0}, {static_cast<long long>(kWaitNs)}, {0}, {1},
-                                                      {1ll << 20}, {4ll << 30}, {0}, {4}};
+                                                      {1ll << 20}, {4ll << 30}, {0}, {4}, {1}};
 static const char* const kOptionNames[kOptCount] = {"force_general", "stage_wait_ns", "debug_skip_staging",
                                                     "use_tuning", "default_candidates", "rerun_record_bytes",
-                                                    "rapidrand", "server_finalizers"};
+                                                    "rapidrand", "server_finalizers", "binary_floyd"};
 
 long long option(Option o) { return g_options[o].load(std::memory_order_relaxed); }
 

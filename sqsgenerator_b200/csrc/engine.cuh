@@ -127,7 +127,7 @@ struct PartDesc {
   uint32_t smem_off;      // part base in dynamic shared memory
   // offsets inside the staged section (identical in the blob and in shared memory)
   uint32_t cube_off;      // prefactors, pair weights, targets: 3 x S*K*K of T
-  uint32_t win_off;       // 2 x n_windows u32
+  uint32_t win_off;       // 2 x n_windows u32 bounds [lo, hi), then n_windows u32 draw words (see shuffle_part)
   uint32_t stream_off;    // stream u32 words
   uint32_t species_off;   // N packed species codes (8 * species index)
   // shared-memory-only regions, relative to the part base
@@ -169,7 +169,7 @@ struct PartDesc {
   unsigned long long dd_stride;
   // reference-stream debug mode: random words one shuffle of the part draws (sum over windows of n_w - 1)
   uint32_t chain_draws;
-  uint32_t chain_pad;
+  uint32_t ones;          // sites of species 1 (two-species parts: the binary path's minority count)
 };
 
 // A translation of the cell grid (bit c = x + A*(y + B*z)) by (dx, dy, dz), as rotations inside rows

@@ -4,7 +4,8 @@
 //   1. (random mode) Fisher-Yates-shuffles every window of every part of the packed initial
 //      arrangement with the words of a xoshiro128** generator seeded by one Philox4x32-10 block
 //      (key = seed, counter = (0, 0, configuration id, part); philox.cuh) and the reference's bounded
-//      draw p = (x * i) >> 32 (include/sqsgen/core/shuffle.h:28-50);
+//      draw p = (x * i) >> 32 (include/sqsgen/core/shuffle.h:28-50); a window of two species draws
+//      its rarer species' sites by Floyd's sampling instead (same distribution, fewer draws);
 //   2. counts ordered bonds (s, species[i], species[j]) over the part's pairs (optimization.h:74-77);
 //   3. evaluates the objective in T with the reference's loop order and no FMA contraction
 //      (optimization.h:79-103), summing parts left to right from T(0) (sqs.h:417-418, fold.h:51-53);
@@ -242,8 +243,26 @@ __device__ __forceinline__ void swap_draw(uint8_t* col, uint32_t lo, uint32_t i,
   col[b] = va;
 }
 
+// Floyd's sampling of an m-subset of a window of n sites (Bentley and Floyd, "A sample of brilliance",
+// CACM 30(9), 1987): for j = n-m .. n-1 draw t uniform in [0, j] and take t, or j when t is taken. The
+// window starts filled with the other species, so "taken" is "holds the rarer species". Every
+// m-subset is equally likely, which is the distribution of the window's sites of that species after
+// a Fisher-Yates shuffle, with m draws instead of n - 1.
+__device__ __forceinline__ void floyd_window(uint8_t* col, uint32_t lo, uint32_t n, uint32_t word,
+                                             xoshiro128ss& words) {
+  const uint32_t m = word & 0xffffu;
+  const uint8_t rare = static_cast<uint8_t>(word >> 16);
+  for (uint32_t j = n - m; j < n; ++j) {
+    const uint32_t at = site_off(lo + __umulhi(words.next(), j + 1));  // (x * (j+1)) >> 32: t in [0, j]
+    col[col[at] == rare ? site_off(lo + j) : at] = rare;
+  }
+}
+
 // core/shuffle.h:39-50 with the words of shuffle_words (philox.cuh): a xoshiro128** generator seeded
-// by the Philox4x32-10 block of (seed; iteration, chain, part); the windows draw one after another.
+// by the Philox4x32-10 block of (seed; iteration, chain, part); the windows draw one after another. A
+// window of exactly two species (draw word != 0, staged after the window bounds) takes Floyd's
+// sampling of its rarer species' sites instead of the swaps; the staged initial arrangement holds the
+// other species on it.
 __device__ __forceinline__ void shuffle_part(uint8_t* smem, const PartDesc& P, int t, uint32_t it,
                                              unsigned long long chain, uint32_t part, uint32_t k0, uint32_t k1) {
   uint8_t* col = part_base(smem, P) + P.col_off + 4 * t;
@@ -251,8 +270,12 @@ __device__ __forceinline__ void shuffle_part(uint8_t* smem, const PartDesc& P, i
   xoshiro128ss words =
       shuffle_words(it, static_cast<uint32_t>(chain), (static_cast<uint32_t>(chain >> 32) << 8) | part, k0, k1);
   for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
-    const uint32_t lo = win[2 * wi];
-    for (uint32_t i = win[2 * wi + 1] - lo; i > 1; --i) swap_draw(col, lo, i, words.next());
+    const uint32_t lo = win[2 * wi], n = win[2 * wi + 1] - lo, fw = win[2 * P.n_windows + wi];
+    if (fw) {
+      floyd_window(col, lo, n, fw, words);
+    } else {
+      for (uint32_t i = n; i > 1; --i) swap_draw(col, lo, i, words.next());
+    }
   }
 }
 
@@ -702,7 +725,7 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
   const uint64_t my_off = static_cast<uint64_t>(t) * base + min(static_cast<uint64_t>(t), rem);
   const uint64_t max_count = base + (rem ? 1 : 0);
   constexpr bool systematic = SYS;  // J.mode == 1
-  // random mode: configuration id is the Fisher-Yates shuffle of the packed initial arrangement with
+  // random mode: configuration id is the shuffle (shuffle_part) of the staged initial arrangement with
   // the words seeded by (seed, id) (shuffle_words); it depends on nothing but (seed, id), so any split
   // of the job into tiles, launches or devices evaluates the same configurations
   const uint32_t k0 = static_cast<uint32_t>(J.seed), k1 = static_cast<uint32_t>(J.seed >> 32);
@@ -754,8 +777,8 @@ __device__ __forceinline__ void run_tile(const JobDesc& J, uint8_t* smem, LevelS
 //   A = sum_i b_i popc(NB_s[i] & v)  = n(s,1,1)
 //   E = sum_i b_i popc(NB_s[i])      = n(s,1,1) + n(s,1,0)
 // and n(s,0,0) = P_s minus the rest: the ordered counts of optimization.h:74-77, exactly. The
-// Fisher-Yates draws and the visiting order are the general path's, so both evaluate the same
-// configurations for a job.
+// draws (Fisher-Yates swaps, or Floyd's sampling on a two-species window) and the visiting order are
+// the general path's, so both evaluate the same configurations for a job.
 template <int W> struct Word;
 template <> struct Word<1> {
   using type = uint32_t;
@@ -877,12 +900,12 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
   const T* w = f + 4 * S;
   const T* tg = w + 4 * S;
   const uint32_t* win = reinterpret_cast<const uint32_t*>(part + P.win_off);
-  V v0 = 0;  // the packed initial arrangement
+  V v0 = 0;  // the staged initial arrangement (random jobs: the other species on each Floyd window)
   for (uint32_t x = 0; x < N; ++x)
     if (part[P.species_off + x]) v0 |= V(1) << (N - 1 - x);
-  // minority sites: the same number in every configuration (shuffles keep the composition)
-  int nb = 0;
-  for (V y = (P.k2_zeros ? ~v0 : v0) & low_mask<V>(N); y; y &= y - 1) ++nb;
+  // minority sites: the same number in every configuration (shuffles keep the composition; the staged
+  // arrangement of a random job holds only the other species on its Floyd windows)
+  const int nb = static_cast<int>(P.k2_zeros ? N - P.ones : P.ones);
   V v = v0;
   uint32_t wn = 0, wshift = 0;
   V wmask = 0;
@@ -921,13 +944,21 @@ __device__ __forceinline__ void run_tile_k2(const JobDesc& J, uint8_t* smem, Lev
             shuffle_words(0u, static_cast<uint32_t>(cid), static_cast<uint32_t>(cid >> 32) << 8, k0, k1);
         v = v0;
         for (uint32_t wi = 0; wi < P.n_windows; ++wi) {
-          const uint32_t lo = win[2 * wi];
+          const uint32_t lo = win[2 * wi], n = win[2 * wi + 1] - lo, fw = win[2 * P.n_windows + wi];
           const uint32_t top = N - 1 - lo;  // bit of the window's first site
-          for (uint32_t i = win[2 * wi + 1] - lo; i > 1; --i) {
-            const uint32_t pp = __umulhi(words.next(), i);
-            const uint32_t ba = top - (i - 1), bb = top - pp;
-            const V dlt = ((v >> ba) ^ (v >> bb)) & V(1);
-            v ^= (dlt << ba) | (dlt << bb);
+          if (fw) {  // floyd_window on bits: the window holds the other species, flip the drawn sites
+            const V rare = (fw >> 16) & 0xffu ? V(1) : V(0);
+            for (uint32_t j = n - (fw & 0xffffu); j < n; ++j) {
+              const uint32_t bt = top - __umulhi(words.next(), j + 1);
+              v ^= V(1) << (((v >> bt) & V(1)) == rare ? top - j : bt);
+            }
+          } else {
+            for (uint32_t i = n; i > 1; --i) {
+              const uint32_t pp = __umulhi(words.next(), i);
+              const uint32_t ba = top - (i - 1), bb = top - pp;
+              const V dlt = ((v >> ba) ^ (v >> bb)) & V(1);
+              v ^= (dlt << ba) | (dlt << bb);
+            }
           }
         }
       }

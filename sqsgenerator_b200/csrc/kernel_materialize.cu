@@ -1,7 +1,7 @@
 // sqsg_materialize: full records for selected candidates.
 //
 // The engine appends only (objective, id) per candidate. A configuration depends on nothing but the
-// job and its id — random mode: the Fisher-Yates shuffle of the packed initial arrangement with the
+// job and its id — random mode: the shuffle (shuffle_part) of the staged initial arrangement with the
 // words seeded by id; systematic mode: the multiset permutation of rank id (core/permutation.h:52-78) — so
 // the full record of a selected candidate (species, per-part objective and SRO cube) is rebuilt here,
 // once, through the general pair-stream path: ordered bonds (core/optimization.h:74-77), objective and

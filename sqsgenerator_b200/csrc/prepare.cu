@@ -129,6 +129,25 @@ static uint64_t window_permutations(const sqsg_sublattice& sl, PartDesc& pd) {
   return total;
 }
 
+// Draw word of a random-mode window with exactly two species: m (the rarer species' sites, ties to the
+// higher species index) | its code << 16 | the other code << 24; 0 for any other window, which takes
+// the Fisher-Yates shuffle.
+static uint32_t floyd_word(const sqsg_sublattice& sl, uint32_t w) {
+  const uint32_t lo = sl.windows[2 * w], hi = sl.windows[2 * w + 1];
+  uint32_t counts[kMaxSpecies] = {0};
+  for (uint32_t x = lo; x < hi; ++x) counts[sl.species[x]]++;
+  uint32_t a = kMaxSpecies, b = kMaxSpecies, distinct = 0;
+  for (uint32_t v = 0; v < static_cast<uint32_t>(kMaxSpecies); ++v)
+    if (counts[v]) {
+      ++distinct;
+      (a == kMaxSpecies ? a : b) = v;
+    }
+  if (distinct != 2) return 0u;
+  const uint32_t rare = counts[b] <= counts[a] ? b : a, other = rare == a ? b : a;
+  if (counts[rare] > 0xffffu) return 0u;
+  return counts[rare] | (rare << 3) << 16 | (other << 3) << 24;
+}
+
 // Lattice-path tables of one part, from its supercell hint (sqsg_sublattice::lattice): valid only
 // when the sites are a bijection onto (unit-cell site, cell) and every pair belongs to a translation
 // class {(beta, c), (beta2, c + d)} that the pair list holds completely — once per cell, or once per
@@ -465,6 +484,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
     P.n_species = sl.n_species;
     P.n_shells = sl.n_shells;
     P.n_windows = sl.n_windows;
+    for (uint32_t x = 0; x < sl.n_sites; ++x) P.ones += sl.species[x] == 1 ? 1u : 0u;
     P.hw = (sl.n_species + 1) / 2;
     if (sl.n_species > 4) d.kw = 2;
     P.stream_words = static_cast<uint32_t>(streams[p].size());
@@ -551,7 +571,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
     P.cube_off = 0;
     off = align_up(3 * skk * pj.tsz, 16);
     P.win_off = static_cast<uint32_t>(off);
-    off = align_up(off + 8ull * sl.n_windows, 16);
+    off = align_up(off + 12ull * sl.n_windows, 16);
     P.species_off = static_cast<uint32_t>(off);
     off = align_up(off + sl.n_sites, 16);
     if (k2) {
@@ -725,6 +745,15 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
     std::memcpy(base + P.win_off, sl.windows, 8ull * sl.n_windows);
     std::memcpy(base + P.stream_off, streams[p].data(), 4ull * streams[p].size());
     for (uint32_t x = 0; x < sl.n_sites; ++x) base[P.species_off + x] = static_cast<uint8_t>(sl.species[x] << 3);
+    // random mode: a window of exactly two species draws the sites of its rarer species (Floyd's
+    // sampling, see shuffle_part), starting from the window filled with the other species
+    const bool floyd = !pj.systematic && !pj.chain && option(kOptBinaryFloyd) != 0;
+    for (uint32_t w = 0; w < sl.n_windows; ++w) {
+      const uint32_t word = floyd ? floyd_word(sl, w) : 0u;
+      std::memcpy(base + P.win_off + 8ull * sl.n_windows + 4ull * w, &word, 4);
+      if (word)
+        for (uint32_t x = sl.windows[2 * w]; x < sl.windows[2 * w + 1]; ++x) base[P.species_off + x] = word >> 24;
+    }
     const auto& k2d = k2_data[p];
     if (!k2d.first.empty()) std::memcpy(base + P.k2_off, k2d.first.data(), 4 * k2d.first.size());
     if (!k2d.second.empty()) std::memcpy(base + P.k2_shell_off, k2d.second.data(), 4 * k2d.second.size());

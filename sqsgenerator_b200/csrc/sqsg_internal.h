@@ -23,6 +23,7 @@ enum Option : int {
   kOptRerunRecordBytes = 5,   // bytes of full records a re-run of an overflowed job may produce
   kOptRapidrand = 6,          // debug: random jobs follow the reference's seeded single-thread trajectory
   kOptServerFinalizers = 7,   // result-selection threads of a server created afterwards
+  kOptBinaryFloyd = 8,        // 1: random windows of two species draw their minority sites (Floyd)
   kOptCount
 };
 long long option(Option o);

@@ -1,5 +1,5 @@
 // Tile decomposition of a job's configuration range. A configuration depends only on the job and
-// its id (random mode: Fisher-Yates with words seeded by id; systematic mode: rank = id), so any
+// its id (random mode: a shuffle with words seeded by id; systematic mode: rank = id), so any
 // decomposition evaluates the same configurations; tiles only shape the schedule.
 //
 // Tiles are guided: each takes about 1/2048 of what is left (large tiles first, then smaller ones

@@ -93,26 +93,36 @@ def trace(config, capacity):
 
 
 def trace_mismatches(d, sp, bd, ob, prec, limit=None):
-    """Recompute ordered bonds and objective of every traced configuration with the oracle; return
-    the mismatching rows."""
+    """Recompute ordered bonds and objective of every traced configuration with the oracle, and check
+    that each is an arrangement of the packed one (every window keeps its species multiset, sites outside
+    the windows keep theirs); return the mismatching rows."""
     n = len(ob) if limit is None else min(limit, len(ob))
     T = np.float64 if prec in ("double", 1) else np.float32
     bad = []
     total = None
     bonds_ok = np.ones(n, dtype=bool)
+    comp_ok = np.ones(n, dtype=bool)
     o1 = o2 = 0
     for part in d:
         npart = len(part.species_packed)
         skk = part.prefactors.size
-        b, o = oracle.evaluate_many(part, sp[:n, o1:o1 + npart], prec)
+        rows = sp[:n, o1:o1 + npart]
+        packed = np.asarray(part.species_packed)
+        fixed = np.ones(npart, dtype=bool)
+        for lo, hi in np.asarray(part.windows).tolist():
+            fixed[lo:hi] = False
+            comp_ok &= np.all(np.sort(rows[:, lo:hi], axis=1) == np.sort(packed[lo:hi]), axis=1)
+        comp_ok &= np.all(rows[:, fixed] == packed[fixed], axis=1)
+        b, o = oracle.evaluate_many(part, rows, prec)
         bonds_ok &= np.all(b.reshape(n, skk).astype(np.uint32) == bd[:n, o2:o2 + skk], axis=1)
         total = o if total is None else (total + o).astype(T)
         o1 += npart
         o2 += skk
     obj_ok = total.view(np.uint32 if T is np.float32 else np.uint64) == np.asarray(ob[:n], T).view(
         np.uint32 if T is np.float32 else np.uint64)
-    for k in np.flatnonzero(~(bonds_ok & obj_ok))[:20]:
-        bad.append((int(k), "bonds" if not bonds_ok[k] else "objective", total[k], ob[k]))
+    for k in np.flatnonzero(~(bonds_ok & obj_ok & comp_ok))[:20]:
+        what = "composition" if not comp_ok[k] else ("bonds" if not bonds_ok[k] else "objective")
+        bad.append((int(k), what, total[k], ob[k]))
     return bad
 
 

@@ -1,9 +1,11 @@
-"""Test-side Philox4x32-10 (Salmon et al., SC'11), xoshiro128** and the Fisher-Yates shuffle the device runs.
+"""Test-side Philox4x32-10 (Salmon et al., SC'11), xoshiro128** and the shuffle the device runs.
 
 Used to predict, configuration by configuration, what the random mode evaluates: configuration g of a job
-is the Fisher-Yates shuffle of the packed arrangement whose words come from a xoshiro128** generator seeded
-with the Philox block of counter (0, iteration, g_lo, g_hi << 8 | part) and key (seed_lo, seed_hi), bounded
-like core/shuffle.h:28-32 of the reference: p = (x * i) >> 32.
+is the shuffle of the packed arrangement whose words come from a xoshiro128** generator seeded with the
+Philox block of counter (0, iteration, g_lo, g_hi << 8 | part) and key (seed_lo, seed_hi), bounded like
+core/shuffle.h:28-32 of the reference: p = (x * i) >> 32. Each window in turn takes a Fisher-Yates pass,
+or, when it holds exactly two species and the binary_floyd option is on (the default), Floyd's sampling of
+the sites of its rarer species (ties: the higher species index) over the window filled with the other one.
 """
 M0, M1 = 0xD2511F53, 0xCD9E8D57
 W0, W1 = 0x9E3779B9, 0xBB67AE85
@@ -56,16 +58,38 @@ class Xoshiro128ss:
         return r
 
 
-def shuffle(species, windows, seed, chain, iteration, part=0):
-    """One Fisher-Yates pass over every window, in place on a list: the words come from a xoshiro128**
-    generator whose state is the Philox4x32-10 block of counter (0, iteration, chain_lo,
-    chain_hi << 8 | part) and key (seed_lo, seed_hi)."""
+def floyd_choice(window):
+    """(m, rare, other) of a window of exactly two species, else None: rare is the species with fewer
+    sites (ties: the higher index) and m its site count."""
+    values = sorted(set(window))
+    if len(values) != 2:
+        return None
+    a, b = values
+    na, nb = window.count(a), window.count(b)
+    rare, other = (b, a) if nb <= na else (a, b)
+    return min(na, nb), rare, other
+
+
+def shuffle(species, windows, seed, chain, iteration, part=0, floyd=True):
+    """One shuffle of every window, in place on a list: the words come from a xoshiro128** generator
+    whose state is the Philox4x32-10 block of counter (0, iteration, chain_lo, chain_hi << 8 | part) and
+    key (seed_lo, seed_hi). ``species`` must be the packed arrangement (the rule that picks Floyd's
+    sampling reads each window's species)."""
     k = (seed & MASK, (seed >> 32) & MASK)
     c_lo = chain & MASK
     c_hi = (((chain >> 32) << 8) | part) & MASK
     gen = Xoshiro128ss(philox4x32_10((0, iteration & MASK, c_lo, c_hi), k))
     for lo, hi in windows:
-        for i in range(hi - lo, 1, -1):
+        n = hi - lo
+        choice = floyd_choice(species[lo:hi]) if floyd else None
+        if choice is not None:
+            m, rare, other = choice
+            species[lo:hi] = [other] * n
+            for j in range(n - m, n):
+                t = (gen.next() * (j + 1)) >> 32
+                species[lo + (j if species[lo + t] == rare else t)] = rare
+            continue
+        for i in range(n, 1, -1):
             p = (gen.next() * i) >> 32
             a, b = lo + i - 1, lo + p
             species[a], species[b] = species[b], species[a]

@@ -369,23 +369,26 @@ def test_fcc32_systematic_full_space_levels(prec):
 
 
 # --------------------------------------------------------------------------- RNG stream and fast path
-@pytest.mark.parametrize("composition", [{"Ti": 16, "Al": 16}, {"Ti": 11, "Al": 11, "Nb": 10}],
-                         ids=["binary_fast_path", "ternary_general_path"])
-def test_random_stream_is_philox_fisher_yates(composition):
-    """Configuration g is the Fisher-Yates shuffle of the packed initial arrangement with xoshiro128** words
-    seeded by the Philox block of counter g (tests/philox_ref.py): it depends on (seed, g) alone, not on
-    tiles, launches or devices."""
+@pytest.mark.parametrize("composition,floyd", [({"Ti": 16, "Al": 16}, 1), ({"Ti": 16, "Al": 16}, 0),
+                                               ({"Ti": 7, "Al": 25}, 1), ({"Ti": 11, "Al": 11, "Nb": 10}, 1)],
+                         ids=["binary_fast_path_floyd", "binary_fast_path_fisher_yates", "binary_skewed_floyd",
+                              "ternary_general_path"])
+def test_random_stream_is_philox_fisher_yates(composition, floyd):
+    """Configuration g is the shuffle of the packed initial arrangement with xoshiro128** words seeded by
+    the Philox block of counter g (tests/philox_ref.py) — Fisher-Yates, or Floyd's sampling of the rarer
+    species on a two-species window: it depends on (seed, g) alone, not on tiles, launches or devices."""
     import philox_ref
 
     total = 2_097_153
     cfg = cases.fcc32("double", composition=composition, iterations=total, seed=0x1234_5678_9ABC)
-    c, d, pack, sp, bd, ob, ids = cases.trace(cfg, total)
+    with N.options(binary_floyd=floyd):
+        c, d, pack, sp, bd, ob, ids = cases.trace(cfg, total)
     assert np.array_equal(ids, np.arange(total, dtype=np.uint64))
     windows = [tuple(w) for w in d[0].windows.tolist()]
     rng = np.random.default_rng(0)
     for g in sorted(set(rng.choice(total, size=400, replace=False).tolist()) | {0, 1, total - 1}):
         conf = d[0].species_packed.tolist()
-        philox_ref.shuffle(conf, windows, cfg["seed"], g, 0)
+        philox_ref.shuffle(conf, windows, cfg["seed"], g, 0, floyd=bool(floyd))
         assert conf == sp[g].tolist(), g
     assert cases.trace_mismatches(d, sp[:1500], bd[:1500], ob[:1500], "double") == []
 

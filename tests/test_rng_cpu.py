@@ -65,3 +65,41 @@ def test_shuffle_is_a_permutation_of_each_window():
     for g in range(50):
         conf = philox_ref.shuffle(list(species), windows, 99, g, 0)
         assert sorted(conf[:22]) == sorted(species[:22]) and sorted(conf[22:]) == sorted(species[22:])
+
+
+def test_floyd_windows_take_every_arrangement_equally_often():
+    """Floyd's sampling on a two-species window (6 sites, 2 of the rarer species: 15 arrangements) and
+    Fisher-Yates on the same window give each arrangement with probability 1/15: chi-square of 15,000
+    seeded configurations against uniform, far below the 0.1 % point of 14 degrees of freedom (36.1)."""
+    species = [1, 1, 0, 0, 0, 0]
+    assert philox_ref.floyd_choice(species) == (2, 1, 0)
+    assert philox_ref.floyd_choice([0, 0, 1, 1]) == (2, 1, 0)  # ties: the higher species index
+    assert philox_ref.floyd_choice([0, 1, 2]) is None
+    for floyd in (True, False):
+        seen = {}
+        for g in range(15_000):
+            conf = tuple(philox_ref.shuffle(list(species), [(0, 6)], 7, g, 0, floyd=floyd))
+            assert sorted(conf) == sorted(species)
+            seen[conf] = seen.get(conf, 0) + 1
+        assert len(seen) == 15
+        chi2 = sum((c - 1000) ** 2 / 1000 for c in seen.values())
+        assert chi2 < 36.1, (floyd, chi2)
+
+
+def test_floyd_window_draws_m_words():
+    """A two-species window takes one word per site of its rarer species: the next window's draws start
+    m words into the stream (here m = 3 of 10 sites, then a three-species window)."""
+    species = [0] * 7 + [1] * 3 + [0, 1, 2, 2]
+    windows = [(0, 10), (10, 14)]
+    k, it, g = 5, 0, 11
+    got = philox_ref.shuffle(list(species), windows, k, g, it)
+    gen = philox_ref.Xoshiro128ss(philox_ref.philox4x32_10((0, it, g, 0), (k, 0)))
+    want = [0] * 10
+    for j in range(7, 10):
+        t = (gen.next() * (j + 1)) >> 32
+        want[j if want[t] == 1 else t] = 1
+    tail = species[10:]
+    for i in range(4, 1, -1):
+        p = (gen.next() * i) >> 32
+        tail[i - 1], tail[p] = tail[p], tail[i - 1]
+    assert got == want + tail
