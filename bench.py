@@ -45,7 +45,7 @@ def workload_config(name: str):
             "P=240 pairs), weights 1.0/0.5, pair weights 1, keep 10, float64")
     if name == "random":
         return cases.fcc32("double", iterations=1_000_000, seed=42), (
-            "fcc 2x2x2 (32 sites) A16B16 random, 1e6 Fisher-Yates configurations (Philox-seeded xoshiro128** words), 2 shells, weights 1.0/0.5, "
+            "fcc 2x2x2 (32 sites) A16B16 random, 1e6 random configurations (Floyd sampling of the 16 B sites, Philox-seeded xoshiro128** words), 2 shells, weights 1.0/0.5, "
             "pair weights 1, keep 10, float64")
     if name == "quinary":
         return cases.quinary("double", cells=(4, 4, 4), iterations=20_000_000, seed=0, keep=10,
