@@ -177,7 +177,7 @@ struct PartDesc {
 // 64-bit word per word of the job's cell sets (W = lat_words): the staged table holds LatTrW<W>.
 template <int W> struct LatTrW {
   uint32_t sx, sxr, sy, syr, sz, szr, pad0, pad1;
-  unsigned long long mxh[W], mxl[W], myh[W], myl[W];
+  unsigned long long mxh[W], myh[W];  // cells whose source does not wrap in x, in y (the rest wrap)
 };
 using LatTr = LatTrW<2>;  // the host's working form (written out at the job's width)
 

@@ -1071,18 +1071,21 @@ template <int W> __device__ __forceinline__ LatBits<W> lat_shr(const LatBits<W>&
 }
 
 // Translation of a cell set by (tx, ty, tz): rotations inside rows of A bits, blocks of A*B bits and
-// the whole grid of A*B*C bits (masks select the cells that wrap); a zero shift skips its stage.
+// the whole grid of A*B*C bits; a zero shift skips its stage. mxh, myh mark the cells whose source does
+// not wrap (taken from the left shift); the others take the right shift. Outside the grid a set has
+// no bits and the right shifts bring in none (their sources lie past the grid), so one select per
+// word, a single three-input logic op, blends the two shifts.
 template <int W>
 __device__ __forceinline__ LatBits<W> lat_translate(LatBits<W> v, const LatTrW<W>* t, const LatBits<W>& full) {
   if (t->sx) {
     const LatBits<W> h = lat_shl<W>(v, t->sx), l = lat_shr<W>(v, t->sxr);
 #pragma unroll
-    for (int k = 0; k < W; ++k) v.w[k] = (h.w[k] & t->mxh[k]) | (l.w[k] & t->mxl[k]);
+    for (int k = 0; k < W; ++k) v.w[k] = (h.w[k] & t->mxh[k]) | (l.w[k] & ~t->mxh[k]);
   }
   if (t->sy) {
     const LatBits<W> h = lat_shl<W>(v, t->sy), l = lat_shr<W>(v, t->syr);
 #pragma unroll
-    for (int k = 0; k < W; ++k) v.w[k] = (h.w[k] & t->myh[k]) | (l.w[k] & t->myl[k]);
+    for (int k = 0; k < W; ++k) v.w[k] = (h.w[k] & t->myh[k]) | (l.w[k] & ~t->myh[k]);
   }
   if (t->sz) {
     const LatBits<W> h = lat_shl<W>(v, t->sz), l = lat_shr<W>(v, t->szr);

@@ -248,8 +248,8 @@ static bool lattice_tables(const sqsg_sublattice& sl, LatticeTables& L) {
     for (uint32_t c = 0; c < L.cells; ++c) {
       const uint32_t x = c % A, y = (c / A) % B;
       const unsigned long long bit = 1ull << (c % 64);
-      (x >= tx ? t.mxh : t.mxl)[c / 64] |= bit;
-      (y >= ty ? t.myh : t.myl)[c / 64] |= bit;
+      if (x >= tx) t.mxh[c / 64] |= bit;
+      if (y >= ty) t.myh[c / 64] |= bit;
     }
     const uint32_t idx = static_cast<uint32_t>(L.tr.size());
     L.tr.push_back(t);
@@ -769,7 +769,7 @@ PreparedJob prepare(const sqsg_job& job, uint64_t trace_capacity, const Tuning* 
       } else {  // one-word cell sets: the masks' first words only
         for (size_t k = 0; k < LT.tr.size(); ++k) {
           const LatTr& t = LT.tr[k];
-          const LatTrW<1> o{t.sx, t.sxr, t.sy, t.syr, t.sz, t.szr, 0u, 0u, {t.mxh[0]}, {t.mxl[0]}, {t.myh[0]}, {t.myl[0]}};
+          const LatTrW<1> o{t.sx, t.sxr, t.sy, t.syr, t.sz, t.szr, 0u, 0u, {t.mxh[0]}, {t.myh[0]}};
           std::memcpy(base + P.lat_tr_off + k * sizeof(LatTrW<1>), &o, sizeof(o));
         }
       }
