@@ -1206,10 +1206,35 @@ static bool try_admit(ServerState& S) {
   return true;
 }
 
+// Candidate records a (re-)run of J may keep in the arena: the re-run budget, and what the arena holds
+// next to the job's own data.
+static uint64_t arena_record_limit(const ServerState& S, const ServerJob& J) {
+  const uint64_t arena_bytes = S.opt.arena_bytes;
+  return std::min<uint64_t>(rerun_limit(J.pj),
+                            (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) /
+                                sizeof(Cand));
+}
+
+// Puts a job whose candidate buffer overflowed back at the front of the queue, with the threshold,
+// buffer and distinct-configuration table that assess() asks for (the same configurations are
+// evaluated again). Called with S.m held, after the job's arena memory was released.
+static void requeue_rerun(ServerState& S, std::unique_ptr<ServerJob> job, const Outcome& o) {
+  ServerJob& J = *job;
+  J.capacity = o.rerun_capacity;
+  J.slots = o.rerun_slots;
+  J.fixed_threshold = true;
+  J.start_threshold = o.rerun_threshold;
+  J.attempt++;
+  S.pending.push_front(std::move(job));
+  S.cv_work.notify_one();
+}
+
 // Collects a finished job on the worker thread: counters and level table come back on the copy
 // stream (the records too when the level table overflowed) and the job's slot is released at once.
-// Its arena memory stays with it until a finalizer thread has selected the result set, so that
-// admission and launches go on meanwhile.
+// A job that must run again with an exact level table is requeued here (the decision reads only the
+// counters and the level table), not behind the finalizers, which may be busy with large result
+// sets. Otherwise its arena memory stays with it until a finalizer thread has selected the result
+// set, so that admission and launches go on meanwhile.
 static void collect(ServerState& S, uint32_t slot) {
   ServerState::Collected c;
   c.job = std::move(S.slots[slot]);
@@ -1227,6 +1252,23 @@ static void collect(ServerState& S, uint32_t slot) {
     CUDA_CHECK(cudaMemcpyAsync(c.records.data(), S.arena + J.arena_off + J.blob_bytes, n * sizeof(Cand),
                                cudaMemcpyDeviceToHost, S.copy));
     CUDA_CHECK(cudaStreamSynchronize(S.copy));
+  }
+  if (!J.slots && !c.cnt[kLevelOverflow]) {
+    Outcome o;
+    bool decided = false;
+    try {
+      check_job_counters(c.cnt.data());
+      o = assess(J.pj, c.cnt.data(), c.levels.data(), c.records, n, J.capacity, !J.user_capacity && J.attempt < 2,
+                 arena_record_limit(S, J));
+      decided = true;
+    } catch (std::exception const&) {
+      // the finalizer reports the job's error
+    }
+    if (decided && o.rerun) {
+      arena_free(S, J.arena_off, J.arena_bytes);
+      requeue_rerun(S, std::move(c.job), o);
+      return;
+    }
   }
   S.collected.push_back(std::move(c));
   S.cv_fin.notify_one();
@@ -1252,7 +1294,6 @@ static void finalizer_loop(ServerState* Sp) {
     if (S.stop) break;
     ServerState::Collected c = std::move(S.collected.front());
     S.collected.pop_front();
-    const uint64_t arena_bytes = S.opt.arena_bytes;
     lock.unlock();
     ServerJob& J = *c.job;
     std::string error;
@@ -1266,10 +1307,7 @@ static void finalizer_loop(ServerState* Sp) {
     }
     const unsigned long long* cnt = c.cnt.data();
     const uint64_t n = std::min<uint64_t>(cnt[kCandidates], J.capacity);
-    const uint64_t arena_records =
-        std::min<uint64_t>(rerun_limit(J.pj),
-                           (arena_bytes - std::min<uint64_t>(arena_bytes, align_up(J.pj.blob.size(), 256) + 256)) /
-                               sizeof(Cand));
+    const uint64_t arena_records = arena_record_limit(S, J);
     Run r;
     Outcome o;
     uint64_t fin_d2h = c.records.size() * sizeof(Cand);
@@ -1317,13 +1355,7 @@ static void finalizer_loop(ServerState* Sp) {
       S.failed[J.ticket] = {SQSG_ERR_CUDA, error};
       S.cv_done.notify_all();
     } else if (o.rerun) {
-      J.capacity = o.rerun_capacity;
-      J.slots = o.rerun_slots;
-      J.fixed_threshold = true;
-      J.start_threshold = o.rerun_threshold;
-      J.attempt++;
-      S.pending.push_front(std::move(c.job));
-      S.cv_work.notify_one();
+      requeue_rerun(S, std::move(c.job), o);
     } else {
       S.stats.completed++;
       S.stats.configurations += cnt[kFinished];
@@ -1469,8 +1501,14 @@ static void server_loop(ServerState* Sp) {
     bool progress = false;
     if (S.broken.empty()) {
       try {
-        CUDA_CHECK(cudaMemcpyAsync(S.h_ctl, S.d_ctl, kCtlBytes, cudaMemcpyDeviceToHost, S.copy));
-        CUDA_CHECK(cudaStreamSynchronize(S.copy));
+        // the control block comes back without the lock held: only this thread uses the copy stream
+        // and changes the slots it describes, and submissions and finalizers need not wait for a copy
+        // engine that may be busy with large result sets
+        lock.unlock();
+        cudaError_t ce = cudaMemcpyAsync(S.h_ctl, S.d_ctl, kCtlBytes, cudaMemcpyDeviceToHost, S.copy);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(S.copy);
+        lock.lock();
+        CUDA_CHECK(ce);
         if (const unsigned long long st = S.device_status())
           throw cuda_error("device error " + std::to_string(st) + " in the serving kernel");
         for (uint32_t k = 0; k < S.slots.size(); ++k) {
