@@ -130,6 +130,22 @@ def test_served_admission_waits_for_memory():
     del c0
 
 
+def test_served_rerun_after_overflow():
+    """Jobs whose best levels hold more configurations than their candidate buffer (256) run again with the
+    exact threshold, requeued as soon as they are collected; the results equal sqsg_optimize's alone."""
+    cfgs = [cases.fcc32("double", iterations=200000, seed=s, pair_weights=None) for s in (11, 12, 13)]
+    ref = alone(cfgs)
+    with S.Server(0, default_max_results=256) as srv:
+        tickets = [srv.submit(cfg) for cfg in cfgs]
+        for k, t in enumerate(tickets):
+            run = srv.wait_run(t, timeout=120)
+            c = S.parse_config(cfgs[k])
+            assert records(run, c, S.prepare(c)) == ref[k]
+            N.lib().sqsg_run_free(run)
+        st = srv.stats()
+    assert st["completed"] == 3 and st["admitted"] > 3  # every job overflowed once
+
+
 def test_server_rejects_jobs_that_never_fit():
     with S.Server(0, arena_bytes=1 << 20) as srv:
         with pytest.raises(N.NativeError) as e:
