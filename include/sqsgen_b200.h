@@ -286,7 +286,9 @@ typedef struct {
   sqsg_part_plan parts[8];
   uint64_t bucket;        /* the job's bucket in the tuning table (see sqsg_autotune) */
   int32_t tuned;          /* 1 when the launch follows a measured tuning entry */
-  uint32_t reserved2;
+  uint32_t shuffle_draws; /* random mode: bounded draws per configuration over all parts (a window of
+                             two species draws its rarer species' sites, option "binary_floyd";
+                             another window n - 1); 0 in systematic mode */
 } sqsg_plan;
 
 /* How sqsg_optimize would run the job: per optimised structure the evaluation path, and the launch

@@ -115,7 +115,7 @@ class SqsgPartPlan(C.Structure):
 class SqsgPlan(C.Structure):
     _fields_ = [("n_parts", C.c_uint32), ("smem_bytes", C.c_uint32), ("ctas_per_sm", C.c_uint32),
                 ("record_bytes", C.c_uint32), ("kernel", C.c_char * 32), ("parts", SqsgPartPlan * 8),
-                ("bucket", C.c_uint64), ("tuned", C.c_int32), ("reserved2", C.c_uint32)]
+                ("bucket", C.c_uint64), ("tuned", C.c_int32), ("shuffle_draws", C.c_uint32)]
 
 
 class SqsgTuning(C.Structure):
@@ -259,7 +259,8 @@ def plan(job) -> dict:
                   lattice_units=int(p.parts[k].lattice_units))
              for k in range(p.n_parts)]
     return dict(kernel=p.kernel.decode(), smem_bytes=int(p.smem_bytes), ctas_per_sm=int(p.ctas_per_sm),
-                record_bytes=int(p.record_bytes), parts=parts, bucket=int(p.bucket), tuned=bool(p.tuned))
+                record_bytes=int(p.record_bytes), parts=parts, bucket=int(p.bucket), tuned=bool(p.tuned),
+                shuffle_draws=int(p.shuffle_draws))
 
 
 def autotune(job, seconds: float = 2.0) -> tuple[dict, list[dict]]:

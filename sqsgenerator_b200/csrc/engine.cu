@@ -1749,6 +1749,16 @@ sqsg_status sqsg_plan_job(const sqsg_job* job, sqsg_plan* plan) {
       plan->parts[p].stream_narrow = static_cast<int32_t>(P.stream_narrow);
       plan->parts[p].stream_staged = P.stream_global ? 0 : 1;
       if (d.lat) plan->parts[p].lattice_units = static_cast<uint32_t>(lattice_units(pj, p));
+      if (!pj.systematic) {  // random words per configuration: Floyd windows draw m, the others n - 1
+        const uint8_t* base = pj.blob.data() + P.blob_off + P.win_off;
+        for (uint32_t w = 0; w < P.n_windows; ++w) {
+          uint32_t lo, hi, fw;
+          std::memcpy(&lo, base + 8ull * w, 4);
+          std::memcpy(&hi, base + 8ull * w + 4, 4);
+          std::memcpy(&fw, base + 8ull * P.n_windows + 4ull * w, 4);
+          plan->shuffle_draws += fw ? (fw & 0xffffu) : hi - lo - 1;
+        }
+      }
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) == cudaSuccess && job->device >= 0 && job->device < ndev) {

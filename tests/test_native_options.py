@@ -178,3 +178,22 @@ def test_rapidrand_debug_option_takes_the_pair_stream():
     with N.options(rapidrand=1):
         assert plan_of(cfg)["parts"][0]["path"] == "general"
     assert N.get_option("rapidrand") == 0
+
+
+def test_binary_floyd_option_sets_the_draws_per_configuration():
+    """A random window of two species draws the sites of its rarer species (Floyd's sampling); with
+    binary_floyd = 0, or with three species, a window takes n - 1 Fisher-Yates draws; systematic jobs
+    draw nothing."""
+    assert N.get_option("binary_floyd") == 1
+    assert plan_of(cases.fcc32("double", iterations=1000))["shuffle_draws"] == 16
+    assert plan_of(cases.fcc32("double", composition={"Ti": 7, "Al": 25}, iterations=1000))["shuffle_draws"] == 7
+    assert plan_of(cases.fcc32("double", composition={"Ti": 11, "Al": 11, "Nb": 10},
+                               iterations=1000))["shuffle_draws"] == 31
+    assert plan_of(cases.rocksalt_split("double", iterations=1000))["shuffle_draws"] == 16 + 4  # Ti16Al16, N28B4
+    assert plan_of(cases.fcc32("double", iteration_mode="systematic", seed=None,
+                               iterations=None))["shuffle_draws"] == 0
+    with N.options(binary_floyd=0):
+        assert plan_of(cases.fcc32("double", iterations=1000))["shuffle_draws"] == 31
+        assert plan_of(cases.rocksalt_split("double", iterations=1000))["shuffle_draws"] == 31 + 31
+    with N.options(rapidrand=1):  # the reference's stream: Fisher-Yates on every window
+        assert plan_of(cases.fcc32("double", iterations=1000, chunk_size=100))["shuffle_draws"] == 31
