@@ -136,13 +136,11 @@ static uint32_t floyd_word(const sqsg_sublattice& sl, uint32_t w) {
   const uint32_t lo = sl.windows[2 * w], hi = sl.windows[2 * w + 1];
   uint32_t counts[kMaxSpecies] = {0};
   for (uint32_t x = lo; x < hi; ++x) counts[sl.species[x]]++;
-  uint32_t a = kMaxSpecies, b = kMaxSpecies, distinct = 0;
+  uint32_t present[kMaxSpecies], distinct = 0;  // species of the window, ascending
   for (uint32_t v = 0; v < static_cast<uint32_t>(kMaxSpecies); ++v)
-    if (counts[v]) {
-      ++distinct;
-      (a == kMaxSpecies ? a : b) = v;
-    }
+    if (counts[v]) present[distinct++] = v;
   if (distinct != 2) return 0u;
+  const uint32_t a = present[0], b = present[1];
   const uint32_t rare = counts[b] <= counts[a] ? b : a, other = rare == a ? b : a;
   if (counts[rare] > 0xffffu) return 0u;
   return counts[rare] | (rare << 3) << 16 | (other << 3) << 24;
