@@ -8,6 +8,7 @@ defaults and error keys/codes. Like the reference's Python binding, failures are
 from __future__ import annotations
 
 import json
+import numbers
 import os
 from typing import Any
 
@@ -66,12 +67,20 @@ def _structure(doc, T) -> tuple[Structure, tuple]:
     for k in ("lattice", "coords"):
         if k not in s:
             _fail(k, ParseErrorCode.not_found, f"Missing \"{k}\"")
-    lattice = np.asarray(s["lattice"], dtype=T)
-    coords = np.asarray(s["coords"], dtype=T)
-    if lattice.shape != (3, 3):
-        _fail("lattice", ParseErrorCode.bad_value, "lattice must be a 3x3 matrix")
-    if coords.ndim != 2 or coords.shape[1] != 3:
-        _fail("coords", ParseErrorCode.bad_value, "coords must be a N x 3 matrix")
+    # a value that does not convert to the matrix type is a type error (the reference's get_as of an
+    # Eigen matrix, structure.h:143-144)
+    try:
+        lattice = np.asarray(s["lattice"], dtype=T)
+    except (TypeError, ValueError):
+        lattice = None
+    if lattice is None or lattice.shape != (3, 3):
+        _fail("lattice", ParseErrorCode.type_error, "lattice must be a 3x3 matrix")
+    try:
+        coords = np.asarray(s["coords"], dtype=T)
+    except (TypeError, ValueError):
+        coords = None
+    if coords is None or coords.ndim != 2 or coords.shape[1] != 3:
+        _fail("coords", ParseErrorCode.type_error, "coords must be a N x 3 matrix")
     if "species" not in s:
         _fail("species", ParseErrorCode.not_found, "Missing \"species\"")
     sp = list(s["species"])
@@ -156,6 +165,10 @@ def _composition(doc, species, mode) -> list[Sublattice]:
         for k, v in d.items():
             if k not in SYMBOL_MAP:
                 continue
+            # the amount is read as an integer (composition.h:106): anything else is a type error
+            if isinstance(v, (bool, np.bool_)) or not isinstance(v, (numbers.Real, np.number)):
+                _fail("composition", ParseErrorCode.type_error,
+                      f"The amount of \"{k}\" atoms must be an integer, not {v!r}")
             amount = int(v)
             if amount > len(sites) or amount < 0:
                 _fail("composition", ParseErrorCode.bad_value,
