@@ -201,3 +201,59 @@ def test_arrays_interact_mode_with_two_sublattices():
     c = S.parse_config(with_two_sublattices((3, 3, 3)))
     assert not isinstance(c, S.ParseError), c
     assert len(c.pair_weights) == len(c.target_objective) == len(c.prefactors) == 1
+
+
+def _re_w_first():
+    """The reference's "re-w.first" template: bcc Re-W 50/50, 3x3x3, first shell only, at most 10
+    results per objective."""
+    a = 3.165
+    return {"structure": {"lattice": [[a, 0, 0], [0, a, 0], [0, 0, a]], "coords": [[0, 0, 0], [0.5, 0.5, 0.5]],
+                          "species": ["W", "Re"], "supercell": [3, 3, 3]},
+            "iterations": 50_000_000, "shell_weights": {"1": 1.0}, "composition": {"W": 27, "Re": 27},
+            "max_results_per_objective": 10}
+
+
+def _ti_al_b_n():
+    """The reference's "ti-al-b-n" template: rocksalt TiN 3x3x3 in split mode, TiAl on the metal sites
+    towards ordering (target -1), NB on the non-metal sites towards clustering (target +1)."""
+    a = 4.253534
+    coords = [[0.5, 0, 0], [0.5, 0.5, 0.5], [0, 0, 0.5], [0, 0.5, 0], [0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5],
+              [0.5, 0.5, 0]]
+    return {"iterations": 1_000_000_000, "sublattice_mode": "split",
+            "structure": {"supercell": [3, 3, 3], "species": ["Ti"] * 4 + ["N"] * 4,
+                          "lattice": [[a, 0, 0], [0, a, 0], [0, 0, a]], "coords": coords},
+            "composition": [{"sites": "Ti", "Ti": 54, "Al": 54}, {"sites": "N", "N": 54, "B": 54}],
+            "target_objective": [-1, 1]}
+
+
+def test_templates_parse_like_the_reference():
+    """The reference's shipped templates (its test_templates.py runs them through the CLI) parse, and
+    carry what they say: sites, shells, caps, per-sublattice targets."""
+    c = S.parse_config(_re_w_first())
+    assert not isinstance(c, S.ParseError), c
+    assert c.iterations == 50_000_000 and c.max_results_per_objective == 10
+    assert list(c.shell_weights[0]) == [1] and len(c.composition) == 1
+    assert len(c.composition[0].sites) == 54
+    c = S.parse_config(_ti_al_b_n())
+    assert not isinstance(c, S.ParseError), c
+    assert int(c.sublattice_mode) == int(S.SublatticeMode.split) and len(c.composition) == 2
+    assert [len(sl.sites) for sl in c.composition] == [108, 108]
+    assert np.all(c.target_objective[0] == -1) and np.all(c.target_objective[1] == 1)
+
+
+def test_templates_take_the_fast_paths():
+    """Without a device, the plan of each template: the bit-mask path for the 54-site binary bcc cell,
+    the lattice path for both rocksalt sublattices."""
+    from sqsgenerator_b200 import _native as N
+    from sqsgenerator_b200.optimize import build_job
+
+    def plan(cfg):
+        c = S.parse_config(cfg)
+        d = S.prepare(c)
+        job, _ = build_job(c, d)
+        return N.plan(job)
+
+    p = plan({**_re_w_first(), "iterations": 1000})
+    assert [x["path"] for x in p["parts"]] == ["bitmask"] and p["shuffle_draws"] == 27
+    p = plan({**_ti_al_b_n(), "iterations": 1000})
+    assert [x["path"] for x in p["parts"]] == ["lattice", "lattice"] and p["shuffle_draws"] == 54 + 54
