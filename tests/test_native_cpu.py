@@ -189,3 +189,34 @@ def test_parse_arrays_broadcast():
     assert np.all(c.prefactors[0] == 0.5)
     bad = {**cases.fcc32(), "target_objective": np.zeros((3, 2, 2)).tolist()}
     assert code(S.parse_config(bad)) == ("target_objective", ParseErrorCode.bad_value)
+
+
+def test_structure_sliced_like_reference():
+    """core/structure.h sliced, as the reference's tests/test_structure.cpp:192-207 checks it: indices
+    out of range and an empty selection are errors, repeated indices repeat the site."""
+    from sqsgenerator_b200.core import Structure
+
+    s = Structure(np.diag([1.0, 2.0, 3.0]), np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]]),
+                  [11, 12, 13, 14])
+    assert len(s.sliced(range(4))) == 4
+    with pytest.raises(IndexError):
+        s.sliced(range(-1, 4))
+    with pytest.raises(IndexError):
+        s.sliced(range(3, 6))
+    with pytest.raises(ValueError):
+        s.sliced([])
+    r = s.sliced([1, 1, 1])
+    assert r.species == [12, 12, 12]
+    assert len({tuple(c) for c in r.frac_coords.tolist()}) == 1
+
+
+def test_fcc_naive_shell_distances():
+    """tests/test_structure.cpp:209-220 of the reference: the naive shell distances of an fcc 3x3x3 cell
+    of one species (lattice constant 1) are 0, 1/sqrt(2), 1, sqrt(1.5), sqrt(2), sqrt(2.5), sqrt(3),
+    sqrt(3.5), sqrt(4.5), sqrt(5.5) (its coordination numbers are checked in
+    test_prefactors_and_pairs_match_oracle)."""
+    L, F, Sp = N.supercell(np.eye(3), [[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]], [1, 1, 1, 1], 3, 3, 3)
+    radii = N.distances_naive(N.distance_matrix(L, F), np.finfo(np.float64).eps, 1e-9)
+    want = [0, 1 / np.sqrt(2), 1, np.sqrt(1.5), np.sqrt(2), np.sqrt(2.5), np.sqrt(3), np.sqrt(3.5), np.sqrt(4.5),
+            np.sqrt(5.5)]
+    assert np.allclose(np.asarray(radii), want, rtol=0, atol=1e-9)
