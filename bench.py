@@ -56,12 +56,14 @@ def workload_config(name: str):
         return cases.rocksalt_split("double", cells=(3, 3, 3), iterations=500_000_000, seed=1,
                                     composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}]), (
             "rocksalt 3x3x3 (216 sites) split: Ti54Al54 cations and N96B12 anions optimised together, 2 shells per "
-            "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations, float64")
+            "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations (Floyd sampling: 54 + 12 draws "
+            "each), float64")
     if name == "split_single":
         return cases.rocksalt_split("single", cells=(3, 3, 3), iterations=500_000_000, seed=1,
                                     composition=[{"sites": "Na", "Ti": 54, "Al": 54}, {"sites": "Cl", "N": 96, "B": 12}]), (
             "rocksalt 3x3x3 (216 sites) split: Ti54Al54 cations and N96B12 anions optimised together, 2 shells per "
-            "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations, float32")
+            "sublattice (P=648+324 each), weights 1.0/0.5, 5e8 configurations (Floyd sampling: 54 + 12 draws "
+            "each), float32")
     if name == "fcc500":
         cfg = cases.fcc32("double", composition={"Ti": 167, "Al": 167, "Nb": 166}, iterations=20_000_000, seed=5,
                           shell_weights={"1": 1.0, "2": 0.5, "3": 1.0 / 3, "4": 0.25}, keep=10)
